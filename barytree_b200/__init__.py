@@ -1,0 +1,258 @@
+"""barytree_b200 -- B200-native barycentric treecode (BaryTree drop-in).
+
+Python host side of the library.  It mirrors the reference's ctypes binding
+(``interfaces/python/BaryTreeInterface.py``): the same enums and the same
+``callTreedriver`` function, so existing scripts switch by changing the
+import.  Everything computes in ``libbarytree_b200.so`` (hand-written sm_100a
+CUDA kernels behind a C ABI); there is no CPU fallback, and loading fails
+loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from enum import IntEnum
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbarytree_b200.so")
+
+
+class CEnum(IntEnum):
+    @classmethod
+    def from_param(cls, obj):
+        return int(obj)
+
+
+class Kernel(CEnum):
+    NO_KERNEL = 0
+    COULOMB = 1
+    YUKAWA = 2
+    REGULARIZED_COULOMB = 3
+    REGULARIZED_YUKAWA = 4
+    ATAN = 5
+    TCF = 6
+    DCF = 7
+    SIN_OVER_R = 8
+    MQ = 9
+
+
+class Singularity(CEnum):
+    NO_SINGULARITY = 0
+    SKIPPING = 1
+    SUBTRACTION = 2
+
+
+class Approximation(CEnum):
+    NO_APPROXIMATION = 0
+    LAGRANGE = 1
+    HERMITE = 2
+
+
+class ComputeType(CEnum):
+    NO_COMPUTE_TYPE = 0
+    PARTICLE_CLUSTER = 1
+    CLUSTER_PARTICLE = 2
+    CLUSTER_CLUSTER = 3
+
+
+# status codes (include/barytree_b200.h)
+BT_OK, BT_ERR_PARAM, BT_ERR_UNSUPPORTED, BT_ERR_CUDA, BT_ERR_TIMEOUT, BT_ERR_NO_DEVICE = range(6)
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+DEGREE_FIXED, DEGREE_LEARNED = 0, 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("degree_policy", ctypes.c_int), ("tolerance", ctypes.c_double),
+                ("device", ctypes.c_int), ("inputs_on_device", ctypes.c_int)]
+
+
+class Report(ctypes.Structure):
+    _fields_ = [("ms_total", ctypes.c_double), ("ms_setup", ctypes.c_double), ("ms_upward", ctypes.c_double),
+                ("ms_compute", ctypes.c_double), ("ms_downward", ctypes.c_double), ("ms_transfer", ctypes.c_double),
+                ("num_pp", ctypes.c_longlong), ("num_pc", ctypes.c_longlong), ("num_cp", ctypes.c_longlong),
+                ("num_cc", ctypes.c_longlong), ("pp_ptwise", ctypes.c_longlong), ("pc_ptwise", ctypes.c_longlong),
+                ("cp_ptwise", ctypes.c_longlong), ("cc_ptwise", ctypes.c_longlong),
+                ("ms_eval_kernel", ctypes.c_double), ("eval_flops", ctypes.c_longlong),
+                ("source_nodes", ctypes.c_int), ("target_nodes", ctypes.c_int), ("kernel_launches", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BaryTreeError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"barytree_b200 error {code}: {msg}")
+        self.code = code
+
+
+_BTI_ARGS = (
+    ctypes.c_int, ctypes.c_int,
+    _dp, _dp, _dp, _dp,
+    _dp, _dp, _dp, _dp, _dp,
+    _dp, ctypes.c_int, ctypes.c_int, _dp,
+    ctypes.c_int, ctypes.c_int, ctypes.c_int,
+    ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+    ctypes.c_double, ctypes.c_double, ctypes.c_int,
+)
+
+# every exported symbol of include/barytree_b200.h
+EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
+                    "bt_tree_dump", "bt_last_error", "bt_kernel_launch_count")
+
+_lib = None
+
+
+def lib():
+    """Load libbarytree_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} not found: build it with `make -C barytree_b200/csrc`")
+    L = ctypes.CDLL(LIB_PATH)
+    L.BaryTreeInterface.argtypes = _BTI_ARGS
+    L.BaryTreeInterface.restype = None
+    L.BaryTreeInterface_ex.argtypes = _BTI_ARGS
+    L.BaryTreeInterface_ex.restype = ctypes.c_int
+    L.bt_eval.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                          ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                          ctypes.POINTER(Options), ctypes.POINTER(Report))
+    L.bt_eval.restype = ctypes.c_int
+    L.bt_direct.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                            ctypes.c_int, ctypes.c_double, ctypes.c_int)
+    L.bt_direct.restype = ctypes.c_int
+    L.bt_lists.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp,
+                           ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                           ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip, _ip, _ip, ctypes.c_long)
+    L.bt_lists.restype = ctypes.c_long
+    L.bt_tree_dump.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, ctypes.c_int)
+    L.bt_tree_dump.restype = ctypes.c_int
+    L.bt_last_error.argtypes = ()
+    L.bt_last_error.restype = ctypes.c_char_p
+    L.bt_kernel_launch_count.argtypes = ()
+    L.bt_kernel_launch_count.restype = ctypes.c_longlong
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().bt_last_error().decode()
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _check(rc):
+    if rc != BT_OK:
+        raise BaryTreeError(rc, last_error())
+
+
+def callTreedriver(numTargets, numSources,
+                   targetX, targetY, targetZ, targetValue,
+                   sourceX, sourceY, sourceZ, sourceValue, sourceWeight,
+                   kernelName, numberOfKernelParameters, kernelParameters, singularityHandling,
+                   approximationName, computeType, GPUpresent=True, verbosity=0,
+                   beta=None, theta=None, degree=None, sourceLeafSize=None, targetLeafSize=None, sizeCheck=None):
+    """Evaluate potentials at the targets; same arguments and defaults as the
+    reference binding (interfaces/python/BaryTreeInterface.py:82-152).
+
+    Either ``beta`` or all of theta/degree/sourceLeafSize/targetLeafSize must
+    be given; sizeCheck defaults to 1.0 (Lagrange) or 4.0 (Hermite).  The
+    computation always runs on the GPU; ``GPUpresent`` is accepted for
+    signature compatibility.  Raises BaryTreeError instead of exiting.
+    """
+    if beta:
+        theta, degree, sourceLeafSize, targetLeafSize = -1.0, -1, 1, 1
+    else:
+        assert theta is not None, "If beta isn't provided, theta must be."
+        assert degree is not None, "If beta isn't provided, degree must be."
+        assert sourceLeafSize is not None, "If beta isn't provided, sourceLeafSize must be."
+        assert targetLeafSize is not None, "If beta isn't provided, targetLeafSize must be."
+        beta = -1
+    if not sizeCheck:
+        sizeCheck = 4.0 if approximationName == Approximation.HERMITE else 1.0
+    tx, ty, tz, sx, sy, sz, sq = map(_c, (targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue))
+    tq = _c(targetValue) if targetValue is not None else None
+    sw = _c(sourceWeight) if sourceWeight is not None else None
+    kp = _c(np.atleast_1d(kernelParameters if kernelParameters is not None else [0.0]))
+    out = np.zeros(numTargets)
+    rc = lib().BaryTreeInterface_ex(int(numTargets), int(numSources), _p(tx), _p(ty), _p(tz), _p(tq),
+                                    _p(sx), _p(sy), _p(sz), _p(sq), _p(sw), _p(out), int(kernelName),
+                                    int(numberOfKernelParameters), _p(kp), int(singularityHandling),
+                                    int(approximationName), int(computeType), float(theta), int(degree),
+                                    int(sourceLeafSize), int(targetLeafSize), float(sizeCheck), float(beta),
+                                    int(verbosity))
+    _check(rc)
+    return out
+
+
+def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0,
+             approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER,
+             theta=0.7, degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
+             precision=PRECISION_FP64, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0,
+             return_report=False):
+    """Extended entry point (bt_eval): options for precision / degree policy and a report."""
+    tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
+    out = np.zeros(len(tx))
+    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0)
+    rep = Report()
+    rc = lib().bt_eval(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
+                       int(kernel), float(kernel_param), int(approximation), int(compute_type), float(theta),
+                       int(degree), int(max_source_leaf), int(max_target_leaf), float(size_check),
+                       ctypes.byref(opts), ctypes.byref(rep))
+    _check(rc)
+    return (out, rep.as_dict()) if return_report else out
+
+
+def direct(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0, device=0):
+    """FP64 direct sum on the GPU (error reference)."""
+    tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
+    out = np.zeros(len(tx))
+    rc = lib().bt_direct(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
+                         int(kernel), float(kernel_param), int(device))
+    _check(rc)
+    return out
+
+
+def interaction_lists(tx, ty, tz, sx, sy, sz, compute_type, approximation, theta, degree,
+                      max_source_leaf, max_target_leaf, size_check):
+    """(units, nodes, entries[k,3]) in the canonical (unit, kind, node) form."""
+    tx, ty, tz, sx, sy, sz = map(_c, (tx, ty, tz, sx, sy, sz))
+    units, nodes = ctypes.c_int(0), ctypes.c_int(0)
+    cap = 1 << 16
+    while True:
+        ent = np.zeros(3 * cap, dtype=np.int32)
+        n = lib().bt_lists(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), int(compute_type),
+                           int(approximation), float(theta), int(degree), int(max_source_leaf),
+                           int(max_target_leaf), float(size_check), ctypes.byref(units), ctypes.byref(nodes),
+                           ent.ctypes.data_as(_ip), cap)
+        if n >= 0:
+            return units.value, nodes.value, ent[: 3 * n].reshape(-1, 3)
+        cap *= 4
+
+
+def tree_summary(x, y, z, maxparnode):
+    """Per node (ibeg, iend, num_children, level) and (box..., radius)."""
+    x, y, z = map(_c, (x, y, z))
+    cap = max(64, 4 * len(x) // max(1, maxparnode) + 64)
+    ints = np.zeros(4 * cap, dtype=np.int32)
+    dbl = np.zeros(7 * cap)
+    n = lib().bt_tree_dump(len(x), _p(x), _p(y), _p(z), int(maxparnode), ints.ctypes.data_as(_ip), _p(dbl), cap)
+    if n < 0:
+        raise BaryTreeError(BT_ERR_PARAM, "tree capacity")
+    return ints[: 4 * n].reshape(-1, 4), dbl[: 7 * n].reshape(-1, 7)
+
+
+def kernel_launch_count() -> int:
+    return int(lib().bt_kernel_launch_count())

@@ -1,0 +1,624 @@
+// bt_api.cu -- C ABI of barytree_b200 and the per-call driver.
+//
+// Call flow (mirrors treedriver, src/drivers/treedriver.c:39-1145):
+//   host:   validate + params (RunParams_Setup) -> trees/batches -> MAC lists
+//           -> device work lists (bt_lists.c)
+//   device: upload -> upward pass (P2M, M2M | Hermite P2M) -> grid-output
+//           evaluation (M2L + CP) -> L2L -> particle-output evaluation
+//           (PC + PP) -> L2P -> download
+//   host:   scatter potentials back to the caller's order
+//           (Particles_Targets_Reorder, src/particles/particles.c:58-94)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/barytree_b200.h"
+#include "bt_device.h"
+#include "bt_host.h"
+
+namespace {
+
+thread_local char g_err[512] = "";
+std::atomic<long long> g_launches{0};
+
+void set_err(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+double now_ms()
+{
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+// Grow-only device arena per device, reused across calls so steady-state
+// calls do not touch cudaMalloc.
+struct Arena {
+    char *base = nullptr;
+    size_t cap = 0, used = 0;
+    bool reserve(size_t bytes)
+    {
+        if (bytes <= cap) return true;
+        if (base) cudaFree(base);
+        base = nullptr;
+        cap = 0;
+        if (cudaMalloc(&base, bytes) != cudaSuccess) { cudaGetLastError(); return false; }
+        cap = bytes;
+        return true;
+    }
+    void *take(size_t bytes)
+    {
+        size_t a = (used + 255) & ~size_t(255);
+        used = a + bytes;
+        return base + a;
+    }
+};
+
+struct DeviceCtx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    cudaEvent_t ev[8] = {};
+    std::mutex mu;
+};
+
+DeviceCtx g_ctx[16];
+std::mutex g_ctx_mu;
+
+int get_ctx(int device, DeviceCtx **out)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_err("no CUDA device available");
+        return BT_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev || device >= 16) {
+        set_err("invalid device ordinal %d", device);
+        return BT_ERR_PARAM;
+    }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    DeviceCtx &c = g_ctx[device];
+    if (cudaSetDevice(device) != cudaSuccess) { set_err("cudaSetDevice failed"); return BT_ERR_CUDA; }
+    if (c.device < 0) {
+        if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_err("stream creation failed");
+            return BT_ERR_CUDA;
+        }
+        for (auto &e : c.ev) cudaEventCreate(&e);
+        c.device = device;
+    }
+    *out = &c;
+    return BT_OK;
+}
+
+// Size accounting pass + allocation pass over the same sequence of requests.
+struct Layout {
+    std::vector<std::pair<void **, size_t>> reqs;
+    template <typename T>
+    void add(T **p, size_t count) { reqs.push_back({(void **)p, sizeof(T) * (count > 0 ? count : 1)}); }
+    size_t total() const
+    {
+        size_t s = 0;
+        for (auto &r : reqs) s = ((s + 255) & ~size_t(255)) + r.second;
+        return s + 256;
+    }
+    void bind(Arena &a)
+    {
+        a.used = 0;
+        for (auto &r : reqs) *r.first = a.take(r.second);
+    }
+};
+
+#define CK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            set_err("CUDA error %s at %s:%d", cudaGetErrorString(e_), __FILE__, __LINE__); \
+            rc = BT_ERR_CUDA;                                                         \
+            goto done;                                                                \
+        }                                                                             \
+    } while (0)
+
+int validate(int nt, int ns, const void *tx, const void *ty, const void *tz, const void *sx, const void *sy,
+             const void *sz, const void *sq, const void *out, const bt_params &p)
+{
+    if (nt < 0 || ns < 0) { set_err("negative particle count"); return BT_ERR_PARAM; }
+    if ((nt > 0 && (!tx || !ty || !tz || !out)) || (ns > 0 && (!sx || !sy || !sz || !sq))) {
+        // Particles_Validate (src/particles/particles.c:170-176) exits here
+        set_err("one or more required particle arrays is unset");
+        return BT_ERR_PARAM;
+    }
+    if (p.kernel != COULOMB && p.kernel != YUKAWA && p.kernel != REGULARIZED_COULOMB) {
+        set_err("kernel %d not provided (COULOMB, YUKAWA, REGULARIZED_COULOMB are)", p.kernel);
+        return BT_ERR_UNSUPPORTED;
+    }
+    if (p.sing == SUBTRACTION) { set_err("singularity subtraction is not provided"); return BT_ERR_UNSUPPORTED; }
+    if (p.sing != SKIPPING) { set_err("invalid singularity %d", p.sing); return BT_ERR_PARAM; }
+    if (p.approx != LAGRANGE && p.approx != HERMITE) { set_err("invalid approximation %d", p.approx); return BT_ERR_PARAM; }
+    if (p.ctype != PARTICLE_CLUSTER && p.ctype != CLUSTER_PARTICLE && p.ctype != CLUSTER_CLUSTER) {
+        set_err("invalid compute type %d", p.ctype);
+        return BT_ERR_PARAM;
+    }
+    if (p.ctype == CLUSTER_CLUSTER && p.approx == HERMITE) {
+        // src/interaction_compute/interaction_compute_cc.c:146-147
+        set_err("cluster-cluster Hermite is inoperable in the reference and not provided");
+        return BT_ERR_UNSUPPORTED;
+    }
+    if (p.degree < 1 || p.degree > 12) { set_err("interpolation degree %d outside 1..12", p.degree); return BT_ERR_UNSUPPORTED; }
+    if (p.maxs < 1 || p.maxt < 1) { set_err("leaf sizes must be >= 1"); return BT_ERR_PARAM; }
+    if (!(p.theta > 0.0)) { set_err("theta must be > 0"); return BT_ERR_PARAM; }
+    return BT_OK;
+}
+
+void hermite_ww(int n, double *ww)
+{
+    // src/clusters/clusters.c:1289-1300
+    for (int i = 0; i <= n; i++) {
+        double xx = i * M_PI / n;
+        ww[i] = -cos(xx) / (2 * sin(xx) * sin(xx));
+    }
+    ww[0] = 0.25 * (n * n / 3.0 + 1.0 / 6.0);
+    ww[n] = -ww[0];
+}
+
+void fill_grids(const bt_tree &t, int n, std::vector<double> &grid, std::vector<double> &len)
+{
+    int np1 = n + 1;
+    grid.assign((size_t)t.n * 3 * np1, 0.0);
+    len.assign((size_t)t.n * 3, 0.0);
+    for (int i = 0; i < t.n; i++) {
+        double *g = grid.data() + (size_t)i * 3 * np1;
+        bt_cheb_nodes(n, t.x0[i], t.x1[i], g);
+        bt_cheb_nodes(n, t.y0[i], t.y1[i], g + np1);
+        bt_cheb_nodes(n, t.z0[i], t.z1[i], g + 2 * np1);
+        len[3 * i] = t.x1[i] - t.x0[i];
+        len[3 * i + 1] = t.y1[i] - t.y0[i];
+        len[3 * i + 2] = t.z1[i] - t.z0[i];
+    }
+}
+
+// Work items (unit, chunk) sorted by decreasing cost so the block scheduler
+// starts the longest work first.
+std::vector<int2> make_items(int units, const int *count_of_unit, int chunk, const std::vector<double> &cost)
+{
+    std::vector<std::pair<double, int2>> v;
+    for (int u = 0; u < units; u++) {
+        int m = count_of_unit[u];
+        int nch = (m + chunk - 1) / chunk;
+        for (int c = 0; c < nch; c++) v.push_back({cost[u], make_int2(u, c)});
+    }
+    std::stable_sort(v.begin(), v.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    std::vector<int2> out(v.size());
+    for (size_t i = 0; i < v.size(); i++) out[i] = v[i].second;
+    return out;
+}
+
+void count_interactions(const bt_plan &pl, bt_report *r)
+{
+    // pointwise counts as src/drivers/treedriver.c:185-202, 467-483, 757-793
+    const bt_params &o = pl.prm;
+    long long P = o.P;
+    r->num_pp = r->num_pc = r->num_cp = r->num_cc = 0;
+    r->pp_ptwise = r->pc_ptwise = r->cp_ptwise = r->cc_ptwise = 0;
+    if (o.ctype == PARTICLE_CLUSTER || o.ctype == CLUSTER_PARTICLE) {
+        const bt_tree &trav = o.ctype == PARTICLE_CLUSTER ? pl.st : pl.tt;
+        const bt_tree &bat = o.ctype == PARTICLE_CLUSTER ? pl.tt : pl.st;
+        for (int i = 0; i < bat.nleaves; i++) {
+            long long m = bat.numpar[bat.leaves[i]];
+            for (int64_t k = pl.pp.off[i]; k < pl.pp.off[i + 1]; k++) r->pp_ptwise += m * trav.numpar[pl.pp.idx[k]];
+            long long na = pl.ap.off[i + 1] - pl.ap.off[i];
+            if (o.ctype == PARTICLE_CLUSTER) r->pc_ptwise += na * m * P;
+            else r->cp_ptwise += na * m * P;
+            r->num_pp += pl.pp.off[i + 1] - pl.pp.off[i];
+            if (o.ctype == PARTICLE_CLUSTER) r->num_pc += na; else r->num_cp += na;
+        }
+    } else {
+        for (int i = 0; i < pl.tt.n; i++) {
+            long long m = pl.tt.numpar[i];
+            for (int64_t k = pl.pp.off[i]; k < pl.pp.off[i + 1]; k++) r->pp_ptwise += m * pl.st.numpar[pl.pp.idx[k]];
+            for (int64_t k = pl.cp.off[i]; k < pl.cp.off[i + 1]; k++) r->cp_ptwise += P * pl.st.numpar[pl.cp.idx[k]];
+            r->pc_ptwise += (pl.pc.off[i + 1] - pl.pc.off[i]) * m * P;
+            r->cc_ptwise += (pl.ap.off[i + 1] - pl.ap.off[i]) * P * P;
+            r->num_pp += pl.pp.off[i + 1] - pl.pp.off[i];
+            r->num_pc += pl.pc.off[i + 1] - pl.pc.off[i];
+            r->num_cp += pl.cp.off[i + 1] - pl.cp.off[i];
+            r->num_cc += pl.ap.off[i + 1] - pl.ap.off[i];
+        }
+    }
+}
+
+// Build the host plan: copies, trees, lists.
+void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty, const double *tz,
+                const double *sx, const double *sy, const double *sz, const double *sq)
+{
+    bt_parts_init(&pl.src, ns, sx, sy, sz, sq);
+    bt_parts_init(&pl.tgt, nt, tx, ty, tz, nullptr);
+    bt_tree_build(&pl.st, &pl.src, pl.prm.maxs);
+    bt_tree_build(&pl.tt, &pl.tgt, pl.prm.maxt);
+    bt_plan_lists(&pl);
+}
+
+// Device evaluation of a built plan; writes potentials in caller order to out_host.
+int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out_host, bt_report *rep)
+{
+    const bt_params &o = pl.prm;
+    const int n = o.degree, np1 = n + 1, P = o.P;
+    const bool herm = o.approx == HERMITE;
+    const int nq = herm ? 8 : 1;
+    const bt_tree &S = pl.st, &T = pl.tt;
+    const int ns = pl.src.n, nt = pl.tgt.n;
+    cudaStream_t st = ctx->stream;
+    int rc = BT_OK;
+    double t0 = now_ms();
+    long long launches = 0;
+
+    std::vector<double> sgrid, slen, tgrid, tlen;
+    fill_grids(S, n, sgrid, slen);
+    fill_grids(T, n, tgrid, tlen);
+    double ww[BT_MAX_DEGREE + 1];
+    hermite_ww(n, ww);
+
+    // work items
+    const bool need_src_clusters = (o.ctype != CLUSTER_PARTICLE);
+    const bool need_tgt_grids = (o.ctype != PARTICLE_CLUSTER);
+    std::vector<int> leaf_count(T.nleaves);
+    std::vector<double> leaf_cost(T.nleaves, 0.0);
+    for (int u = 0; u < T.nleaves; u++) {
+        leaf_count[u] = T.numpar[T.leaves[u]];
+        double c = 0;
+        c += (double)(pl.t_approx.off[u + 1] - pl.t_approx.off[u]) * P * nq;
+        for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) c += S.numpar[pl.t_direct.idx[k]];
+        leaf_cost[u] = c;
+    }
+    std::vector<int2> ev_items = make_items(T.nleaves, leaf_count.data(), 128, leaf_cost);
+    std::vector<int2> grid_items, l2p_items;
+    if (need_tgt_grids) {
+        std::vector<int> pcount(T.n, P);
+        std::vector<double> gcost(T.n, 0.0);
+        for (int i = 0; i < T.n; i++) {
+            double c = (double)(pl.g_cc.off[i + 1] - pl.g_cc.off[i]) * P;
+            for (int64_t k = pl.g_cp.off[i]; k < pl.g_cp.off[i + 1]; k++) c += S.numpar[pl.g_cp.idx[k]] * nq;
+            gcost[i] = c;
+        }
+        grid_items = make_items(T.n, pcount.data(), 128, gcost);
+        std::vector<double> lcost(T.nleaves, 1.0);
+        l2p_items = make_items(T.nleaves, leaf_count.data(), 128, lcost);
+    }
+    std::vector<int> s_nleafpar;
+
+    // device layout
+    double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx, *d_ty, *d_tz, *d_pot, *d_sgrid, *d_tgrid, *d_slen, *d_tlen, *d_ww;
+    double *d_Q = nullptr, *d_Phi = nullptr;
+    int *d_sibeg, *d_snum, *d_snch, *d_sch, *d_sleaves, *d_slvl;
+    int *d_tibeg, *d_tnum, *d_tnch, *d_tch, *d_tpar, *d_tleaves, *d_tlvl;
+    int64_t *d_aoff, *d_doff, *d_ccoff, *d_cpoff;
+    int *d_aidx, *d_didx, *d_ccidx, *d_cpidx;
+    int2 *d_evitems, *d_griditems, *d_l2pitems;
+    Layout L;
+    L.add(&d_sx, ns); L.add(&d_sy, ns); L.add(&d_sz, ns); L.add(&d_sq, ns);
+    L.add(&d_tx, nt); L.add(&d_ty, nt); L.add(&d_tz, nt); L.add(&d_pot, nt);
+    L.add(&d_sgrid, sgrid.size()); L.add(&d_tgrid, tgrid.size());
+    L.add(&d_slen, slen.size()); L.add(&d_tlen, tlen.size()); L.add(&d_ww, BT_MAX_DEGREE + 1);
+    if (need_src_clusters) L.add(&d_Q, (size_t)S.n * P * nq);
+    if (need_tgt_grids) L.add(&d_Phi, (size_t)T.n * P * nq);
+    L.add(&d_sibeg, S.n); L.add(&d_snum, S.n); L.add(&d_snch, S.n); L.add(&d_sch, 8 * (size_t)S.n);
+    L.add(&d_sleaves, S.nleaves); L.add(&d_slvl, S.lvl_off ? S.lvl_off[S.max_depth] : 0);
+    L.add(&d_tibeg, T.n); L.add(&d_tnum, T.n); L.add(&d_tnch, T.n); L.add(&d_tch, 8 * (size_t)T.n);
+    L.add(&d_tpar, T.n); L.add(&d_tleaves, T.nleaves); L.add(&d_tlvl, T.lvl_off ? T.lvl_off[T.max_depth] : 0);
+    L.add(&d_aoff, pl.t_approx.rows + 1); L.add(&d_aidx, pl.t_approx.off[pl.t_approx.rows]);
+    L.add(&d_doff, pl.t_direct.rows + 1); L.add(&d_didx, pl.t_direct.off[pl.t_direct.rows]);
+    L.add(&d_ccoff, pl.g_cc.rows + 1); L.add(&d_ccidx, pl.g_cc.off[pl.g_cc.rows]);
+    L.add(&d_cpoff, pl.g_cp.rows + 1); L.add(&d_cpidx, pl.g_cp.off[pl.g_cp.rows]);
+    L.add(&d_evitems, ev_items.size()); L.add(&d_griditems, grid_items.size()); L.add(&d_l2pitems, l2p_items.size());
+
+    if (!ctx->arena.reserve(L.total())) {
+        set_err("device allocation of %zu bytes failed", L.total());
+        return BT_ERR_CUDA;
+    }
+    L.bind(ctx->arena);
+
+    double t_setup = now_ms();
+    {
+#define UP(dst, src, cnt)                                                                              \
+    if ((cnt) > 0) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
+        UP(d_sx, pl.src.x, ns); UP(d_sy, pl.src.y, ns); UP(d_sz, pl.src.z, ns); UP(d_sq, pl.src.q, ns);
+        UP(d_tx, pl.tgt.x, nt); UP(d_ty, pl.tgt.y, nt); UP(d_tz, pl.tgt.z, nt);
+        UP(d_sgrid, sgrid.data(), sgrid.size()); UP(d_tgrid, tgrid.data(), tgrid.size());
+        UP(d_slen, slen.data(), slen.size()); UP(d_tlen, tlen.data(), tlen.size());
+        UP(d_ww, ww, n + 1);
+        UP(d_sibeg, S.ibeg, S.n); UP(d_snum, S.numpar, S.n); UP(d_snch, S.nchild, S.n); UP(d_sch, S.child, 8 * (size_t)S.n);
+        UP(d_sleaves, S.leaves, S.nleaves);
+        if (S.lvl_off) UP(d_slvl, S.lvl_nodes, S.lvl_off[S.max_depth]);
+        UP(d_tibeg, T.ibeg, T.n); UP(d_tnum, T.numpar, T.n); UP(d_tnch, T.nchild, T.n); UP(d_tch, T.child, 8 * (size_t)T.n);
+        UP(d_tpar, T.parent, T.n); UP(d_tleaves, T.leaves, T.nleaves);
+        if (T.lvl_off) UP(d_tlvl, T.lvl_nodes, T.lvl_off[T.max_depth]);
+        UP(d_aoff, pl.t_approx.off, pl.t_approx.rows + 1); UP(d_aidx, pl.t_approx.idx, pl.t_approx.off[pl.t_approx.rows]);
+        UP(d_doff, pl.t_direct.off, pl.t_direct.rows + 1); UP(d_didx, pl.t_direct.idx, pl.t_direct.off[pl.t_direct.rows]);
+        UP(d_ccoff, pl.g_cc.off, pl.g_cc.rows + 1); UP(d_ccidx, pl.g_cc.idx, pl.g_cc.off[pl.g_cc.rows]);
+        UP(d_cpoff, pl.g_cp.off, pl.g_cp.rows + 1); UP(d_cpidx, pl.g_cp.idx, pl.g_cp.off[pl.g_cp.rows]);
+        UP(d_evitems, ev_items.data(), ev_items.size());
+        UP(d_griditems, grid_items.data(), grid_items.size());
+        UP(d_l2pitems, l2p_items.data(), l2p_items.size());
+#undef UP
+        cudaEvent_t *ev = ctx->ev;
+        CK(cudaEventRecord(ev[0], st));
+        // upward pass
+        if (need_src_clusters && ns > 0) {
+            bt::launch_p2m(n, herm, S.nleaves, d_sleaves, S.n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
+                           d_sz, d_sq, d_Q, st);
+            launches++;
+            if (!herm) {
+                for (int l = S.max_depth - 1; l >= 0; l--) {
+                    int cnt = S.lvl_off[l + 1] - S.lvl_off[l];
+                    if (cnt > 0) {
+                        bt::launch_m2m(n, cnt, d_slvl + S.lvl_off[l], d_snch, d_sch, d_sgrid, d_Q, st);
+                        launches++;
+                    }
+                }
+            }
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev[1], st));
+        // grid-output evaluation (CP, M2L) and L2L
+        if (need_tgt_grids && nt > 0) {
+            bt::EvalGridsArgs g;
+            g.n = n; g.nitems = (int)grid_items.size(); g.items = d_griditems; g.t_grid = d_tgrid;
+            g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_cpoff; g.p_idx = d_cpidx;
+            g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.Q = d_Q;
+            g.sx = d_sx; g.sy = d_sy; g.sz = d_sz; g.sq = d_sq; g.kp = o.kp; g.Phi = d_Phi;
+            bt::launch_eval_grids(o.kernel, herm, g, st);
+            launches++;
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev[2], st));
+        // particle-output evaluation (PC, PP)
+        if (nt > 0) {
+            bt::EvalTargetsArgs a;
+            a.n = n; a.nitems = (int)ev_items.size(); a.items = d_evitems; a.leaf_node = d_tleaves;
+            a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.a_off = d_aoff; a.a_idx = d_aidx; a.d_off = d_doff; a.d_idx = d_didx;
+            a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_grid = d_sgrid; a.Q = d_Q;
+            a.sx = d_sx; a.sy = d_sy; a.sz = d_sz; a.sq = d_sq; a.tx = d_tx; a.ty = d_ty; a.tz = d_tz;
+            a.kp = o.kp; a.pot = d_pot;
+            bt::launch_eval_targets(o.kernel, herm, a, st);
+            launches++;
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev[3], st));
+        // downward pass
+        if (need_tgt_grids && nt > 0) {
+            if (!herm) {
+                for (int l = 0; l < T.max_depth; l++) {
+                    int cnt = T.lvl_off[l + 1] - T.lvl_off[l];
+                    if (cnt > 0) {
+                        bt::launch_l2l(n, cnt, d_tlvl + T.lvl_off[l], d_tnch, d_tch, d_tgrid, d_Phi, st);
+                        launches++;
+                    }
+                }
+            }
+            bt::launch_l2p(n, herm, (int)l2p_items.size(), d_l2pitems, d_tleaves, d_tpar, d_tibeg, d_tnum, d_tgrid,
+                           d_tlen, d_ww, d_Phi, d_tx, d_ty, d_tz, d_pot, st);
+            launches++;
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev[4], st));
+        std::vector<double> pot(nt > 0 ? nt : 1);
+        if (nt > 0) CK(cudaMemcpyAsync(pot.data(), d_pot, sizeof(double) * nt, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int i = 0; i < nt; i++) out_host[pl.tgt.order[i]] = pot[i];
+        g_launches += launches;
+        if (rep) {
+            float a = 0, b = 0, c = 0, d = 0;
+            cudaEventElapsedTime(&a, ev[0], ev[1]);
+            cudaEventElapsedTime(&b, ev[1], ev[2]);
+            cudaEventElapsedTime(&c, ev[2], ev[3]);
+            cudaEventElapsedTime(&d, ev[3], ev[4]);
+            rep->ms_upward = a;
+            rep->ms_compute = b + c;
+            rep->ms_downward = d;
+            rep->ms_eval_kernel = c;
+            rep->kernel_launches = (int)launches;
+            rep->source_nodes = S.n;
+            rep->target_nodes = T.n;
+            double tend = now_ms();
+            rep->ms_transfer = (tend - t_setup) - (a + b + c + d);
+            rep->ms_total += tend - t0;
+        }
+    }
+done:
+    return rc;
+}
+
+int eval_common(int nt, int ns, const double *tx, const double *ty, const double *tz, const double *sx,
+                const double *sy, const double *sz, const double *sq, double *out, bt_params &prm,
+                const bt_options *opts, bt_report *rep)
+{
+    g_err[0] = 0;
+    int rc = validate(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, prm);
+    if (rc != BT_OK) return rc;
+    if (nt > 0) memset(out, 0, sizeof(double) * (size_t)nt);
+    if (rep) memset(rep, 0, sizeof(*rep));
+    if (nt == 0 || ns == 0) return BT_OK;
+    int device = opts ? opts->device : 0;
+    if (opts && opts->precision != BT_PRECISION_FP64) { set_err("mixed precision not provided yet"); return BT_ERR_UNSUPPORTED; }
+    DeviceCtx *ctx = nullptr;
+    rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    double t0 = now_ms();
+    bt_plan pl;
+    memset(&pl, 0, sizeof pl);
+    pl.prm = prm;
+    build_plan(pl, nt, ns, tx, ty, tz, sx, sy, sz, sq);
+    double t1 = now_ms();
+    if (rep) {
+        rep->ms_setup = t1 - t0;
+        rep->ms_total = t1 - t0;
+        count_interactions(pl, rep);
+    }
+    rc = run_plan(ctx, pl, out, rep);
+    bt_plan_free(&pl);
+    if (rc != BT_OK) memset(out, 0, sizeof(double) * (size_t)nt);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *bt_last_error(void) { return g_err; }
+
+long long bt_kernel_launch_count(void) { return g_launches.load(); }
+
+int BaryTreeInterface_ex(int numTargets, int numSources, const double *targetX, const double *targetY,
+                         const double *targetZ, const double *targetValue, const double *sourceX,
+                         const double *sourceY, const double *sourceZ, const double *sourceValue,
+                         const double *sourceWeight, double *outputArray, int kernel, int numKernelParams,
+                         const double *kernelParams, int singularity, int approximation, int compute_type,
+                         double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+                         double sizeCheck, double beta, int verbosity)
+{
+    (void)targetValue; (void)sourceWeight;
+    bt_params prm;
+    bt_params_setup(&prm, kernel, numKernelParams, kernelParams, singularity, approximation, compute_type, theta,
+                    interpOrder, maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, beta, verbosity);
+    bt_report rep;
+    int rc = eval_common(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+                         outputArray, prm, nullptr, verbosity > 0 ? &rep : nullptr);
+    if (verbosity > 0 && rc == BT_OK) {
+        printf("[BaryTree] barytree_b200: %d targets, %d sources, setup %.3f ms, upward %.3f ms, "
+               "compute %.3f ms, downward %.3f ms, total %.3f ms\n",
+               numTargets, numSources, rep.ms_setup, rep.ms_upward, rep.ms_compute, rep.ms_downward, rep.ms_total);
+    }
+    return rc;
+}
+
+void BaryTreeInterface(int numTargets, int numSources, double *targetX, double *targetY, double *targetZ,
+                       double *targetValue, double *sourceX, double *sourceY, double *sourceZ, double *sourceValue,
+                       double *sourceWeight, double *outputArray, KERNEL kernel, int numKernelParams,
+                       double *kernelParams, SINGULARITY singularity, APPROXIMATION approximation,
+                       COMPUTE_TYPE compute_type, double theta, int interpOrder, int maxPerSourceLeaf,
+                       int maxPerTargetLeaf, double sizeCheck, double beta, int verbosity)
+{
+    int rc = BaryTreeInterface_ex(numTargets, numSources, targetX, targetY, targetZ, targetValue, sourceX, sourceY,
+                                  sourceZ, sourceValue, sourceWeight, outputArray, kernel, numKernelParams,
+                                  kernelParams, singularity, approximation, compute_type, theta, interpOrder,
+                                  maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, beta, verbosity);
+    if (rc != BT_OK) fprintf(stderr, "[BaryTree] ERROR (%d): %s\n", rc, g_err);
+}
+
+int bt_eval(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,
+            const double *sourceX, const double *sourceY, const double *sourceZ, const double *sourceValue,
+            double *outputArray, int kernel, double kernelParam, int approximation, int compute_type, double theta,
+            int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck, const bt_options *opts,
+            bt_report *report)
+{
+    bt_params prm;
+    bt_params_setup(&prm, kernel, 1, &kernelParam, SKIPPING, approximation, compute_type, theta, interpOrder,
+                    maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
+    return eval_common(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+                       outputArray, prm, opts, report);
+}
+
+int bt_direct(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,
+              const double *sourceX, const double *sourceY, const double *sourceZ, const double *sourceValue,
+              double *outputArray, int kernel, double kernelParam, int device)
+{
+    g_err[0] = 0;
+    if (numTargets < 0 || numSources < 0) { set_err("negative count"); return BT_ERR_PARAM; }
+    if (numTargets == 0) return BT_OK;
+    if (!targetX || !targetY || !targetZ || !outputArray || (numSources > 0 && (!sourceX || !sourceY || !sourceZ || !sourceValue))) {
+        set_err("NULL array");
+        return BT_ERR_PARAM;
+    }
+    if (kernel != COULOMB && kernel != YUKAWA && kernel != REGULARIZED_COULOMB) { set_err("kernel not provided"); return BT_ERR_UNSUPPORTED; }
+    DeviceCtx *ctx = nullptr;
+    int rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = ctx->stream;
+    double *d_t[3], *d_s[4], *d_o;
+    {
+        Layout L;
+        for (int i = 0; i < 3; i++) L.add(&d_t[i], numTargets);
+        for (int i = 0; i < 4; i++) L.add(&d_s[i], numSources);
+        L.add(&d_o, numTargets);
+        if (!ctx->arena.reserve(L.total())) { set_err("device allocation failed"); return BT_ERR_CUDA; }
+        L.bind(ctx->arena);
+        const double *ht[3] = {targetX, targetY, targetZ};
+        const double *hs[4] = {sourceX, sourceY, sourceZ, sourceValue};
+        for (int i = 0; i < 3; i++) CK(cudaMemcpyAsync(d_t[i], ht[i], sizeof(double) * numTargets, cudaMemcpyHostToDevice, st));
+        if (numSources > 0)
+            for (int i = 0; i < 4; i++) CK(cudaMemcpyAsync(d_s[i], hs[i], sizeof(double) * numSources, cudaMemcpyHostToDevice, st));
+        bt::launch_direct(kernel, numTargets, numSources, d_t[0], d_t[1], d_t[2], d_s[0], d_s[1], d_s[2], d_s[3],
+                          kernelParam, d_o, st);
+        g_launches += 1;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(outputArray, d_o, sizeof(double) * numTargets, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+done:
+    return rc;
+}
+
+long bt_lists(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,
+              const double *sourceX, const double *sourceY, const double *sourceZ, int compute_type,
+              int approximation, double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+              double sizeCheck, int *units, int *nodes, int *entries, long cap)
+{
+    bt_plan pl;
+    memset(&pl, 0, sizeof pl);
+    bt_params_setup(&pl.prm, COULOMB, 0, nullptr, SKIPPING, approximation, compute_type, theta, interpOrder,
+                    maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
+    build_plan(pl, numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, nullptr);
+    *units = pl.pp.rows;
+    *nodes = compute_type == CLUSTER_PARTICLE ? pl.tt.n : pl.st.n;
+    long cnt = 0;
+    for (int u = 0; u < pl.pp.rows; u++) {
+        const bt_csr *kinds[4] = {&pl.pp, &pl.ap, &pl.pc, &pl.cp};
+        for (int k = 0; k < 4; k++)
+            for (int64_t e = kinds[k]->off[u]; e < kinds[k]->off[u + 1]; e++) {
+                if (cnt < cap) {
+                    entries[3 * cnt] = u; entries[3 * cnt + 1] = k; entries[3 * cnt + 2] = kinds[k]->idx[e];
+                }
+                cnt++;
+            }
+    }
+    bt_plan_free(&pl);
+    return cnt <= cap ? cnt : -1;
+}
+
+int bt_tree_dump(int n, const double *x, const double *y, const double *z, int maxparnode, int *ints, double *dbl, int cap)
+{
+    bt_parts p;
+    bt_parts_init(&p, n, x, y, z, nullptr);
+    bt_tree t;
+    bt_tree_build(&t, &p, maxparnode);
+    int nn = t.n;
+    if (nn <= cap) {
+        for (int i = 0; i < nn; i++) {
+            ints[4 * i] = t.ibeg[i] + 1; ints[4 * i + 1] = t.ibeg[i] + t.numpar[i];
+            ints[4 * i + 2] = t.nchild[i]; ints[4 * i + 3] = t.level[i];
+            double d[7] = {t.x0[i], t.x1[i], t.y0[i], t.y1[i], t.z0[i], t.z1[i], t.rad[i]};
+            memcpy(dbl + 7 * i, d, sizeof d);
+        }
+    }
+    bt_tree_free(&t);
+    bt_parts_free(&p);
+    return nn <= cap ? nn : -1;
+}
+
+}  // extern "C"

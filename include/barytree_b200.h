@@ -1,0 +1,149 @@
+/*
+ * barytree_b200 -- B200-native barycentric treecode behind BaryTree's C entry point.
+ *
+ * C ABI only: plain pointers, sizes and enums.  All arrays are caller-owned
+ * host memory unless a function says otherwise.  Library: libbarytree_b200.so.
+ */
+#ifndef BARYTREE_B200_H
+#define BARYTREE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Enum values are fixed by the reference's public header
+ * (src/interface/BaryTreeInterface.h:7-48), so existing callers and their
+ * ctypes/Fortran bindings pass the same integers. */
+#ifndef H_BARYTREE_TYPES_H
+#define H_BARYTREE_TYPES_H
+typedef enum KERNEL {
+    NO_KERNEL, COULOMB, YUKAWA, REGULARIZED_COULOMB, REGULARIZED_YUKAWA,
+    ATAN, TCF, DCF, SIN_OVER_R, MQ, RBS_U, RBS_V, USER
+} KERNEL;
+typedef enum SINGULARITY { NO_SINGULARITY, SKIPPING, SUBTRACTION } SINGULARITY;
+typedef enum APPROXIMATION { NO_APPROX, LAGRANGE, HERMITE } APPROXIMATION;
+typedef enum COMPUTE_TYPE { NO_COMPUTE_TYPE, PARTICLE_CLUSTER, CLUSTER_PARTICLE, CLUSTER_CLUSTER } COMPUTE_TYPE;
+#endif
+
+/* Status codes returned by the *_ex / bt_* entry points. */
+enum {
+    BT_OK = 0,
+    BT_ERR_PARAM = 1,        /* invalid argument (NULL array, bad size, bad enum) */
+    BT_ERR_UNSUPPORTED = 2,  /* valid but not provided (the reference exits here too) */
+    BT_ERR_CUDA = 3,         /* CUDA runtime error or allocation failure */
+    BT_ERR_TIMEOUT = 4,      /* a bounded device wait expired */
+    BT_ERR_NO_DEVICE = 5     /* no usable CUDA device */
+};
+
+/* Drop-in replacement for the reference entry point
+ * (src/interface/BaryTreeInterface.h:52-59, src/interface/BaryTreeInterface.c:18-62).
+ * Same arguments, same meaning: outputArray is zeroed, then receives the
+ * potential at each target in the caller's order.  Inputs are not modified.
+ * The reference exits the process on invalid or unsupported combinations;
+ * this version prints the reason and returns with outputArray zeroed
+ * (call BaryTreeInterface_ex to get the status).  No MPI is required. */
+void BaryTreeInterface(int numTargets, int numSources,
+                       double *targetX, double *targetY, double *targetZ, double *targetValue,
+                       double *sourceX, double *sourceY, double *sourceZ, double *sourceValue,
+                       double *sourceWeight, double *outputArray,
+                       KERNEL kernel, int numKernelParams, double *kernelParams,
+                       SINGULARITY singularity, APPROXIMATION approximation, COMPUTE_TYPE compute_type,
+                       double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+                       double sizeCheck, double beta, int verbosity);
+
+/* Same as BaryTreeInterface, returning a BT_* status instead of exiting. */
+int BaryTreeInterface_ex(int numTargets, int numSources,
+                         const double *targetX, const double *targetY, const double *targetZ,
+                         const double *targetValue,
+                         const double *sourceX, const double *sourceY, const double *sourceZ,
+                         const double *sourceValue, const double *sourceWeight, double *outputArray,
+                         int kernel, int numKernelParams, const double *kernelParams,
+                         int singularity, int approximation, int compute_type,
+                         double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+                         double sizeCheck, double beta, int verbosity);
+
+/* ---------------------------------------------------------------------- */
+/* Extended interface (no counterpart in the reference).                   */
+/* ---------------------------------------------------------------------- */
+
+/* Arithmetic of the interaction kernels. */
+enum { BT_PRECISION_FP64 = 0,   /* plain FP64 everywhere (the parity path)            */
+       BT_PRECISION_MIXED = 1   /* FP32 kernel evaluations on centre-relative coordinates,
+                                   compensated per-target accumulation, FP64 boxes, node
+                                   placement, coincidence tests and final reduction      */ };
+
+/* Interpolation degree policy. */
+enum { BT_DEGREE_FIXED = 0,     /* every approximation uses interpOrder                 */
+       BT_DEGREE_LEARNED = 1    /* per-interaction degree from the loaded selector MLP  */ };
+
+/* Per-call options.  Zero-initialise, then set what you need. */
+typedef struct bt_options {
+    int precision;        /* BT_PRECISION_*                                          */
+    int degree_policy;    /* BT_DEGREE_*                                             */
+    double tolerance;     /* target relative L2 error for BT_DEGREE_LEARNED           */
+    int device;           /* CUDA device ordinal                                      */
+    int inputs_on_device; /* 1: the x,y,z,q pointers passed to bt_eval are device
+                             pointers (FP64) and output is a device pointer          */
+} bt_options;
+
+/* Per-call report (all optional: pass NULL). */
+typedef struct bt_report {
+    double ms_total, ms_setup, ms_upward, ms_compute, ms_downward, ms_transfer;
+    long long num_pp, num_pc, num_cp, num_cc;                 /* cluster-wise interactions */
+    long long pp_ptwise, pc_ptwise, cp_ptwise, cc_ptwise;     /* pointwise, counted as the
+                                                                 reference counts them
+                                                                 (src/drivers/treedriver.c:467-483,757-793) */
+    double ms_eval_kernel;     /* device time of the dominant evaluation kernel */
+    long long eval_flops;      /* algorithmic FLOPs of that kernel               */
+    int source_nodes, target_nodes, kernel_launches;
+} bt_report;
+
+/* Treecode evaluation with options and a report.  Same meaning of the
+ * physical arguments as BaryTreeInterface_ex. */
+int bt_eval(int numTargets, int numSources,
+            const double *targetX, const double *targetY, const double *targetZ,
+            const double *sourceX, const double *sourceY, const double *sourceZ,
+            const double *sourceValue, double *outputArray,
+            int kernel, double kernelParam, int approximation, int compute_type,
+            double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+            double sizeCheck, const bt_options *opts, bt_report *report);
+
+/* FP64 direct sum on the GPU (the error reference for large N):
+ * out[i] = sum_j q_j K(t_i, s_j) with the reference's skipping rules
+ * (src/interaction_compute/interaction_compute_direct.c:26-231). */
+int bt_direct(int numTargets, int numSources,
+              const double *targetX, const double *targetY, const double *targetZ,
+              const double *sourceX, const double *sourceY, const double *sourceZ,
+              const double *sourceValue, double *outputArray,
+              int kernel, double kernelParam, int device);
+
+/* Interaction lists as the product builds them, in the canonical triple form
+ * (unit, kind, node): kind 0 = PP, 1 = approx (PC / CP / CC), 2 = PC (CC
+ * mode), 3 = CP (CC mode).  Mirrors InteractionLists_Make
+ * (src/interaction_lists/interaction_lists.c:48-234).  Returns the number of
+ * triples, or -1 if `cap` is too small. */
+long bt_lists(int numTargets, int numSources,
+              const double *targetX, const double *targetY, const double *targetZ,
+              const double *sourceX, const double *sourceY, const double *sourceZ,
+              int compute_type, int approximation, double theta, int interpOrder,
+              int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck,
+              int *units, int *nodes, int *entries, long cap);
+
+/* Tree summary, as bto_tree in the oracle: per node (ibeg 1-based, iend,
+ * num_children, level) and (x_min,x_max,y_min,y_max,z_min,z_max,radius).
+ * Mirrors Tree_Sources_Construct (src/tree/tree.c:19-59). */
+int bt_tree_dump(int n, const double *x, const double *y, const double *z, int maxparnode,
+            int *ints, double *dbl, int cap);
+
+/* Last error message of the calling thread ("" if none). */
+const char *bt_last_error(void);
+
+/* Number of CUDA kernels this library launched in this process (for checks). */
+long long bt_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BARYTREE_B200_H */
