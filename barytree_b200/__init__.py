@@ -102,7 +102,7 @@ _BTI_ARGS = (
 
 # every exported symbol of include/barytree_b200.h
 EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
-                    "bt_tree_dump", "bt_last_error", "bt_kernel_launch_count")
+                    "bt_tree_dump", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count")
 
 _lib = None
 
@@ -133,6 +133,8 @@ def lib():
     L.bt_lists.restype = ctypes.c_long
     L.bt_tree_dump.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, ctypes.c_int)
     L.bt_tree_dump.restype = ctypes.c_int
+    L.bt_measure_peaks.argtypes = (ctypes.c_int, _dp, _dp, _dp)
+    L.bt_measure_peaks.restype = ctypes.c_int
     L.bt_last_error.argtypes = ()
     L.bt_last_error.restype = ctypes.c_char_p
     L.bt_kernel_launch_count.argtypes = ()
@@ -213,6 +215,29 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
                        ctypes.byref(opts), ctypes.byref(rep))
     _check(rc)
     return (out, rep.as_dict()) if return_report else out
+
+
+def treecode_ptr(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, kernel=Kernel.COULOMB, kernel_param=0.0,
+                 approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7,
+                 degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64,
+                 degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0, inputs_on_device=False):
+    """bt_eval on raw addresses (ints): device pointers when inputs_on_device, else host pointers."""
+    cast = lambda a: ctypes.cast(ctypes.c_void_p(int(a)), _dp)  # noqa: E731
+    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), int(bool(inputs_on_device)))
+    rep = Report()
+    rc = lib().bt_eval(int(nt), int(ns), cast(tx), cast(ty), cast(tz), cast(sx), cast(sy), cast(sz), cast(sq),
+                       cast(out), int(kernel), float(kernel_param), int(approximation), int(compute_type),
+                       float(theta), int(degree), int(max_source_leaf), int(max_target_leaf), float(size_check),
+                       ctypes.byref(opts), ctypes.byref(rep))
+    _check(rc)
+    return rep.as_dict()
+
+
+def measure_peaks(device=0):
+    """(fp64 TFLOP/s, fp32 TFLOP/s, rsqrt Gop/s) measured by the library's probes."""
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _check(lib().bt_measure_peaks(int(device), ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+    return a.value, b.value, c.value
 
 
 def direct(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0, device=0):

@@ -207,6 +207,16 @@ std::vector<int2> make_items(int units, const int *count_of_unit, int chunk, con
     return out;
 }
 
+// Algorithmic FLOPs per pointwise interaction (FMA = 2): Coulomb 10
+// (3 sub, 5 for r^2, 2 for the charge multiply-add; the reciprocal square
+// root is a special-function op and not counted), regularized Coulomb 11,
+// Yukawa 13 (+ kappa*r and the exp multiply); Hermite PC/CP 30.
+double flops_per_eval(const bt_params &o, bool approx_side)
+{
+    if (approx_side && o.approx == HERMITE) return 30.0;
+    return o.kernel == COULOMB ? 10.0 : o.kernel == YUKAWA ? 13.0 : 11.0;
+}
+
 void count_interactions(const bt_plan &pl, bt_report *r)
 {
     // pointwise counts as src/drivers/treedriver.c:185-202, 467-483, 757-793
@@ -239,6 +249,9 @@ void count_interactions(const bt_plan &pl, bt_report *r)
             r->num_cc += pl.ap.off[i + 1] - pl.ap.off[i];
         }
     }
+    // FLOPs of the particle-output evaluation kernel (PP + PC)
+    long long pp = r->pp_ptwise, pc = (o.ctype == CLUSTER_PARTICLE) ? 0 : r->pc_ptwise;
+    r->eval_flops = (long long)(pp * flops_per_eval(o, false) + pc * flops_per_eval(o, true));
 }
 
 // Build the host plan: copies, trees, lists.
@@ -253,7 +266,7 @@ void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty,
 }
 
 // Device evaluation of a built plan; writes potentials in caller order to out_host.
-int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out_host, bt_report *rep)
+int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_report *rep)
 {
     const bt_params &o = pl.prm;
     const int n = o.degree, np1 = n + 1, P = o.P;
@@ -308,6 +321,8 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out_host, bt_report *rep)
     int64_t *d_aoff, *d_doff, *d_ccoff, *d_cpoff;
     int *d_aidx, *d_didx, *d_ccidx, *d_cpidx;
     int2 *d_evitems, *d_griditems, *d_l2pitems;
+    int *d_order;
+    double *d_out;
     Layout L;
     L.add(&d_sx, ns); L.add(&d_sy, ns); L.add(&d_sz, ns); L.add(&d_sq, ns);
     L.add(&d_tx, nt); L.add(&d_ty, nt); L.add(&d_tz, nt); L.add(&d_pot, nt);
@@ -324,6 +339,7 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out_host, bt_report *rep)
     L.add(&d_ccoff, pl.g_cc.rows + 1); L.add(&d_ccidx, pl.g_cc.off[pl.g_cc.rows]);
     L.add(&d_cpoff, pl.g_cp.rows + 1); L.add(&d_cpidx, pl.g_cp.off[pl.g_cp.rows]);
     L.add(&d_evitems, ev_items.size()); L.add(&d_griditems, grid_items.size()); L.add(&d_l2pitems, l2p_items.size());
+    L.add(&d_order, nt); L.add(&d_out, nt);
 
     if (!ctx->arena.reserve(L.total())) {
         set_err("device allocation of %zu bytes failed", L.total());
@@ -353,6 +369,7 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out_host, bt_report *rep)
         UP(d_evitems, ev_items.data(), ev_items.size());
         UP(d_griditems, grid_items.data(), grid_items.size());
         UP(d_l2pitems, l2p_items.data(), l2p_items.size());
+        UP(d_order, pl.tgt.order, nt);
 #undef UP
         cudaEvent_t *ev = ctx->ev;
         CK(cudaEventRecord(ev[0], st));
@@ -415,10 +432,12 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out_host, bt_report *rep)
         }
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev[4], st));
-        std::vector<double> pot(nt > 0 ? nt : 1);
-        if (nt > 0) CK(cudaMemcpyAsync(pot.data(), d_pot, sizeof(double) * nt, cudaMemcpyDeviceToHost, st));
+        bt::launch_scatter(nt, d_order, d_pot, out_on_device ? out : d_out, st);
+        launches++;
+        CK(cudaGetLastError());
+        if (!out_on_device && nt > 0)
+            CK(cudaMemcpyAsync(out, d_out, sizeof(double) * nt, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        for (int i = 0; i < nt; i++) out_host[pl.tgt.order[i]] = pot[i];
         g_launches += launches;
         if (rep) {
             float a = 0, b = 0, c = 0, d = 0;
@@ -449,9 +468,14 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
     g_err[0] = 0;
     int rc = validate(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, prm);
     if (rc != BT_OK) return rc;
-    if (nt > 0) memset(out, 0, sizeof(double) * (size_t)nt);
+    const bool out_dev = opts && opts->inputs_on_device;
+    if (nt > 0 && !out_dev) memset(out, 0, sizeof(double) * (size_t)nt);
     if (rep) memset(rep, 0, sizeof(*rep));
-    if (nt == 0 || ns == 0) return BT_OK;
+    if (nt == 0) return BT_OK;
+    if (ns == 0) {
+        if (out_dev && cudaMemset(out, 0, sizeof(double) * (size_t)nt) != cudaSuccess) { set_err("cudaMemset failed"); return BT_ERR_CUDA; }
+        return BT_OK;
+    }
     int device = opts ? opts->device : 0;
     if (opts && opts->precision != BT_PRECISION_FP64) { set_err("mixed precision not provided yet"); return BT_ERR_UNSUPPORTED; }
     DeviceCtx *ctx = nullptr;
@@ -459,6 +483,27 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
     if (rc != BT_OK) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
     double t0 = now_ms();
+    const bool on_dev = opts && opts->inputs_on_device;
+    std::vector<double> hbuf;
+    if (on_dev) {
+        // Device-resident inputs: the host builds the tree, so bring the
+        // coordinates over once.
+        hbuf.resize((size_t)3 * nt + 4 * (size_t)ns);
+        const double *src[7] = {tx, ty, tz, sx, sy, sz, sq};
+        size_t cnt[7] = {(size_t)nt, (size_t)nt, (size_t)nt, (size_t)ns, (size_t)ns, (size_t)ns, (size_t)ns};
+        double *dst = hbuf.data();
+        const double *hp[7];
+        for (int k = 0; k < 7; k++) {
+            if (cudaMemcpyAsync(dst, src[k], sizeof(double) * cnt[k], cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) {
+                set_err("copy of device inputs failed");
+                return BT_ERR_CUDA;
+            }
+            hp[k] = dst;
+            dst += cnt[k];
+        }
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { set_err("copy of device inputs failed"); return BT_ERR_CUDA; }
+        tx = hp[0]; ty = hp[1]; tz = hp[2]; sx = hp[3]; sy = hp[4]; sz = hp[5]; sq = hp[6];
+    }
     bt_plan pl;
     memset(&pl, 0, sizeof pl);
     pl.prm = prm;
@@ -469,9 +514,9 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         rep->ms_total = t1 - t0;
         count_interactions(pl, rep);
     }
-    rc = run_plan(ctx, pl, out, rep);
+    rc = run_plan(ctx, pl, out, on_dev, rep);
     bt_plan_free(&pl);
-    if (rc != BT_OK) memset(out, 0, sizeof(double) * (size_t)nt);
+    if (rc != BT_OK && !on_dev) memset(out, 0, sizeof(double) * (size_t)nt);
     return rc;
 }
 
@@ -572,6 +617,28 @@ int bt_direct(int numTargets, int numSources, const double *targetX, const doubl
     }
 done:
     return rc;
+}
+
+int bt_measure_peaks(int device, double *fp64_tflops, double *fp32_tflops, double *rsqrt_gops)
+{
+    DeviceCtx *ctx = nullptr;
+    int rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { set_err("device query failed"); return BT_ERR_CUDA; }
+    int sms = prop.multiProcessorCount;
+    if (!ctx->arena.reserve((size_t)sms * 8 * 256 * sizeof(double))) { set_err("device allocation failed"); return BT_ERR_CUDA; }
+    double ops;
+    float ms = bt::run_probe(0, sms, &ops, ctx->arena.base, ctx->stream);
+    if (fp64_tflops) *fp64_tflops = 2.0 * ops / (ms * 1e-3) / 1e12;
+    ms = bt::run_probe(1, sms, &ops, ctx->arena.base, ctx->stream);
+    if (fp32_tflops) *fp32_tflops = 2.0 * ops / (ms * 1e-3) / 1e12;
+    ms = bt::run_probe(2, sms, &ops, ctx->arena.base, ctx->stream);
+    if (rsqrt_gops) *rsqrt_gops = ops / (ms * 1e-3) / 1e9;
+    g_launches += 6;
+    if (cudaGetLastError() != cudaSuccess) { set_err("probe launch failed"); return BT_ERR_CUDA; }
+    return BT_OK;
 }
 
 long bt_lists(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,

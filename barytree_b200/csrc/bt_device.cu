@@ -569,6 +569,75 @@ k_direct(int nt, int ns, const double *__restrict__ tx, const double *__restrict
     if (active) out[t] = acc;
 }
 
+// Output in the caller's order (Particles_Targets_Reorder, src/particles/particles.c:58-94).
+__global__ void k_scatter(int n, const int *__restrict__ order, const double *__restrict__ src, double *__restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[order[i]] = src[i];
+}
+
+// Throughput probes: independent FMA chains per thread (8 in flight), and a
+// reciprocal-square-root stream.  The results are written so nothing is dead.
+template <typename R>
+__global__ void k_fma_probe(int iters, R seed, R *out)
+{
+    R a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = seed + (R)(threadIdx.x + k);
+    const R b = (R)0.9999999, c = (R)1e-7;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = a[k] * b + c;
+    }
+    R s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    if (s == (R)-1) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+__global__ void k_rsqrt_probe(int iters, float seed, float *out)
+{
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = seed + (float)(threadIdx.x + k);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = rsqrtf(a[k]);
+    }
+    float s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    if (s == -1.f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+void launch_scatter(int n, const int *order, const double *src, double *dst, cudaStream_t st)
+{
+    if (n > 0) k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, order, src, dst);
+}
+
+// Returns device milliseconds of one probe launch; ops = launched FMA/rsqrt count.
+float run_probe(int which, int sms, double *ops, void *scratch, cudaStream_t st)
+{
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    for (int rep = 0; rep < 2; rep++) {
+        cudaEventRecord(a, st);
+        if (which == 0) k_fma_probe<double><<<blocks, threads, 0, st>>>(iters, 1.0, (double *)scratch);
+        else if (which == 1) k_fma_probe<float><<<blocks, threads, 0, st>>>(iters, 1.0f, (float *)scratch);
+        else k_rsqrt_probe<<<blocks, threads, 0, st>>>(iters, 2.0f, (float *)scratch);
+        cudaEventRecord(b, st);
+    }
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ops = (double)blocks * threads * iters * 8;
+    return ms;
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------

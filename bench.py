@@ -1,0 +1,326 @@
+"""Benchmark of the treecode evaluation on B200 (one JSON line on rank 0).
+
+A step is one complete treecode evaluation (tree, lists, upward pass,
+interaction kernels, downward pass, reorder) of one synthetic system of the
+chosen configuration.
+
+  value  -- targets/s with the inputs resident in HBM when the timed region
+            starts (bt_eval with device pointers)
+  e2e    -- targets/s through the C ABI with pinned host buffers, host->device
+            copies of the inputs and the device->host read of the potentials
+            inside the timed region
+  roofline -- the dominant kernel (particle-output evaluation, PC + PP):
+            algorithmic FLOPs / its CUDA-event time against the SIMT FMA peak
+            measured on this GPU by the library's probes
+  cpu_baseline -- the reference BaryTree (built from its own sources) on a
+            bounded sample of the workload on the host cores
+
+Multi-GPU (--gpus N under torchrun): every rank evaluates its own independent
+system of the configuration (weak scaling, no data-path collective); the
+timing is the max over ranks.
+
+`--impl reference` times the reference's CPU implementation on this host's
+cores instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    1: dict(workload="N=100,000 uniform [-1,1]^3, charges U[-1,1], Coulomb, particle-cluster Lagrange n=8, "
+                     "theta 0.7, leaf 2000", N=100_000, dist="uniform", kernel=1, kp=0.0, approx=1, ctype=1,
+            degree=8, theta=0.7, leaf=2000, sc=1.0, sample_n=60_000),
+    2: dict(workload="N=1,000,000 uniform [-1,1]^3, charges U[-1,1], Yukawa kappa=0.5, cluster-cluster "
+                     "Lagrange n=8, theta 0.8, leaf 2000", N=1_000_000, dist="uniform", kernel=2, kp=0.5, approx=1,
+            ctype=3, degree=8, theta=0.8, leaf=2000, sc=1.0, sample_n=60_000),
+    3: dict(workload="N=4,000,000 Gaussian sigma 0.25 clipped to [-1,1]^3, charges +-1, Coulomb, particle-cluster "
+                     "Hermite n=6, theta 0.7, leaf 1000, size check 4", N=4_000_000, dist="gauss", kernel=1, kp=0.0,
+            approx=2, ctype=1, degree=6, theta=0.7, leaf=1000, sc=4.0, sample_n=60_000),
+}
+
+
+def make_inputs(cfg, seed):
+    """Seeded synthetic inputs with the configuration's distribution (numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    n = cfg["N"] if "n_override" not in cfg else cfg["n_override"]
+    if cfg["dist"] == "uniform":
+        x, y, z = (rng.uniform(-1, 1, n) for _ in range(3))
+        q = rng.uniform(-1, 1, n)
+    elif cfg["dist"] == "gauss":
+        x, y, z = (np.clip(rng.normal(0, 0.25, n), -1, 1) for _ in range(3))
+        q = rng.choice([-1.0, 1.0], n)
+    else:
+        raise ValueError(cfg["dist"])
+    return x, y, z, q
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [c.strip() for c in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_sample_worker(args):
+    """One bounded sample of the workload through the reference CPU build."""
+    cfg, seed, n = args
+    from oracle import oracle as O
+    c = dict(cfg)
+    c["n_override"] = n
+    x, y, z, q = make_inputs(c, seed)
+    t0 = time.perf_counter()
+    O.ref_treecode(x.copy(), y.copy(), z.copy(), None, x, y, z, q, None, c["kernel"], [c["kp"]], 1, c["approx"],
+                   c["ctype"], c["theta"], c["degree"], c["leaf"], c["leaf"], c["sc"], -1.0, 0)
+    return n, time.perf_counter() - t0
+
+
+def cpu_baseline(cfg, cores=1):
+    """The reference (oracle/_ref) on `cores` independent samples, one core each."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    n = cfg["sample_n"]
+    if cores == 1:
+        done, secs = reference_sample_worker((cfg, 1000, n))
+        value = done / secs
+    else:
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        t0 = time.perf_counter()
+        with ctx.Pool(cores) as pool:
+            res = pool.map(reference_sample_worker, [(cfg, 1000 + i, n) for i in range(cores)])
+        secs = time.perf_counter() - t0
+        value = sum(r[0] for r in res) / secs
+    return {"value": value, "unit": "targets/s", "cores": cores, "kind": "reference",
+            "sample": f"reference BaryTree CPU build (gcc -O3, serial) on {cores} independent system(s) of "
+                      f"N={n} with this configuration's distribution and parameters; {secs:.1f} s wall"}
+
+
+def traffic_from_profiles(config_id):
+    """DRAM bytes per launch of the evaluation kernel, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"eval_targets_config{config_id}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def run_reference_arm(args, cfg, rank, world):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(cfg, cores)
+    for _ in range(args.steps):
+        b = cpu_baseline(cfg, cores)
+        if b is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
+            return
+        vals.append(b["value"])
+    v = statistics.mean(vals)
+    line = {"metric": "targets/s", "value": v, "unit": "targets/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "config_id": args.config},
+            "cpu_baseline": {"value": v, "unit": "targets/s", "cores": cores, "kind": "reference",
+                             "sample": b["sample"]},
+            "e2e": {"value": v, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=2, choices=sorted(CONFIGS))
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, cfg, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    import barytree_b200 as B
+    B.lib()
+
+    dev = torch.device("cuda", local)
+    x, y, z, q = make_inputs(cfg, seed=rank)
+    n = len(x)
+    prec = B.PRECISION_MIXED if args.precision == "mixed" else B.PRECISION_FP64
+    common = dict(kernel=cfg["kernel"], kernel_param=cfg["kp"], approximation=cfg["approx"],
+                  compute_type=cfg["ctype"], theta=cfg["theta"], degree=cfg["degree"], max_source_leaf=cfg["leaf"],
+                  max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=local)
+
+    # device-resident inputs (targets are separate arrays with the same coordinates)
+    d_in = [torch.from_numpy(a).to(dev) for a in (x, y, z, x.copy(), y.copy(), z.copy(), q)]
+    d_out = torch.empty(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)     # > L2 (126 MB)
+
+    def step_device():
+        return B.treecode_ptr(n, n, *(t.data_ptr() for t in d_in[3:6]), *(t.data_ptr() for t in d_in[:3]),
+                              d_in[6].data_ptr(), d_out.data_ptr(), inputs_on_device=True, **common)
+
+    # pinned host buffers for the end-to-end path
+    h_in = [torch.from_numpy(a.copy()).pin_memory() for a in (x, y, z, x, y, z, q)]
+    h_out = torch.empty(n, dtype=torch.float64).pin_memory()
+
+    def step_host():
+        return B.treecode_ptr(n, n, *(t.data_ptr() for t in h_in[3:6]), *(t.data_ptr() for t in h_in[:3]),
+                              h_in[6].data_ptr(), h_out.data_ptr(), inputs_on_device=False, **common)
+
+    def timed(step, k):
+        """K steps, each bracketed by CUDA events on the current stream; L2 flushed between steps."""
+        total, reps = 0.0, []
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            reps.append(step())
+            e1.record()
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+        return total, reps
+
+    for _ in range(args.warmup):
+        step_device()
+        step_host()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = B.kernel_launch_count()
+    ms_dev, reps = timed(step_device, args.steps)
+    launches = B.kernel_launch_count() - launches0
+    clock_info = clocks.stop()
+    torch.cuda.synchronize()
+    ms_e2e, _ = timed(step_host, args.steps)
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([ms_dev, ms_e2e], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_dev, ms_e2e = float(t[0]), float(t[1])
+
+    # accuracy of the last step vs the FP64 direct sum on 10,000 strided targets (outside timing)
+    idx = np.arange(0, n, max(1, n // 10000))
+    d = B.direct(x[idx], y[idx], z[idx], x, y, z, q, cfg["kernel"], cfg["kp"], device=local)
+    pot = d_out.cpu().numpy()[idx]
+    rel_l2 = float(np.linalg.norm(pot - d) / np.linalg.norm(d))
+    rel_max = float(np.max(np.abs(pot - d)) / np.max(np.abs(d)))
+
+    if rank == 0:
+        fp64_peak, fp32_peak, rsqrt_rate = B.measure_peaks(local)
+        rep = reps[-1]
+        ev_ms = statistics.mean(r["ms_eval_kernel"] for r in reps)
+        achieved = rep["eval_flops"] / (ev_ms * 1e-3) / 1e12 if ev_ms > 0 else None
+        peak = fp64_peak if prec == B.PRECISION_FP64 else fp32_peak
+        value = world * n / (ms_dev / args.steps * 1e-3)
+        e2e = world * n / (ms_e2e / args.steps * 1e-3)
+        line = {
+            "metric": "targets/s", "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == B.PRECISION_FP64 else "f32+f64",
+            "data": "synthetic (seeded numpy PCG64 with the configuration's distribution)",
+            "config": {"workload": cfg["workload"], "config_id": args.config, "precision": args.precision,
+                       "degree_policy": "fixed", "l2": "flushed between steps (256 MB write)",
+                       "parallelism": f"{world} independent system(s), one per GPU",
+                       "rel_l2_vs_fp64_direct": rel_l2, "rel_max_vs_fp64_direct": rel_max,
+                       "direct_sample_targets": len(idx)},
+            "e2e": {"value": e2e, "unit": "targets/s", "h2d_bytes_per_step": 7 * 8 * n,
+                    "d2h_bytes_per_step": 8 * n, "ms_per_step": ms_e2e / args.steps},
+            "roofline": {"bound": "fp64-simt" if prec == B.PRECISION_FP64 else "fp32-simt",
+                         "kernel": "k_eval_targets (PC + PP)", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if achieved else None,
+                         "peak_source": "measured by bt_measure_peaks on this GPU (FMA=2 FLOP)",
+                         "traffic": traffic_from_profiles(args.config),
+                         "flops_per_launch": rep["eval_flops"], "ms_per_launch": ev_ms,
+                         "rsqrt_gops_measured": rsqrt_rate},
+            "phases_ms": {k: rep[k] for k in ("ms_setup", "ms_upward", "ms_compute", "ms_downward", "ms_transfer")},
+            "interactions": {k: rep[k] for k in ("pp_ptwise", "pc_ptwise", "cp_ptwise", "cc_ptwise")},
+            "clocks": clock_info,
+            "gpu_launches": launches,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(cfg, 1)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

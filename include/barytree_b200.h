@@ -137,6 +137,12 @@ long bt_lists(int numTargets, int numSources,
 int bt_tree_dump(int n, const double *x, const double *y, const double *z, int maxparnode,
             int *ints, double *dbl, int cap);
 
+/* Throughput microbenchmarks on `device` (the roofline denominators of the
+ * SIMT evaluation kernels): dependent-FMA streams in FP64 and FP32 and a
+ * reciprocal-square-root stream, each over all SMs.  Results in TFLOP/s
+ * (FMA = 2 FLOP) and Gop/s. */
+int bt_measure_peaks(int device, double *fp64_tflops, double *fp32_tflops, double *rsqrt_gops);
+
 /* Last error message of the calling thread ("" if none). */
 const char *bt_last_error(void);
 
