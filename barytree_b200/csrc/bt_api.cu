@@ -23,6 +23,7 @@
 
 #include "../../include/barytree_b200.h"
 #include "bt_device.h"
+#include "bt_mixed.h"
 #include "bt_host.h"
 
 namespace {
@@ -254,6 +255,38 @@ void count_interactions(const bt_plan &pl, bt_report *r)
     r->eval_flops = (long long)(pp * flops_per_eval(o, false) + pc * flops_per_eval(o, true));
 }
 
+// For every node: the range of its leaves in the tree's DFS leaf order (the
+// leaves under a node are contiguous there because numbering is pre-order).
+void leaf_ranges(const bt_tree &t, std::vector<int> &first, std::vector<int> &count)
+{
+    first.assign(t.n, 0);
+    count.assign(t.n, 0);
+    std::vector<int> pos(t.n, -1);
+    for (int i = 0; i < t.nleaves; i++) pos[t.leaves[i]] = i;
+    for (int v = t.n - 1; v >= 0; v--) {
+        if (t.nchild[v] == 0) { first[v] = pos[v]; count[v] = 1; continue; }
+        first[v] = first[t.child[8 * v]];
+        int c = 0;
+        for (int k = 0; k < t.nchild[v]; k++) c += count[t.child[8 * v + k]];
+        count[v] = c;
+    }
+}
+
+// Replace every node entry of a CSR by the leaves under it, in DFS order.
+void expand_to_leaves(const bt_csr &in, const bt_tree &t, const std::vector<int> &first,
+                      const std::vector<int> &count, std::vector<int64_t> &off, std::vector<int> &idx)
+{
+    off.assign(in.rows + 1, 0);
+    idx.clear();
+    for (int r = 0; r < in.rows; r++) {
+        for (int64_t k = in.off[r]; k < in.off[r + 1]; k++) {
+            int s = in.idx[k];
+            for (int l = 0; l < count[s]; l++) idx.push_back(t.leaves[first[s] + l]);
+        }
+        off[r + 1] = (int64_t)idx.size();
+    }
+}
+
 // Build the host plan: copies, trees, lists.
 void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty, const double *tz,
                 const double *sx, const double *sy, const double *sz, const double *sq)
@@ -311,7 +344,22 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
         std::vector<double> lcost(T.nleaves, 1.0);
         l2p_items = make_items(T.nleaves, leaf_count.data(), 128, lcost);
     }
-    std::vector<int> s_nleafpar;
+    // mixed precision: Lagrange only (Hermite evaluates in FP64); node
+    // centres and leaf-expanded near-field / CP lists
+    const bool mixed = o.precision == BT_PRECISION_MIXED && !herm;
+    std::vector<double> sctr, tctr;
+    std::vector<int64_t> mx_doff, mx_cpoff;
+    std::vector<int> mx_didx, mx_cpidx;
+    if (mixed) {
+        sctr.resize(3 * (size_t)S.n);
+        tctr.resize(3 * (size_t)T.n);
+        for (int i = 0; i < S.n; i++) { sctr[3 * i] = S.xm[i]; sctr[3 * i + 1] = S.ym[i]; sctr[3 * i + 2] = S.zm[i]; }
+        for (int i = 0; i < T.n; i++) { tctr[3 * i] = T.xm[i]; tctr[3 * i + 1] = T.ym[i]; tctr[3 * i + 2] = T.zm[i]; }
+        std::vector<int> lf, lc;
+        leaf_ranges(S, lf, lc);
+        expand_to_leaves(pl.t_direct, S, lf, lc, mx_doff, mx_didx);
+        expand_to_leaves(pl.g_cp, S, lf, lc, mx_cpoff, mx_cpidx);
+    }
 
     // device layout
     double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx, *d_ty, *d_tz, *d_pot, *d_sgrid, *d_tgrid, *d_slen, *d_tlen, *d_ww;
@@ -340,6 +388,18 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
     L.add(&d_cpoff, pl.g_cp.rows + 1); L.add(&d_cpidx, pl.g_cp.off[pl.g_cp.rows]);
     L.add(&d_evitems, ev_items.size()); L.add(&d_griditems, grid_items.size()); L.add(&d_l2pitems, l2p_items.size());
     L.add(&d_order, nt); L.add(&d_out, nt);
+    float4 *d_spos = nullptr, *d_tpos = nullptr;
+    float *d_Q32 = nullptr;
+    double *d_sctr = nullptr, *d_tctr = nullptr;
+    int64_t *d_mxdoff = nullptr, *d_mxcpoff = nullptr;
+    int *d_mxdidx = nullptr, *d_mxcpidx = nullptr;
+    if (mixed) {
+        L.add(&d_spos, ns); L.add(&d_tpos, nt);
+        if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P);
+        L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
+        L.add(&d_mxdoff, mx_doff.size()); L.add(&d_mxdidx, mx_didx.size());
+        L.add(&d_mxcpoff, mx_cpoff.size()); L.add(&d_mxcpidx, mx_cpidx.size());
+    }
 
     if (!ctx->arena.reserve(L.total())) {
         set_err("device allocation of %zu bytes failed", L.total());
@@ -370,8 +430,18 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
         UP(d_griditems, grid_items.data(), grid_items.size());
         UP(d_l2pitems, l2p_items.data(), l2p_items.size());
         UP(d_order, pl.tgt.order, nt);
+        if (mixed) {
+            UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
+            UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
+            UP(d_mxcpoff, mx_cpoff.data(), mx_cpoff.size()); UP(d_mxcpidx, mx_cpidx.data(), mx_cpidx.size());
+        }
 #undef UP
         cudaEvent_t *ev = ctx->ev;
+        if (mixed) {
+            bt::launch_rel_positions(S.nleaves, d_sleaves, d_sibeg, d_snum, d_sctr, d_sx, d_sy, d_sz, d_sq, d_spos, st);
+            bt::launch_rel_positions(T.nleaves, d_tleaves, d_tibeg, d_tnum, d_tctr, d_tx, d_ty, d_tz, nullptr, d_tpos, st);
+            launches += 2;
+        }
         CK(cudaEventRecord(ev[0], st));
         // upward pass
         if (need_src_clusters && ns > 0) {
@@ -387,11 +457,23 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
                     }
                 }
             }
+            if (mixed) {
+                bt::launch_to_f32((size_t)S.n * P, d_Q, d_Q32, st);
+                launches++;
+            }
         }
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev[1], st));
         // grid-output evaluation (CP, M2L) and L2L
-        if (need_tgt_grids && nt > 0) {
+        if (need_tgt_grids && nt > 0 && mixed) {
+            bt::MixedGridsArgs g;
+            g.n = n; g.nitems = (int)grid_items.size(); g.items = d_griditems; g.t_grid = d_tgrid; g.t_ctr = d_tctr;
+            g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_mxcpoff; g.p_idx = d_mxcpidx;
+            g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.s_ctr = d_sctr; g.Q32 = d_Q32;
+            g.spos = d_spos; g.kp = o.kp; g.Phi = d_Phi;
+            bt::launch_eval_grids_mixed(o.kernel, g, st);
+            launches++;
+        } else if (need_tgt_grids && nt > 0) {
             bt::EvalGridsArgs g;
             g.n = n; g.nitems = (int)grid_items.size(); g.items = d_griditems; g.t_grid = d_tgrid;
             g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_cpoff; g.p_idx = d_cpidx;
@@ -403,7 +485,18 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev[2], st));
         // particle-output evaluation (PC, PP)
-        if (nt > 0) {
+        if (nt > 0 && mixed) {
+            bt::MixedTargetsArgs a;
+            memset(&a, 0, sizeof a);
+            a.n = n; a.max_np1 = n + 1; a.nitems = (int)ev_items.size(); a.items = d_evitems;
+            a.leaf_node = d_tleaves; a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.t_ctr = d_tctr; a.tpos = d_tpos;
+            a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = nullptr;
+            a.s_grid[n] = d_sgrid; a.Q32[n] = d_Q32;
+            a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
+            a.spos = d_spos; a.kp = o.kp; a.pot = d_pot;
+            bt::launch_eval_targets_mixed(o.kernel, a, st);
+            launches++;
+        } else if (nt > 0) {
             bt::EvalTargetsArgs a;
             a.n = n; a.nitems = (int)ev_items.size(); a.items = d_evitems; a.leaf_node = d_tleaves;
             a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.a_off = d_aoff; a.a_idx = d_aidx; a.d_off = d_doff; a.d_idx = d_didx;
@@ -477,7 +570,11 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         return BT_OK;
     }
     int device = opts ? opts->device : 0;
-    if (opts && opts->precision != BT_PRECISION_FP64) { set_err("mixed precision not provided yet"); return BT_ERR_UNSUPPORTED; }
+    if (opts && opts->precision != BT_PRECISION_FP64 && opts->precision != BT_PRECISION_MIXED) {
+        set_err("invalid precision %d", opts->precision);
+        return BT_ERR_PARAM;
+    }
+    prm.precision = opts ? opts->precision : BT_PRECISION_FP64;
     DeviceCtx *ctx = nullptr;
     rc = get_ctx(device, &ctx);
     if (rc != BT_OK) return rc;

@@ -45,6 +45,7 @@ typedef struct {
     int kernel, approx, sing, ctype, degree, P, maxs, maxt;
     double theta, size_check, kp, beta;
     int verbosity;
+    int precision;          /* 0 = FP64, 1 = mixed (FP32 evaluations, FP64 reductions) */
 } bt_params;
 
 /* Everything the device side needs for one evaluation. */

@@ -1,0 +1,50 @@
+// bt_mixed.h -- launchers of the mixed-precision kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace bt {
+
+constexpr int MX_MAX_DEG = 12;
+
+struct MixedTargetsArgs {
+    int n, max_np1, nitems;
+    const int2 *items;
+    const int *leaf_node, *t_ibeg, *t_numpar;
+    const double *t_ctr;                        // target node centres (FP64, 3 per node)
+    const float4 *tpos;                         // targets relative to their leaf centre
+    const int64_t *a_off; const int *a_idx;     // source clusters per target leaf
+    const unsigned char *a_deg;                 // per-entry degree (nullptr: all n)
+    const double *s_grid[MX_MAX_DEG + 1];       // per degree: node grids (FP64)
+    const float *Q32[MX_MAX_DEG + 1];           // per degree: proxy charges (FP32)
+    const int64_t *d_off; const int *d_idx;     // source leaves per target leaf
+    const int *s_ibeg, *s_numpar;
+    const double *s_ctr;                        // source node centres
+    const float4 *spos;                         // sources relative to their leaf centre, with charge
+    double kp;
+    double *pot;
+};
+
+struct MixedGridsArgs {
+    int n, nitems;
+    const int2 *items;
+    const double *t_grid, *t_ctr;
+    const int64_t *c_off; const int *c_idx;     // M2L source clusters per target node
+    const int64_t *p_off; const int *p_idx;     // CP source leaves per target node
+    const int *s_ibeg, *s_numpar;
+    const double *s_grid, *s_ctr;
+    const float *Q32;
+    const float4 *spos;
+    double kp;
+    double *Phi;
+};
+
+void launch_rel_positions(int nleaves, const int *leaves, const int *ibeg, const int *numpar, const double *ctr,
+                          const double *x, const double *y, const double *z, const double *q, float4 *out,
+                          cudaStream_t st);
+void launch_to_f32(size_t n, const double *src, float *dst, cudaStream_t st);
+void launch_eval_targets_mixed(int kernel, const MixedTargetsArgs &a, cudaStream_t st);
+void launch_eval_grids_mixed(int kernel, const MixedGridsArgs &a, cudaStream_t st);
+
+}  // namespace bt

@@ -1,0 +1,68 @@
+"""GPU accuracy of the mixed-precision path.
+
+Mixed precision evaluates PP/PC/CP/M2L in FP32 on centre-relative
+coordinates with FP64 reductions.  Bar: relative L2 difference from the FP64
+treecode <= 2e-7 (FP32 rounding of centre-relative displacements and of the
+proxy charges), and relative L2 error against the FP64 direct sum within the
+1e-6 tolerance at degree 8.
+"""
+import numpy as np
+import pytest
+
+import barytree_b200 as B
+from conftest import uniform_inputs
+
+pytestmark = pytest.mark.gpu
+
+TOL_VS_FP64_TREE = 2e-7
+TOL_VS_DIRECT = 1e-6
+
+
+def _run(args, precision):
+    tx, ty, tz, sx, sy, sz, sq, kernel, kp, ctype, degree, leaf = args
+    return B.treecode(tx, ty, tz, sx, sy, sz, sq, kernel=kernel, kernel_param=kp, compute_type=ctype, theta=0.7,
+                      degree=degree, max_source_leaf=leaf, max_target_leaf=leaf, precision=precision)
+
+
+@pytest.mark.parametrize("ctype", [1, 2, 3])
+@pytest.mark.parametrize("kernel,kp", [(1, 0.0), (2, 0.5), (3, 1e-3)])
+def test_mixed_matches_fp64_tree(ctype, kernel, kp):
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(31 + kernel, 30000, targets="other")
+    args = (tx, ty, tz, sx, sy, sz, sq, kernel, kp, ctype, 6, 400)
+    a = _run(args, B.PRECISION_MIXED)
+    b = _run(args, B.PRECISION_FP64)
+    err = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert err <= TOL_VS_FP64_TREE, err
+
+
+@pytest.mark.parametrize("ctype", [1, 3])
+def test_mixed_vs_direct_degree8(ctype):
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(2, 60000)
+    pot = _run((tx, ty, tz, sx, sy, sz, sq, 1, 0.0, ctype, 8, 1000), B.PRECISION_MIXED)
+    idx = np.arange(0, len(tx), 7)
+    d = B.direct(tx[idx], ty[idx], tz[idx], sx, sy, sz, sq)
+    assert np.linalg.norm(pot[idx] - d) / np.linalg.norm(d) <= TOL_VS_DIRECT
+
+
+def test_mixed_hermite_runs_in_fp64():
+    """Hermite has no FP32 kernels: the mixed option evaluates it with the FP64 kernels."""
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(4, 8000)
+    a = B.treecode(tx, ty, tz, sx, sy, sz, sq, approximation=2, degree=4, max_source_leaf=200,
+                   max_target_leaf=200, size_check=4.0, precision=B.PRECISION_MIXED)
+    b = B.treecode(tx, ty, tz, sx, sy, sz, sq, approximation=2, degree=4, max_source_leaf=200,
+                   max_target_leaf=200, size_check=4.0, precision=B.PRECISION_FP64)
+    assert np.array_equal(a, b)
+
+
+def test_mixed_coincident_points():
+    """Targets equal to sources, and every source duplicated: coincident
+    pairs must be skipped (r^2 == 0), as in the FP64 path."""
+    rng = np.random.default_rng(9)
+    x, y, z = (np.repeat(rng.uniform(-1, 1, 10000), 2) for _ in range(3))
+    q = rng.uniform(-1, 1, 20000)
+    a = B.treecode(x, y, z, x, y, z, q, degree=6, max_source_leaf=300, max_target_leaf=300,
+                   precision=B.PRECISION_MIXED)
+    b = B.treecode(x, y, z, x, y, z, q, degree=6, max_source_leaf=300, max_target_leaf=300,
+                   precision=B.PRECISION_FP64)
+    assert np.all(np.isfinite(a))
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-6
