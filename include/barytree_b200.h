@@ -13,6 +13,12 @@
 extern "C" {
 #endif
 
+/* The library is built with hidden visibility; only what this header
+ * declares is exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 /* Enum values are fixed by the reference's public header
  * (src/interface/BaryTreeInterface.h:7-48), so existing callers and their
  * ctypes/Fortran bindings pass the same integers. */
@@ -148,6 +154,10 @@ const char *bt_last_error(void);
 
 /* Number of CUDA kernels this library launched in this process (for checks). */
 long long bt_kernel_launch_count(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }
