@@ -50,9 +50,11 @@ double now_ms()
 struct Arena {
     char *base = nullptr;
     size_t cap = 0, used = 0;
+    bool fixed = false;     // wraps caller-provided memory: never grows, never frees
     bool reserve(size_t bytes)
     {
         if (bytes <= cap) return true;
+        if (fixed) return false;
         if (base) cudaFree(base);
         base = nullptr;
         cap = 0;
@@ -299,7 +301,7 @@ void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty,
 }
 
 // Device evaluation of a built plan; writes potentials in caller order to out_host.
-int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_report *rep)
+int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on_device, bt_report *rep)
 {
     const bt_params &o = pl.prm;
     const int n = o.degree, np1 = n + 1, P = o.P;
@@ -330,7 +332,9 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
         for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) c += S.numpar[pl.t_direct.idx[k]];
         leaf_cost[u] = c;
     }
-    std::vector<int2> ev_items = make_items(T.nleaves, leaf_count.data(), 128, leaf_cost);
+    const bool mixed = o.precision == BT_PRECISION_MIXED && !herm;
+    std::vector<int2> ev_items =
+        make_items(T.nleaves, leaf_count.data(), mixed ? bt::mixed_targets_chunk() : 128, leaf_cost);
     std::vector<int2> grid_items, l2p_items;
     if (need_tgt_grids) {
         std::vector<int> pcount(T.n, P);
@@ -345,11 +349,13 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
         l2p_items = make_items(T.nleaves, leaf_count.data(), 128, lcost);
     }
     // mixed precision: Lagrange only (Hermite evaluates in FP64); node
-    // centres and leaf-expanded near-field / CP lists
-    const bool mixed = o.precision == BT_PRECISION_MIXED && !herm;
+    // centres, leaf-expanded near-field / CP lists, and per near-field entry
+    // whether the two leaves' boxes overlap (only then can a target coincide
+    // with a source, so only then is the skipping test evaluated)
     std::vector<double> sctr, tctr;
     std::vector<int64_t> mx_doff, mx_cpoff;
     std::vector<int> mx_didx, mx_cpidx;
+    std::vector<unsigned char> mx_dflag;
     if (mixed) {
         sctr.resize(3 * (size_t)S.n);
         tctr.resize(3 * (size_t)T.n);
@@ -359,6 +365,16 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
         leaf_ranges(S, lf, lc);
         expand_to_leaves(pl.t_direct, S, lf, lc, mx_doff, mx_didx);
         expand_to_leaves(pl.g_cp, S, lf, lc, mx_cpoff, mx_cpidx);
+        mx_dflag.resize(mx_didx.size());
+        for (int u = 0; u < T.nleaves; u++) {
+            int t = T.leaves[u];
+            for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) {
+                int s = mx_didx[k];
+                bool ov = T.x0[t] <= S.x1[s] && S.x0[s] <= T.x1[t] && T.y0[t] <= S.y1[s] && S.y0[s] <= T.y1[t] &&
+                          T.z0[t] <= S.z1[s] && S.z0[s] <= T.z1[t];
+                mx_dflag[k] = ov ? 1 : 0;
+            }
+        }
     }
 
     // device layout
@@ -393,19 +409,24 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
     double *d_sctr = nullptr, *d_tctr = nullptr;
     int64_t *d_mxdoff = nullptr, *d_mxcpoff = nullptr;
     int *d_mxdidx = nullptr, *d_mxcpidx = nullptr;
+    unsigned char *d_mxdflag = nullptr;
     if (mixed) {
         L.add(&d_spos, ns); L.add(&d_tpos, nt);
         if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P);
         L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
-        L.add(&d_mxdoff, mx_doff.size()); L.add(&d_mxdidx, mx_didx.size());
+        L.add(&d_mxdoff, mx_doff.size()); L.add(&d_mxdidx, mx_didx.size()); L.add(&d_mxdflag, mx_dflag.size());
         L.add(&d_mxcpoff, mx_cpoff.size()); L.add(&d_mxcpidx, mx_cpidx.size());
     }
 
-    if (!ctx->arena.reserve(L.total())) {
+    if (!arena.reserve(L.total())) {
+        if (arena.fixed) {
+            set_err("this call needs %zu bytes of device scratch; the static scratch holds %zu", L.total(), arena.cap);
+            return BT_ERR_PARAM;
+        }
         set_err("device allocation of %zu bytes failed", L.total());
         return BT_ERR_CUDA;
     }
-    L.bind(ctx->arena);
+    L.bind(arena);
 
     double t_setup = now_ms();
     {
@@ -433,6 +454,7 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
         if (mixed) {
             UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
+            UP(d_mxdflag, mx_dflag.data(), mx_dflag.size());
             UP(d_mxcpoff, mx_cpoff.data(), mx_cpoff.size()); UP(d_mxcpidx, mx_cpidx.data(), mx_cpidx.size());
         }
 #undef UP
@@ -470,7 +492,7 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
             g.n = n; g.nitems = (int)grid_items.size(); g.items = d_griditems; g.t_grid = d_tgrid; g.t_ctr = d_tctr;
             g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_mxcpoff; g.p_idx = d_mxcpidx;
             g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.s_ctr = d_sctr; g.Q32 = d_Q32;
-            g.spos = d_spos; g.kp = o.kp; g.Phi = d_Phi;
+            g.spos = d_spos; g.kc = bt::mixed_kernel_constant(o.kernel, o.kp); g.Phi = d_Phi;
             bt::launch_eval_grids_mixed(o.kernel, g, st);
             launches++;
         } else if (need_tgt_grids && nt > 0) {
@@ -492,8 +514,8 @@ int run_plan(DeviceCtx *ctx, bt_plan &pl, double *out, bool out_on_device, bt_re
             a.leaf_node = d_tleaves; a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.t_ctr = d_tctr; a.tpos = d_tpos;
             a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = nullptr;
             a.s_grid[n] = d_sgrid; a.Q32[n] = d_Q32;
-            a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
-            a.spos = d_spos; a.kp = o.kp; a.pot = d_pot;
+            a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.d_flag = d_mxdflag; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
+            a.spos = d_spos; a.kc = bt::mixed_kernel_constant(o.kernel, o.kp); a.pot = d_pot;
             bt::launch_eval_targets_mixed(o.kernel, a, st);
             launches++;
         } else if (nt > 0) {
@@ -579,6 +601,7 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
     rc = get_ctx(device, &ctx);
     if (rc != BT_OK) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    Arena *arena = &ctx->arena;
     double t0 = now_ms();
     const bool on_dev = opts && opts->inputs_on_device;
     std::vector<double> hbuf;
@@ -611,7 +634,7 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         rep->ms_total = t1 - t0;
         count_interactions(pl, rep);
     }
-    rc = run_plan(ctx, pl, out, on_dev, rep);
+    rc = run_plan(ctx, *arena, pl, out, on_dev, rep);
     bt_plan_free(&pl);
     if (rc != BT_OK && !on_dev) memset(out, 0, sizeof(double) * (size_t)nt);
     return rc;

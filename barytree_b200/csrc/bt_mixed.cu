@@ -5,13 +5,18 @@
 // ever sees displacements of the size of the interaction, never absolute
 // positions.  Centre offsets between the two sides of an interaction are
 // formed in FP64 and rounded once.  Per-interaction partial sums are FP32
-// (far field: Kahan-compensated); they are folded into an FP64 per-target
-// accumulator after every list entry / tile, which is the FP64 far+near
-// reduction.  Tree boxes, Chebyshev node placement, exact-node coincidence
-// tests and the barycentric passes stay FP64 (bt_device.cu).
+// (far field: Kahan-compensated per grid row); they are folded into an FP64
+// per-target accumulator after every list entry / tile, which is the FP64
+// far+near reduction.  Tree boxes, Chebyshev node placement, exact-node
+// coincidence tests and the barycentric passes stay FP64 (bt_device.cu).
 //
-// The far-field loops are instantiated per degree (NP1 = n+1, template) so
-// the target-relative grid coordinates of one axis live in registers.
+// Throughput: the kernels are issue-bound, so each thread evaluates two
+// targets against every shared-memory value it loads, the coincidence test
+// of the skipping kernels runs only for source leaves whose box overlaps the
+// target leaf's box, and the special functions are single MUFU instructions
+// (rsqrt.approx / ex2.approx, flush-to-zero).  The far-field loops are
+// instantiated per degree (NP1 = n+1) so one axis of grid coordinates lives
+// in registers.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -21,28 +26,49 @@
 
 namespace bt {
 
+__device__ __forceinline__ float rsqrt_apx(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float ex2_apx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Kernel value for a well-separated pair.  kc: Yukawa -kappa*log2(e);
+// regularised Coulomb eps^2; unused for Coulomb.
 template <int KT>
-__device__ __forceinline__ float kf_far(float r2, float q, float kp)
+__device__ __forceinline__ float kf_far(float r2, float q, float kc)
 {
     if (KT == 1) {
-        return q * rsqrtf(r2);
+        return q * rsqrt_apx(r2);
     } else if (KT == 2) {
-        float rinv = rsqrtf(r2);
-        float r = r2 * rinv;
-        return q * rinv * __expf(-kp * r);
+        // one Newton step on 1/r (the MUFU estimate's error would otherwise
+        // enter both 1/r and the exponent); the FMA pipe has room for it here
+        float rinv = rsqrt_apx(r2);
+        float h = r2 * rinv;
+        float t = fmaf(-0.5f * h, rinv, 1.5f);
+        float e = ex2_apx(kc * (h * t));
+        return (q * (rinv * t)) * e;
     } else {
-        return q * rsqrtf(r2 + kp * kp);
+        return q * rsqrt_apx(r2 + kc);
     }
 }
 
-// PP: the reference skips r^2 <= DBL_MIN (Coulomb) / r <= DBL_MIN (Yukawa);
-// in FP32 the coincident pair gives r2 == 0 exactly.
-template <int KT>
-__device__ __forceinline__ float kf_pp(float r2, float q, float kp)
+// Near-field pair with the reference's skipping rule (r^2 <= DBL_MIN for
+// Coulomb, r <= DBL_MIN for Yukawa; the regularised kernel never skips).  In
+// FP32 a coincident pair gives r2 == 0 exactly.
+template <int KT, bool SKIP>
+__device__ __forceinline__ float kf_pp(float r2, float q, float kc)
 {
-    if (KT == 3) return q * rsqrtf(r2 + kp * kp);
-    float v = kf_far<KT>(r2, q, kp);
-    return r2 > 0.0f ? v : 0.0f;
+    float v = kf_far<KT>(r2, q, kc);
+    if (SKIP && KT != 3) v = r2 > 0.0f ? v : 0.0f;
+    return v;
 }
 
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
@@ -54,47 +80,83 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
 }
 
 constexpr int MX_THREADS = 128;
+constexpr int MX_TPT = 2;                       // targets per thread
+constexpr int MX_CHUNK = MX_THREADS * MX_TPT;   // targets per work item
 constexpr int MX_TILE = 1024;
 
-// Far field of one source cluster at degree NP1-1 for one target at
-// (x,y,z) relative to the target centre; g = grid coordinates relative to the
-// same centre (FP32, smem), q = proxy charges (FP32, smem).
-template <int KT, int NP1>
-__device__ __forceinline__ float pc_cluster(float x, float y, float z, const float *g, const float *q, float kp)
+// Far field of one source cluster (degree NP1-1) for NT targets at (x,y,z),
+// relative to the target centre; g = grid coordinates relative to the same
+// centre, q = proxy charges (shared memory, FP32).
+template <int KT, int NP1, int NT>
+__device__ __forceinline__ void pc_cluster(const float *x, const float *y, const float *z, const float *g,
+                                           const float *q, float kc, float *out)
 {
-    float gx[NP1];
+    float gx[NT][NP1];
 #pragma unroll
-    for (int k = 0; k < NP1; k++) gx[k] = x - g[k];
-    float s = 0.f, c = 0.f;
+    for (int t = 0; t < NT; t++)
+#pragma unroll
+        for (int k = 0; k < NP1; k++) gx[t][k] = x[t] - g[k];
+    float s[NT], c[NT];
+#pragma unroll
+    for (int t = 0; t < NT; t++) { s[t] = 0.f; c[t] = 0.f; }
     int j = 0;
     for (int k3 = 0; k3 < NP1; k3++) {
-        float dz = z - g[2 * NP1 + k3];
+        float gz = g[2 * NP1 + k3];
         for (int k2 = 0; k2 < NP1; k2++) {
-            float dy = y - g[NP1 + k2];
-            float dyz = fmaf(dy, dy, dz * dz);
-            float row = 0.f;
+            float gy = g[NP1 + k2];
+            float dyz[NT], row[NT];
 #pragma unroll
-            for (int k1 = 0; k1 < NP1; k1++) row += kf_far<KT>(fmaf(gx[k1], gx[k1], dyz), q[j + k1], kp);
+            for (int t = 0; t < NT; t++) {
+                float dy = y[t] - gy, dz = z[t] - gz;
+                dyz[t] = fmaf(dy, dy, dz * dz);
+                row[t] = 0.f;
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < NP1; k1++) {
+                float qq = q[j + k1];
+#pragma unroll
+                for (int t = 0; t < NT; t++) row[t] += kf_far<KT>(fmaf(gx[t][k1], gx[t][k1], dyz[t]), qq, kc);
+            }
             j += NP1;
-            kahan_add(s, c, row);
+#pragma unroll
+            for (int t = 0; t < NT; t++) kahan_add(s[t], c[t], row[t]);
         }
     }
-    return s - c;
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = s[t] - c[t];
 }
 
-template <int KT>
-__device__ float pc_cluster_dispatch(int np1, float x, float y, float z, const float *g, const float *q, float kp)
+template <int KT, int NT>
+__device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, const float *z, const float *g,
+                                    const float *q, float kc, float *out)
 {
     switch (np1) {
-#define BT_CASE(N) case N: return pc_cluster<KT, N>(x, y, z, g, q, kp);
+#define BT_CASE(N) case N: pc_cluster<KT, N, NT>(x, y, z, g, q, kc, out); return;
         BT_CASE(2) BT_CASE(3) BT_CASE(4) BT_CASE(5) BT_CASE(6) BT_CASE(7) BT_CASE(8)
         BT_CASE(9) BT_CASE(10) BT_CASE(11) BT_CASE(12) BT_CASE(13)
 #undef BT_CASE
     }
-    return 0.f;
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = 0.f;
 }
 
-// Particle-output evaluation, mixed precision.  One thread per target.
+template <int KT, bool SKIP>
+__device__ __forceinline__ void pp_tile(const float4 *tile, int cm, const float *x, const float *y, const float *z,
+                                        float kc, float *s)
+{
+#pragma unroll 4
+    for (int i = 0; i < cm; i++) {
+        float4 p = tile[i];
+#pragma unroll
+        for (int t = 0; t < MX_TPT; t++) {
+            float dx = x[t] - p.x, dy = y[t] - p.y, dz = z[t] - p.z;
+            s[t] += kf_pp<KT, SKIP>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), p.w, kc);
+        }
+    }
+}
+
+// Particle-output evaluation, mixed precision.  Each thread owns MX_TPT
+// targets of a work item (target leaf, chunk of MX_CHUNK targets).
 template <int KT>
 __global__ void __launch_bounds__(MX_THREADS)
 k_eval_targets_mixed(MixedTargetsArgs a)
@@ -104,15 +166,24 @@ k_eval_targets_mixed(MixedTargetsArgs a)
     const int u = it.x;
     const int tnode = a.leaf_node[u];
     const int tb = a.t_ibeg[tnode], tn = a.t_numpar[tnode];
-    const int ti = it.y * MX_THREADS + threadIdx.x;
-    const bool active = ti < tn;
-    const int t = tb + (active ? ti : 0);
-    const float4 tp = a.tpos[t];
+    float x[MX_TPT], y[MX_TPT], z[MX_TPT];
+    bool act[MX_TPT];
+    int tid[MX_TPT];
+#pragma unroll
+    for (int t = 0; t < MX_TPT; t++) {
+        int ti = it.y * MX_CHUNK + t * MX_THREADS + threadIdx.x;
+        act[t] = ti < tn;
+        tid[t] = tb + (act[t] ? ti : 0);
+        float4 tp = a.tpos[tid[t]];
+        x[t] = tp.x; y[t] = tp.y; z[t] = tp.z;
+    }
     const double cx = a.t_ctr[3 * tnode], cy = a.t_ctr[3 * tnode + 1], cz = a.t_ctr[3 * tnode + 2];
-    const float kp = (float)a.kp;
-    double acc = 0.0;
+    const float kc = (float)a.kc;
+    double acc[MX_TPT];
+#pragma unroll
+    for (int t = 0; t < MX_TPT; t++) acc[t] = 0.0;
 
-    // far field
+    // far field: source clusters
     for (int64_t e = a.a_off[u]; e < a.a_off[u + 1]; e++) {
         const int s = a.a_idx[e];
         const int deg = a.a_deg ? a.a_deg[e] : a.n;
@@ -128,46 +199,45 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         }
         for (int i = threadIdx.x; i < P; i += blockDim.x) q[i] = Qs[i];
         __syncthreads();
-        if (active) acc += (double)pc_cluster_dispatch<KT>(np1, tp.x, tp.y, tp.z, g, q, kp);
+        float v[MX_TPT];
+        pc_cluster_dispatch<KT, MX_TPT>(np1, x, y, z, g, q, kc, v);
+#pragma unroll
+        for (int t = 0; t < MX_TPT; t++) acc[t] += (double)v[t];
         __syncthreads();
     }
     // near field: source leaves, particles relative to their leaf centre
     float4 *tile = reinterpret_cast<float4 *>(smf);
     for (int64_t e = a.d_off[u]; e < a.d_off[u + 1]; e++) {
         const int s = a.d_idx[e];
+        const bool skip = a.d_flag[e] != 0;
         const int sb = a.s_ibeg[s], sn = a.s_numpar[s];
         const float ox = (float)(a.s_ctr[3 * s] - cx), oy = (float)(a.s_ctr[3 * s + 1] - cy),
                     oz = (float)(a.s_ctr[3 * s + 2] - cz);
-        const float x = tp.x - ox, y = tp.y - oy, z = tp.z - oz;   // target in the source leaf's frame
+        float xs[MX_TPT], ys[MX_TPT], zs[MX_TPT];   // targets in the source leaf's frame
+#pragma unroll
+        for (int t = 0; t < MX_TPT; t++) { xs[t] = x[t] - ox; ys[t] = y[t] - oy; zs[t] = z[t] - oz; }
         for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
             int cm = min(MX_TILE, sn - c0);
             for (int i = threadIdx.x; i < cm; i += blockDim.x) tile[i] = a.spos[sb + c0 + i];
             __syncthreads();
-            if (active) {
-                float s0 = 0.f, s1 = 0.f;
-                int i = 0;
-                for (; i + 1 < cm; i += 2) {
-                    float4 p = tile[i], p1 = tile[i + 1];
-                    float dx = x - p.x, dy = y - p.y, dz = z - p.z;
-                    float dx1 = x - p1.x, dy1 = y - p1.y, dz1 = z - p1.z;
-                    s0 += kf_pp<KT>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), p.w, kp);
-                    s1 += kf_pp<KT>(fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1)), p1.w, kp);
-                }
-                if (i < cm) {
-                    float4 p = tile[i];
-                    float dx = x - p.x, dy = y - p.y, dz = z - p.z;
-                    s0 += kf_pp<KT>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), p.w, kp);
-                }
-                acc += (double)s0 + (double)s1;
-            }
+            float sum[MX_TPT];
+#pragma unroll
+            for (int t = 0; t < MX_TPT; t++) sum[t] = 0.f;
+            if (skip) pp_tile<KT, true>(tile, cm, xs, ys, zs, kc, sum);
+            else pp_tile<KT, false>(tile, cm, xs, ys, zs, kc, sum);
+#pragma unroll
+            for (int t = 0; t < MX_TPT; t++) acc[t] += (double)sum[t];
             __syncthreads();
         }
     }
-    if (active) a.pot[t] = acc;
+#pragma unroll
+    for (int t = 0; t < MX_TPT; t++)
+        if (act[t]) a.pot[tid[t]] = acc[t];
 }
 
 // Grid-output evaluation (M2L from source clusters + CP from source leaves)
-// onto the grid of a target node, mixed precision, Lagrange.
+// onto the grid of a target node, mixed precision, Lagrange.  One thread per
+// target grid point.
 template <int KT>
 __global__ void __launch_bounds__(MX_THREADS)
 k_eval_grids_mixed(MixedGridsArgs a)
@@ -181,9 +251,9 @@ k_eval_grids_mixed(MixedGridsArgs a)
     const int jj = active ? j0 : 0;
     const double *tg = a.t_grid + (size_t)T * 3 * np1;
     const double cx = a.t_ctr[3 * T], cy = a.t_ctr[3 * T + 1], cz = a.t_ctr[3 * T + 2];
-    const float x = (float)(tg[jj % np1] - cx), y = (float)(tg[np1 + (jj / np1) % np1] - cy),
-                z = (float)(tg[2 * np1 + jj / (np1 * np1)] - cz);
-    const float kp = (float)a.kp;
+    float x[1] = {(float)(tg[jj % np1] - cx)}, y[1] = {(float)(tg[np1 + (jj / np1) % np1] - cy)},
+          z[1] = {(float)(tg[2 * np1 + jj / (np1 * np1)] - cz)};
+    const float kc = (float)a.kc;
     double acc = 0.0;
     for (int64_t e = a.c_off[T]; e < a.c_off[T + 1]; e++) {
         const int s = a.c_idx[e];
@@ -197,7 +267,9 @@ k_eval_grids_mixed(MixedGridsArgs a)
         }
         for (int i = threadIdx.x; i < P; i += blockDim.x) q[i] = a.Q32[(size_t)s * P + i];
         __syncthreads();
-        if (active) acc += (double)pc_cluster_dispatch<KT>(np1, x, y, z, g, q, kp);
+        float v[1];
+        pc_cluster_dispatch<KT, 1>(np1, x, y, z, g, q, kc, v);
+        acc += (double)v[0];
         __syncthreads();
     }
     float4 *tile = reinterpret_cast<float4 *>(smf);
@@ -206,20 +278,19 @@ k_eval_grids_mixed(MixedGridsArgs a)
         const int sb = a.s_ibeg[s], sn = a.s_numpar[s];
         const float ox = (float)(a.s_ctr[3 * s] - cx), oy = (float)(a.s_ctr[3 * s + 1] - cy),
                     oz = (float)(a.s_ctr[3 * s + 2] - cz);
-        const float xs = x - ox, ys = y - oy, zs = z - oz;
+        const float xs = x[0] - ox, ys = y[0] - oy, zs = z[0] - oz;
         for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
             int cm = min(MX_TILE, sn - c0);
             for (int i = threadIdx.x; i < cm; i += blockDim.x) tile[i] = a.spos[sb + c0 + i];
             __syncthreads();
-            if (active) {
-                float s0 = 0.f;
-                for (int i = 0; i < cm; i++) {
-                    float4 p = tile[i];
-                    float dx = xs - p.x, dy = ys - p.y, dz = zs - p.z;
-                    s0 += kf_far<KT>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), p.w, kp);
-                }
-                acc += (double)s0;
+            float s0 = 0.f;
+#pragma unroll 4
+            for (int i = 0; i < cm; i++) {
+                float4 p = tile[i];
+                float dx = xs - p.x, dy = ys - p.y, dz = zs - p.z;
+                s0 += kf_far<KT>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), p.w, kc);
             }
+            acc += (double)s0;
             __syncthreads();
         }
     }
@@ -255,6 +326,8 @@ void launch_to_f32(size_t n, const double *src, float *dst, cudaStream_t st)
 {
     if (n > 0) k_to_f32<<<1184, 256, 0, st>>>(n, src, dst);
 }
+
+int mixed_targets_chunk() { return MX_CHUNK; }
 
 static size_t mixed_smem(int max_np1)
 {
@@ -293,6 +366,13 @@ void launch_eval_grids_mixed(int kernel, const MixedGridsArgs &a, cudaStream_t s
     if (kernel == 1) eval_grids_mixed_t<1>(a, st);
     else if (kernel == 2) eval_grids_mixed_t<2>(a, st);
     else eval_grids_mixed_t<3>(a, st);
+}
+
+double mixed_kernel_constant(int kernel, double kp)
+{
+    if (kernel == 2) return -kp * 1.4426950408889634;   // exp(-k r) = 2^(-k log2(e) r)
+    if (kernel == 3) return kp * kp;
+    return 0.0;
 }
 
 }  // namespace bt

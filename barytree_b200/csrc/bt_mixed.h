@@ -19,10 +19,11 @@ struct MixedTargetsArgs {
     const double *s_grid[MX_MAX_DEG + 1];       // per degree: node grids (FP64)
     const float *Q32[MX_MAX_DEG + 1];           // per degree: proxy charges (FP32)
     const int64_t *d_off; const int *d_idx;     // source leaves per target leaf
+    const unsigned char *d_flag;                // 1: boxes overlap, apply the coincidence skip
     const int *s_ibeg, *s_numpar;
     const double *s_ctr;                        // source node centres
     const float4 *spos;                         // sources relative to their leaf centre, with charge
-    double kp;
+    double kc;                                  // mixed_kernel_constant()
     double *pot;
 };
 
@@ -36,7 +37,7 @@ struct MixedGridsArgs {
     const double *s_grid, *s_ctr;
     const float *Q32;
     const float4 *spos;
-    double kp;
+    double kc;                                  // mixed_kernel_constant()
     double *Phi;
 };
 
@@ -46,5 +47,7 @@ void launch_rel_positions(int nleaves, const int *leaves, const int *ibeg, const
 void launch_to_f32(size_t n, const double *src, float *dst, cudaStream_t st);
 void launch_eval_targets_mixed(int kernel, const MixedTargetsArgs &a, cudaStream_t st);
 void launch_eval_grids_mixed(int kernel, const MixedGridsArgs &a, cudaStream_t st);
+int mixed_targets_chunk();                                   // targets per work item
+double mixed_kernel_constant(int kernel, double kernel_param);
 
 }  // namespace bt
