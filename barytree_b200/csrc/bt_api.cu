@@ -576,9 +576,43 @@ done:
     return rc;
 }
 
+// ---------------------------------------------------------------------------
+// Static device scratch of the allocation-free entry point bt_eval_noalloc.
+// In host code the symbol is only a host-side stand-in: its device address is
+// looked up once per device (cudaGetSymbolAddress with that device current)
+// and only that address is handed to kernels.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BT_NOALLOC_SCRATCH_BYTES];
+
+struct StaticScratch {
+    bool ready = false;
+    Arena arena;
+};
+StaticScratch g_static_scratch[16];
+
+// Called with `device` current and its context lock held.
+int static_scratch_arena(int device, Arena **out)
+{
+    StaticScratch &s = g_static_scratch[device];
+    if (!s.ready) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || ptr == nullptr) {
+            set_err("cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+            return BT_ERR_CUDA;
+        }
+        s.arena.base = (char *)ptr;
+        s.arena.cap = BT_NOALLOC_SCRATCH_BYTES;
+        s.arena.fixed = true;
+        s.ready = true;
+    }
+    *out = &s.arena;
+    return BT_OK;
+}
+
 int eval_common(int nt, int ns, const double *tx, const double *ty, const double *tz, const double *sx,
                 const double *sy, const double *sz, const double *sq, double *out, bt_params &prm,
-                const bt_options *opts, bt_report *rep)
+                const bt_options *opts, bt_report *rep, bool use_static_scratch = false)
 {
     g_err[0] = 0;
     int rc = validate(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, prm);
@@ -602,6 +636,10 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
     if (rc != BT_OK) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
     Arena *arena = &ctx->arena;
+    if (use_static_scratch) {
+        rc = static_scratch_arena(device, &arena);
+        if (rc != BT_OK) return rc;
+    }
     double t0 = now_ms();
     const bool on_dev = opts && opts->inputs_on_device;
     std::vector<double> hbuf;
@@ -696,6 +734,24 @@ int bt_eval(int numTargets, int numSources, const double *targetX, const double 
                     maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
     return eval_common(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
                        outputArray, prm, opts, report);
+}
+
+int bt_eval_noalloc(int numTargets, int numSources, const double *targetX, const double *targetY,
+                    const double *targetZ, const double *sourceX, const double *sourceY, const double *sourceZ,
+                    const double *sourceValue, double *outputArray, int kernel, double kernelParam,
+                    int approximation, int compute_type, double theta, int interpOrder, int maxPerSourceLeaf,
+                    int maxPerTargetLeaf, double sizeCheck, int precision, int device)
+{
+    bt_params prm;
+    bt_params_setup(&prm, kernel, 1, &kernelParam, SKIPPING, approximation, compute_type, theta, interpOrder,
+                    maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
+    bt_options opts;
+    memset(&opts, 0, sizeof opts);
+    opts.precision = precision;
+    opts.device = device;
+    opts.inputs_on_device = 1;
+    return eval_common(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+                       outputArray, prm, &opts, nullptr, true);
 }
 
 int bt_direct(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,

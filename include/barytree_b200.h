@@ -116,6 +116,41 @@ int bt_eval(int numTargets, int numSources,
             double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
             double sizeCheck, const bt_options *opts, bt_report *report);
 
+/* Allocation-free evaluation (no counterpart in the reference).
+ *
+ * For callers that must not allocate device memory at call time: code
+ * running inside a memory pool or arena that owns the whole device, code
+ * whose allocations must be known before it starts (real-time or
+ * certification settings), and callers that run while another component has
+ * reserved all free memory.  This entry point calls no cudaMalloc, cudaFree
+ * or allocating library routine.  All of its device scratch (sorted particle
+ * copies, tree arrays, interaction lists, proxy charges, grid potentials)
+ * lives in one file-scope static device array of BT_NOALLOC_SCRATCH_BYTES,
+ * which every GPU that loads the library holds until the process exits.
+ *
+ * Arguments are those of bt_eval, except that all seven input arrays and
+ * outputArray are DEVICE pointers (FP64) on `device`, and precision is a
+ * BT_PRECISION_* value.  The result equals bt_eval with inputs_on_device.
+ * A call whose scratch need exceeds the static array returns BT_ERR_PARAM
+ * with a message giving both sizes (roughly up to 5e5 particles at degree 8).
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress with that device current); make that first call
+ * before any stream capture.  Every call on a device shares the one array
+ * and leaves the previous call's contents in it; all kernels write their
+ * scratch before reading it, so nothing needs to start at zero.  Calls
+ * through this library are serialised per device by a lock; work that the
+ * caller launches itself and that overlaps a call on the GPU must not touch
+ * the array (it is private to the library), and two calls that overlapped on
+ * the GPU would race on it. */
+#define BT_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int bt_eval_noalloc(int numTargets, int numSources,
+                    const double *targetX, const double *targetY, const double *targetZ,
+                    const double *sourceX, const double *sourceY, const double *sourceZ,
+                    const double *sourceValue, double *outputArray,
+                    int kernel, double kernelParam, int approximation, int compute_type,
+                    double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+                    double sizeCheck, int precision, int device);
+
 /* FP64 direct sum on the GPU (the error reference for large N):
  * out[i] = sum_j q_j K(t_i, s_j) with the reference's skipping rules
  * (src/interaction_compute/interaction_compute_direct.c:26-231). */
