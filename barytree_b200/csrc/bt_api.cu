@@ -294,9 +294,20 @@ void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty,
                 const double *sx, const double *sy, const double *sz, const double *sq)
 {
     bt_parts_init(&pl.src, ns, sx, sy, sz, sq);
-    bt_parts_init(&pl.tgt, nt, tx, ty, tz, nullptr);
     bt_tree_build(&pl.st, &pl.src, pl.prm.maxs);
-    bt_tree_build(&pl.tt, &pl.tgt, pl.prm.maxt);
+    // Targets at exactly the source positions with the same leaf size give
+    // the same node sets (the build depends only on coordinates and leaf
+    // size), so the target tree and permutation are copies of the source's.
+    bool same = nt == ns && pl.prm.maxs == pl.prm.maxt && (tx == sx || !memcmp(tx, sx, sizeof(double) * nt)) &&
+                (ty == sy || !memcmp(ty, sy, sizeof(double) * nt)) && (tz == sz || !memcmp(tz, sz, sizeof(double) * nt));
+    if (same && nt > 0) {
+        bt_parts_init(&pl.tgt, nt, pl.src.x, pl.src.y, pl.src.z, nullptr);
+        memcpy(pl.tgt.order, pl.src.order, sizeof(int) * (size_t)nt);
+        bt_tree_copy(&pl.tt, &pl.st);
+    } else {
+        bt_parts_init(&pl.tgt, nt, tx, ty, tz, nullptr);
+        bt_tree_build(&pl.tt, &pl.tgt, pl.prm.maxt);
+    }
     bt_plan_lists(&pl);
 }
 

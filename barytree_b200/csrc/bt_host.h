@@ -75,6 +75,7 @@ void bt_parts_init(bt_parts *p, int n, const double *x, const double *y, const d
 void bt_parts_free(bt_parts *p);
 void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode);
 void bt_tree_free(bt_tree *t);
+void bt_tree_copy(bt_tree *dst, const bt_tree *src);
 
 /* bt_lists.c */
 void bt_csr_free(bt_csr *c);

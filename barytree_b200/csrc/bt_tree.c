@@ -15,6 +15,7 @@
  * ind[] order, so node indices equal the reference's.
  */
 #include <math.h>
+#include <omp.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -136,19 +137,30 @@ static void divide_axes(double xl, double yl, double zl, int max_nc, int div[3])
     div[0] = dx; div[1] = dy; div[2] = dz;
 }
 
-static int build_node(bt_tree *t, build_ctx *c, int b, int np, int level, int parent)
+/* One node of the level-synchronous build.  Nodes are created level by
+ * level (breadth first) and renumbered to the reference's pre-order at the
+ * end, so the build can split every node of a level concurrently. */
+typedef struct {
+    int ibeg, np, level, parent, nchild, child[8];
+    int kid_b[8], kid_n[8];
+    double box[6];                  /* x0, x1, y0, y1, z0, z1 */
+} bnode;
+
+/* Nodes at least this large are split with parallel loops; smaller nodes of
+ * a level are split concurrently, one thread per node. */
+#define BT_PAR_NODE 65536
+
+static void split_node(bnode *nd, build_ctx *c, int par)
 {
     bt_parts *p = c->p;
-    tree_grow(t);
-    int idx = t->n++;
-    t->ibeg[idx] = b; t->numpar[idx] = np; t->level[idx] = level; t->parent[idx] = parent;
-    t->nchild[idx] = 0;
-    if (level + 1 > t->max_depth) t->max_depth = level + 1;
+    const int b = nd->ibeg, np = nd->np;
+    const double *xs = p->x + b, *ys = p->y + b, *zs = p->z + b;
+    nd->nchild = 0;
 
     /* bounding box of the node's particles (tree_linked_list.c:188-206) */
-    const double *xs = p->x + b, *ys = p->y + b, *zs = p->z + b;
     double x0 = xs[0], x1 = xs[0], y0 = ys[0], y1 = ys[0], z0 = zs[0], z1 = zs[0];
-    for (int i = 1; i < np; i++) {
+#pragma omp parallel for if (par) reduction(min : x0, y0, z0) reduction(max : x1, y1, z1)
+    for (int i = 0; i < np; i++) {
         if (x0 > xs[i]) x0 = xs[i];
         if (x1 < xs[i]) x1 = xs[i];
         if (y0 > ys[i]) y0 = ys[i];
@@ -156,14 +168,11 @@ static int build_node(bt_tree *t, build_ctx *c, int b, int np, int level, int pa
         if (z0 > zs[i]) z0 = zs[i];
         if (z1 < zs[i]) z1 = zs[i];
     }
+    nd->box[0] = x0; nd->box[1] = x1; nd->box[2] = y0; nd->box[3] = y1; nd->box[4] = z0; nd->box[5] = z1;
+    if (np <= c->maxpar) return;
+
     double xl = x1 - x0, yl = y1 - y0, zl = z1 - z0;
-    t->x0[idx] = x0; t->x1[idx] = x1; t->y0[idx] = y0; t->y1[idx] = y1; t->z0[idx] = z0; t->z1[idx] = z1;
-    double xm = (x1 + x0) / 2.0, ym = (y1 + y0) / 2.0, zm = (z1 + z0) / 2.0;
-    t->xm[idx] = xm; t->ym[idx] = ym; t->zm[idx] = zm;
-    t->rad[idx] = sqrt(xl * xl + yl * yl + zl * zl) / 2.0;
-
-    if (np <= c->maxpar) return idx;
-
+    double mid[3] = {(x1 + x0) / 2.0, (y1 + y0) / 2.0, (z1 + z0) / 2.0};
     int max_nc = (np < 2 * c->maxpar) ? 2 : (np < 4 * c->maxpar) ? 4 : 8;
     int div[3];
     divide_axes(xl, yl, zl, max_nc, div);
@@ -175,31 +184,42 @@ static int build_node(bt_tree *t, build_ctx *c, int b, int np, int level, int pa
      * The k-th divided axis sets bit k of the slot, which is the reference's
      * ind[] position (partition.c:229-282). */
     unsigned char *code = c->code + b;
-    memset(code, 0, (size_t)np);
+#pragma omp parallel for if (par)
+    for (int i = 0; i < np; i++) code[i] = 0;
     int cnt[8] = {np, 0, 0, 0, 0, 0, 0, 0};
     int bit = 0;
     const double *ax[3] = {xs, ys, zs};
-    double mid[3] = {xm, ym, zm};
     for (int a = 0; a < 3; a++) {
         if (!div[a]) continue;
         const double *v = ax[a];
-        double m = mid[a];
-        int newcnt[8] = {0};
+        const double m = mid[a];
+        int nc0 = cnt[0], nc1 = cnt[1], nc2 = cnt[2], nc3 = cnt[3];
+        int pc[4] = {nc0, nc1, nc2, nc3};
+        int newcnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma omp parallel for if (par) reduction(+ : newcnt[:8])
         for (int i = 0; i < np; i++) {
             int part = code[i];
-            int upper = (cnt[part] >= 2) ? !(v[i] <= m) : !(v[i] < m);
-            code[i] = (unsigned char)(part | (upper << bit));
-            newcnt[code[i]]++;
+            int upper = (pc[part] >= 2) ? !(v[i] <= m) : !(v[i] < m);
+            int cd = part | (upper << bit);
+            code[i] = (unsigned char)cd;
+            newcnt[cd]++;
         }
         memcpy(cnt, newcnt, sizeof cnt);
         bit++;
     }
     int nslots = 1 << bit;
+
+    /* A split that leaves every particle in one slot (all particles of an
+     * over-full node at one point) would repeat forever; the reference
+     * recurses without end there.  Keep such a node as a leaf. */
+    for (int s = 0; s < nslots; s++)
+        if (cnt[s] == np) return;
+
     /* Memory layout of the slots: each binary split keeps its lower part
      * first, so the first divided axis is the most significant position key
      * (the slot index with its bits reversed), while children are numbered
      * in slot order.  Same ranges as the reference's ibeg/iend. */
-    int start[8], pos[8];
+    int start[8];
     {
         int off = 0;
         for (int key = 0; key < nslots; key++) {
@@ -209,35 +229,54 @@ static int build_node(bt_tree *t, build_ctx *c, int b, int np, int level, int pa
             off += cnt[s];
         }
     }
-    memcpy(pos, start, sizeof pos);
     double *tx = c->tx + b, *ty = c->ty + b, *tz = c->tz + b, *tq = c->tq + b;
     int *to = c->to + b;
     double *px = p->x + b, *py = p->y + b, *pz = p->z + b, *pq = p->q + b;
     int *po = p->order + b;
-    for (int i = 0; i < np; i++) {
-        int d = pos[code[i]]++;
-        tx[d] = px[i]; ty[d] = py[i]; tz[d] = pz[i]; tq[d] = pq[i]; to[d] = po[i];
+    if (!par) {
+        int pos[8];
+        memcpy(pos, start, sizeof pos);
+        for (int i = 0; i < np; i++) {
+            int d = pos[code[i]]++;
+            tx[d] = px[i]; ty[d] = py[i]; tz[d] = pz[i]; tq[d] = pq[i]; to[d] = po[i];
+        }
+    } else {
+        /* stable parallel counting scatter: every thread scatters its
+         * contiguous chunk behind the chunks of the threads before it */
+        int nth = omp_get_max_threads();
+        int (*tcnt)[8] = calloc((size_t)nth, sizeof(int[8]));
+#pragma omp parallel num_threads(nth)
+        {
+            int t = omp_get_thread_num(), T = omp_get_num_threads();
+            long lo = (long)np * t / T, hi = (long)np * (t + 1) / T;
+            for (long i = lo; i < hi; i++) tcnt[t][code[i]]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                for (int s = 0; s < 8; s++) {
+                    int run = start[s];
+                    for (int u = 0; u < T; u++) { int k = tcnt[u][s]; tcnt[u][s] = run; run += k; }
+                }
+            }
+            int pos[8];
+            memcpy(pos, tcnt[t], sizeof pos);
+            for (long i = lo; i < hi; i++) {
+                int d = pos[code[i]]++;
+                tx[d] = px[i]; ty[d] = py[i]; tz[d] = pz[i]; tq[d] = pq[i]; to[d] = po[i];
+            }
+        }
+        free(tcnt);
     }
-    memcpy(px, tx, sizeof(double) * (size_t)np);
-    memcpy(py, ty, sizeof(double) * (size_t)np);
-    memcpy(pz, tz, sizeof(double) * (size_t)np);
-    memcpy(pq, tq, sizeof(double) * (size_t)np);
-    memcpy(po, to, sizeof(int) * (size_t)np);
-
-    /* A split that leaves every particle in one slot (all particles of an
-     * over-full node at one point) would repeat forever; the reference
-     * recurses without end there.  Keep such a node as a leaf. */
-    for (int s = 0; s < nslots; s++)
-        if (cnt[s] == np) return idx;
-
-    int kids[8], nk = 0;
+#pragma omp parallel for if (par)
+    for (int i = 0; i < np; i++) {
+        px[i] = tx[i]; py[i] = ty[i]; pz[i] = tz[i]; pq[i] = tq[i]; po[i] = to[i];
+    }
     for (int s = 0; s < nslots; s++) {
         if (cnt[s] == 0) continue;             /* empty children are skipped (tree_linked_list.c:266) */
-        kids[nk++] = build_node(t, c, b + start[s], cnt[s], level + 1, idx);
+        nd->kid_b[nd->nchild] = b + start[s];
+        nd->kid_n[nd->nchild] = cnt[s];
+        nd->nchild++;
     }
-    t->nchild[idx] = nk;
-    for (int i = 0; i < nk; i++) t->child[8 * idx + i] = kids[i];
-    return idx;
 }
 
 static void collect(bt_tree *t, int idx, int *nleaf, int *lvl_fill)
@@ -246,6 +285,13 @@ static void collect(bt_tree *t, int idx, int *nleaf, int *lvl_fill)
     int l = t->level[idx];
     t->lvl_nodes[t->lvl_off[l] + lvl_fill[l]++] = idx;
     for (int i = 0; i < t->nchild[idx]; i++) collect(t, t->child[8 * idx + i], nleaf, lvl_fill);
+}
+
+static int preorder(const bnode *nodes, int i, int next, int *pre)
+{
+    pre[i] = next++;
+    for (int k = 0; k < nodes[i].nchild; k++) next = preorder(nodes, nodes[i].child[k], next, pre);
+    return next;
 }
 
 void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
@@ -261,8 +307,60 @@ void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
     c.to = malloc(sizeof(int) * m);
     c.code = malloc(m);
     c.maxpar = maxparnode;
-    build_node(t, &c, 0, p->n, 0, -1);
+
+    int cap = 1024, n = 1;
+    bnode *nodes = malloc(sizeof(bnode) * (size_t)cap);
+    memset(&nodes[0], 0, sizeof(bnode));
+    nodes[0].ibeg = 0; nodes[0].np = p->n; nodes[0].level = 0; nodes[0].parent = -1;
+    int lo = 0, hi = 1, depth = 1;
+    while (lo < hi) {
+        for (int i = lo; i < hi; i++)
+            if (nodes[i].np >= BT_PAR_NODE) split_node(&nodes[i], &c, 1);
+#pragma omp parallel for schedule(dynamic, 2)
+        for (int i = lo; i < hi; i++)
+            if (nodes[i].np < BT_PAR_NODE) split_node(&nodes[i], &c, 0);
+        for (int i = lo; i < hi; i++) {
+            for (int k = 0; k < nodes[i].nchild; k++) {
+                if (n == cap) { cap *= 2; nodes = realloc(nodes, sizeof(bnode) * (size_t)cap); }
+                bnode *ch = &nodes[n];
+                memset(ch, 0, sizeof(bnode));
+                ch->ibeg = nodes[i].kid_b[k]; ch->np = nodes[i].kid_n[k];
+                ch->level = nodes[i].level + 1; ch->parent = i;
+                nodes[i].child[k] = n;
+                if (ch->level + 1 > depth) depth = ch->level + 1;
+                n++;
+            }
+        }
+        lo = hi; hi = n;
+    }
     free(c.tx); free(c.ty); free(c.tz); free(c.tq); free(c.to); free(c.code);
+
+    /* pre-order numbering (TreeLinkedList_SetIndex, src/tree/tree_linked_list.c:284-293) */
+    int *pre = malloc(sizeof(int) * (size_t)n);
+    preorder(nodes, 0, 0, pre);
+    t->cap = 0;
+    t->n = 0;
+    while (t->cap < n) {
+        t->n = t->cap;          /* tree_grow grows when the arrays are full */
+        tree_grow(t);
+    }
+    t->n = n;
+    t->max_depth = depth;
+    for (int i = 0; i < n; i++) {
+        const bnode *nd = &nodes[i];
+        int k = pre[i];
+        t->ibeg[k] = nd->ibeg; t->numpar[k] = nd->np; t->level[k] = nd->level;
+        t->parent[k] = nd->parent >= 0 ? pre[nd->parent] : -1;
+        t->nchild[k] = nd->nchild;
+        for (int j = 0; j < nd->nchild; j++) t->child[8 * k + j] = pre[nd->child[j]];
+        double x0 = nd->box[0], x1 = nd->box[1], y0 = nd->box[2], y1 = nd->box[3], z0 = nd->box[4], z1 = nd->box[5];
+        double xl = x1 - x0, yl = y1 - y0, zl = z1 - z0;
+        t->x0[k] = x0; t->x1[k] = x1; t->y0[k] = y0; t->y1[k] = y1; t->z0[k] = z0; t->z1[k] = z1;
+        t->xm[k] = (x1 + x0) / 2.0; t->ym[k] = (y1 + y0) / 2.0; t->zm[k] = (z1 + z0) / 2.0;
+        t->rad[k] = sqrt(xl * xl + yl * yl + zl * zl) / 2.0;
+    }
+    free(pre);
+    free(nodes);
 
     /* leaves and per-level non-leaf lists, DFS order (src/tree/tree.c:122-153) */
     int nleaf = 0;
@@ -281,6 +379,33 @@ void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
     int nl = 0;
     collect(t, 0, &nl, lvl_cnt);
     free(lvl_cnt);
+}
+
+void bt_tree_copy(bt_tree *dst, const bt_tree *src)
+{
+    memset(dst, 0, sizeof(*dst));
+    dst->max_depth = 1;
+    if (src->n <= 0 || !src->lvl_off) return;
+    int n = src->n;
+    while (dst->cap < n) {
+        dst->n = dst->cap;
+        tree_grow(dst);
+    }
+    dst->n = n;
+    dst->max_depth = src->max_depth;
+    dst->nleaves = src->nleaves;
+#define C(f) memcpy(dst->f, src->f, sizeof(*src->f) * (size_t)n)
+    C(ibeg); C(numpar); C(nchild); C(parent); C(level);
+    C(x0); C(x1); C(y0); C(y1); C(z0); C(z1); C(xm); C(ym); C(zm); C(rad);
+#undef C
+    memcpy(dst->child, src->child, sizeof(int) * 8 * (size_t)n);
+    dst->leaves = malloc(sizeof(int) * (size_t)(src->nleaves > 0 ? src->nleaves : 1));
+    memcpy(dst->leaves, src->leaves, sizeof(int) * (size_t)src->nleaves);
+    dst->lvl_off = malloc(sizeof(int) * (size_t)(src->max_depth + 1));
+    memcpy(dst->lvl_off, src->lvl_off, sizeof(int) * (size_t)(src->max_depth + 1));
+    int nl = src->lvl_off[src->max_depth];
+    dst->lvl_nodes = malloc(sizeof(int) * (size_t)(nl + 1));
+    memcpy(dst->lvl_nodes, src->lvl_nodes, sizeof(int) * (size_t)nl);
 }
 
 void bt_cheb_nodes(int n, double a0, double a1, double *out)
