@@ -102,7 +102,9 @@ _BTI_ARGS = (
 
 # every exported symbol of include/barytree_b200.h
 EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
-                    "bt_tree_dump", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count")
+                    "bt_tree_dump", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
+                    "bt_selector_nweights", "bt_selector_set", "bt_selector_training_data", "bt_selector_train",
+                    "bt_mlp_loss_grad", "bt_mlp_predict")
 
 _lib = None
 
@@ -135,6 +137,21 @@ def lib():
     L.bt_tree_dump.restype = ctypes.c_int
     L.bt_measure_peaks.argtypes = (ctypes.c_int, _dp, _dp, _dp)
     L.bt_measure_peaks.restype = ctypes.c_int
+    _fp = ctypes.POINTER(ctypes.c_float)
+    L.bt_selector_nweights.argtypes = ()
+    L.bt_selector_nweights.restype = ctypes.c_long
+    L.bt_selector_set.argtypes = (_fp, ctypes.c_long)
+    L.bt_selector_set.restype = ctypes.c_int
+    L.bt_selector_training_data.argtypes = (ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_uint, _fp, _fp, ctypes.c_int)
+    L.bt_selector_training_data.restype = ctypes.c_long
+    L.bt_selector_train.argtypes = (_fp, _fp, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                    ctypes.c_uint, _fp, _fp, ctypes.c_int)
+    L.bt_selector_train.restype = ctypes.c_int
+    L.bt_mlp_loss_grad.argtypes = (_fp, _fp, _fp, ctypes.c_int, _fp, _fp, ctypes.c_int)
+    L.bt_mlp_loss_grad.restype = ctypes.c_int
+    L.bt_mlp_predict.argtypes = (_fp, _fp, ctypes.c_long, _fp, ctypes.c_int)
+    L.bt_mlp_predict.restype = ctypes.c_int
     L.bt_last_error.argtypes = ()
     L.bt_last_error.restype = ctypes.c_char_p
     L.bt_kernel_launch_count.argtypes = ()

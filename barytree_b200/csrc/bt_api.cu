@@ -24,6 +24,7 @@
 #include "../../include/barytree_b200.h"
 #include "bt_device.h"
 #include "bt_mixed.h"
+#include "bt_learned.h"
 #include "bt_host.h"
 
 namespace {
@@ -328,6 +329,21 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     std::vector<double> sgrid, slen, tgrid, tlen;
     fill_grids(S, n, sgrid, slen);
     fill_grids(T, n, tgrid, tlen);
+    // further degrees used by a learned per-interaction selection (mixed path)
+    std::vector<int> xdeg;
+    std::vector<std::vector<double>> xgrid;
+    int64_t n_approx = pl.t_approx.off[pl.t_approx.rows];
+    if (pl.a_deg) {
+        bool used[BT_MAX_DEGREE + 1] = {};
+        for (int64_t k = 0; k < n_approx; k++) used[pl.a_deg[k]] = true;
+        for (int d = 1; d <= BT_MAX_DEGREE; d++)
+            if (used[d] && d != n) xdeg.push_back(d);
+        xgrid.resize(xdeg.size());
+        std::vector<double> tmp;
+        for (size_t i = 0; i < xdeg.size(); i++) fill_grids(S, xdeg[i], xgrid[i], tmp);
+    }
+    int max_np1 = n + 1;
+    for (int d : xdeg) max_np1 = std::max(max_np1, d + 1);
     double ww[BT_MAX_DEGREE + 1];
     hermite_ww(n, ww);
 
@@ -339,7 +355,14 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     for (int u = 0; u < T.nleaves; u++) {
         leaf_count[u] = T.numpar[T.leaves[u]];
         double c = 0;
-        c += (double)(pl.t_approx.off[u + 1] - pl.t_approx.off[u]) * P * nq;
+        if (pl.a_deg) {
+            for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++) {
+                double d1 = pl.a_deg[k] + 1;
+                c += d1 * d1 * d1;
+            }
+        } else {
+            c += (double)(pl.t_approx.off[u + 1] - pl.t_approx.off[u]) * P * nq;
+        }
         for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) c += S.numpar[pl.t_direct.idx[k]];
         leaf_cost[u] = c;
     }
@@ -420,13 +443,22 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     double *d_sctr = nullptr, *d_tctr = nullptr;
     int64_t *d_mxdoff = nullptr, *d_mxcpoff = nullptr;
     int *d_mxdidx = nullptr, *d_mxcpidx = nullptr;
-    unsigned char *d_mxdflag = nullptr;
+    unsigned char *d_mxdflag = nullptr, *d_adeg = nullptr;
+    double *d_xgrid[BT_MAX_DEGREE + 1] = {}, *d_xQ[BT_MAX_DEGREE + 1] = {};
+    float *d_xQ32[BT_MAX_DEGREE + 1] = {};
     if (mixed) {
         L.add(&d_spos, ns); L.add(&d_tpos, nt);
         if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P);
         L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
         L.add(&d_mxdoff, mx_doff.size()); L.add(&d_mxdidx, mx_didx.size()); L.add(&d_mxdflag, mx_dflag.size());
         L.add(&d_mxcpoff, mx_cpoff.size()); L.add(&d_mxcpidx, mx_cpidx.size());
+        if (pl.a_deg) L.add(&d_adeg, n_approx);
+        for (size_t i = 0; i < xdeg.size(); i++) {
+            size_t Pd = (size_t)(xdeg[i] + 1) * (xdeg[i] + 1) * (xdeg[i] + 1);
+            L.add(&d_xgrid[i], xgrid[i].size());
+            L.add(&d_xQ[i], (size_t)S.n * Pd);
+            L.add(&d_xQ32[i], (size_t)S.n * Pd);
+        }
     }
 
     if (!arena.reserve(L.total())) {
@@ -466,6 +498,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
             UP(d_mxdflag, mx_dflag.data(), mx_dflag.size());
+            if (pl.a_deg) UP(d_adeg, pl.a_deg, n_approx);
+            for (size_t i = 0; i < xdeg.size(); i++) UP(d_xgrid[i], xgrid[i].data(), xgrid[i].size());
             UP(d_mxcpoff, mx_cpoff.data(), mx_cpoff.size()); UP(d_mxcpidx, mx_cpidx.data(), mx_cpidx.size());
         }
 #undef UP
@@ -492,6 +526,22 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             }
             if (mixed) {
                 bt::launch_to_f32((size_t)S.n * P, d_Q, d_Q32, st);
+                launches++;
+            }
+            // proxy charges at the other degrees chosen per interaction
+            for (size_t i = 0; i < xdeg.size(); i++) {
+                const int d = xdeg[i];
+                bt::launch_p2m(d, false, S.nleaves, d_sleaves, S.n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww, d_sx,
+                               d_sy, d_sz, d_sq, d_xQ[i], st);
+                launches++;
+                for (int l = S.max_depth - 1; l >= 0; l--) {
+                    int cnt = S.lvl_off[l + 1] - S.lvl_off[l];
+                    if (cnt > 0) {
+                        bt::launch_m2m(d, cnt, d_slvl + S.lvl_off[l], d_snch, d_sch, d_xgrid[i], d_xQ[i], st);
+                        launches++;
+                    }
+                }
+                bt::launch_to_f32((size_t)S.n * (d + 1) * (d + 1) * (d + 1), d_xQ[i], d_xQ32[i], st);
                 launches++;
             }
         }
@@ -521,10 +571,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         if (nt > 0 && mixed) {
             bt::MixedTargetsArgs a;
             memset(&a, 0, sizeof a);
-            a.n = n; a.max_np1 = n + 1; a.nitems = (int)ev_items.size(); a.items = d_evitems;
+            a.n = n; a.max_np1 = max_np1; a.nitems = (int)ev_items.size(); a.items = d_evitems;
             a.leaf_node = d_tleaves; a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.t_ctr = d_tctr; a.tpos = d_tpos;
-            a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = nullptr;
+            a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = d_adeg;
             a.s_grid[n] = d_sgrid; a.Q32[n] = d_Q32;
+            for (size_t i = 0; i < xdeg.size(); i++) { a.s_grid[xdeg[i]] = d_xgrid[i]; a.Q32[xdeg[i]] = d_xQ32[i]; }
             a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.d_flag = d_mxdflag; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
             a.spos = d_spos; a.kc = bt::mixed_kernel_constant(o.kernel, o.kp); a.pot = d_pot;
             bt::launch_eval_targets_mixed(o.kernel, a, st);
@@ -588,6 +639,145 @@ done:
 }
 
 // ---------------------------------------------------------------------------
+// Learned degree selection (particle-cluster interactions, mixed path)
+// ---------------------------------------------------------------------------
+std::vector<float> g_selector;      // installed MLP weights (bt_selector_set), process-wide
+std::mutex g_selector_mu;
+constexpr double SELECT_MARGIN_DECADES = 0.5;   // predicted error must sit this far below the budget
+
+void node_geometry(const bt_tree &t, std::vector<double> &ctr, std::vector<double> &rad)
+{
+    ctr.resize(3 * (size_t)t.n);
+    rad.resize(t.n);
+    for (int i = 0; i < t.n; i++) {
+        ctr[3 * i] = t.xm[i]; ctr[3 * i + 1] = t.ym[i]; ctr[3 * i + 2] = t.zm[i];
+        rad[i] = t.rad[i];
+    }
+}
+
+// Predict the error of every particle-cluster entry at every degree, choose
+// the lowest degree under the budget (or direct evaluation), and rewrite the
+// plan's target-leaf lists accordingly.
+int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol)
+{
+    std::vector<float> w;
+    {
+        std::lock_guard<std::mutex> lk(g_selector_mu);
+        w = g_selector;
+    }
+    if ((int)w.size() != bt::MLP_NWEIGHTS) {
+        set_err("no degree selector installed (bt_selector_set)");
+        return BT_ERR_PARAM;
+    }
+    const bt_tree &S = pl.st, &T = pl.tt;
+    const int64_t ne = pl.t_approx.off[pl.t_approx.rows];
+    std::vector<unsigned char> choice(ne > 0 ? ne : 1);
+    cudaStream_t st = ctx->stream;
+    int rc = BT_OK;
+    if (ne > 0) {
+        std::vector<double> sctr, srad, tctr, trad;
+        node_geometry(S, sctr, srad);
+        node_geometry(T, tctr, trad);
+        const int64_t CH = 1 << 18;
+        double *d_sq, *d_mom, *d_sctr, *d_tctr, *d_srad, *d_trad;
+        int *d_sibeg, *d_snum, *d_tnum, *d_idx, *d_unit;
+        int64_t *d_off;
+        float *d_feat, *d_w, *d_act, *d_pred;
+        unsigned char *d_choice;
+        Layout L;
+        L.add(&d_sq, pl.src.n); L.add(&d_mom, 2 * (size_t)S.n); L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
+        L.add(&d_srad, srad.size()); L.add(&d_trad, trad.size()); L.add(&d_sibeg, S.n); L.add(&d_snum, S.n);
+        L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
+        L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size()); L.add(&d_act, 3 * (size_t)CH * bt::MLP_H);
+        L.add(&d_pred, (size_t)ne * bt::MLP_OUT); L.add(&d_choice, ne);
+        if (!arena.reserve(L.total())) {
+            set_err(arena.fixed ? "degree selection needs more scratch than the static array holds"
+                                : "device allocation failed");
+            return arena.fixed ? BT_ERR_PARAM : BT_ERR_CUDA;
+        }
+        L.bind(arena);
+        {
+#define UP(dst, src, cnt) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
+            UP(d_sq, pl.src.q, pl.src.n); UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
+            UP(d_srad, srad.data(), srad.size()); UP(d_trad, trad.data(), trad.size());
+            UP(d_sibeg, S.ibeg, S.n); UP(d_snum, S.numpar, S.n); UP(d_tnum, T.numpar, T.n);
+            UP(d_idx, pl.t_approx.idx, ne); UP(d_unit, T.leaves, T.nleaves);
+            UP(d_off, pl.t_approx.off, pl.t_approx.rows + 1); UP(d_w, w.data(), w.size());
+#undef UP
+            bt::launch_node_moments(S.n, d_sibeg, d_snum, d_sq, d_mom, st);
+            bt::FeatureArgs fa;
+            fa.units = pl.t_approx.rows; fa.off = d_off; fa.idx = d_idx; fa.unit_node = d_unit;
+            fa.t_ctr = d_tctr; fa.s_ctr = d_sctr; fa.t_rad = d_trad; fa.s_rad = d_srad; fa.s_mom = d_mom;
+            fa.t_numpar = d_tnum; fa.s_numpar = d_snum;
+            bt::launch_features(fa, ne, d_feat, st);
+            long long launches = 2;
+            for (int64_t c0 = 0; c0 < ne; c0 += CH) {
+                int B = (int)std::min<int64_t>(CH, ne - c0);
+                bt::mlp_forward(d_w, B, d_feat + c0 * bt::MLP_IN, d_act, d_pred + c0 * bt::MLP_OUT, st);
+                launches += 4;
+            }
+            bt::launch_select(ne, d_pred, d_feat, (float)(log10(tol) - SELECT_MARGIN_DECADES), d_choice, st);
+            launches++;
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(choice.data(), d_choice, ne, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            g_launches += launches;
+        }
+    }
+    {
+        // rewrite the target-leaf lists: chosen degree per kept entry, direct
+        // evaluation for the rest (appended to the direct list)
+        const int rows = pl.t_approx.rows;
+        int64_t *aoff = (int64_t *)malloc(sizeof(int64_t) * (rows + 1));
+        int64_t *doff = (int64_t *)malloc(sizeof(int64_t) * (rows + 1));
+        std::vector<int> aidx, didx;
+        std::vector<unsigned char> adeg;
+        aoff[0] = doff[0] = 0;
+        for (int u = 0; u < rows; u++) {
+            for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++) {
+                if (choice[k] == bt::MLP_PP) didx.push_back(pl.t_approx.idx[k]);
+                else { aidx.push_back(pl.t_approx.idx[k]); adeg.push_back(choice[k]); }
+            }
+            for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) didx.push_back(pl.t_direct.idx[k]);
+            aoff[u + 1] = (int64_t)aidx.size();
+            doff[u + 1] = (int64_t)didx.size();
+        }
+        bt_csr_free(&pl.t_approx);
+        bt_csr_free(&pl.t_direct);
+        pl.t_approx.rows = pl.t_direct.rows = rows;
+        pl.t_approx.off = aoff;
+        pl.t_direct.off = doff;
+        pl.t_approx.idx = (int *)malloc(sizeof(int) * (aidx.size() + 1));
+        pl.t_direct.idx = (int *)malloc(sizeof(int) * (didx.size() + 1));
+        memcpy(pl.t_approx.idx, aidx.data(), sizeof(int) * aidx.size());
+        memcpy(pl.t_direct.idx, didx.data(), sizeof(int) * didx.size());
+        free(pl.a_deg);
+        pl.a_deg = (unsigned char *)malloc(adeg.size() + 1);
+        memcpy(pl.a_deg, adeg.data(), adeg.size());
+    }
+done:
+    return rc;
+}
+
+// Interaction counts after a learned selection (what the kernels evaluate).
+void count_learned(const bt_plan &pl, bt_report *r)
+{
+    const bt_tree &S = pl.st, &T = pl.tt;
+    long long pp = 0, pc = 0;
+    for (int u = 0; u < T.nleaves; u++) {
+        long long m = T.numpar[T.leaves[u]];
+        for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) pp += m * S.numpar[pl.t_direct.idx[k]];
+        for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++) {
+            long long d1 = pl.a_deg[k] + 1;
+            pc += m * d1 * d1 * d1;
+        }
+    }
+    r->pp_ptwise = pp;
+    r->pc_ptwise = pc;
+    r->eval_flops = (long long)(pp * flops_per_eval(pl.prm, false) + pc * flops_per_eval(pl.prm, true));
+}
+
+// ---------------------------------------------------------------------------
 // Static device scratch of the allocation-free entry point bt_eval_noalloc.
 // In host code the symbol is only a host-side stand-in: its device address is
 // looked up once per device (cudaGetSymbolAddress with that device current)
@@ -642,6 +832,17 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         return BT_ERR_PARAM;
     }
     prm.precision = opts ? opts->precision : BT_PRECISION_FP64;
+    const bool learned = opts && opts->degree_policy == BT_DEGREE_LEARNED;
+    if (opts && opts->degree_policy != BT_DEGREE_FIXED && !learned) {
+        set_err("invalid degree policy %d", opts->degree_policy);
+        return BT_ERR_PARAM;
+    }
+    if (learned && (prm.precision != BT_PRECISION_MIXED || prm.ctype != PARTICLE_CLUSTER || prm.approx != LAGRANGE ||
+                    prm.kernel != COULOMB)) {
+        set_err("learned degree selection is provided for mixed precision, particle-cluster, Lagrange, Coulomb");
+        return BT_ERR_UNSUPPORTED;
+    }
+    const double tol = (opts && opts->tolerance > 0) ? opts->tolerance : 1e-6;
     DeviceCtx *ctx = nullptr;
     rc = get_ctx(device, &ctx);
     if (rc != BT_OK) return rc;
@@ -682,6 +883,17 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         rep->ms_setup = t1 - t0;
         rep->ms_total = t1 - t0;
         count_interactions(pl, rep);
+    }
+    if (learned) {
+        rc = select_degrees(ctx, *arena, pl, tol);
+        if (rc != BT_OK) {
+            bt_plan_free(&pl);
+            return rc;
+        }
+        if (rep) {
+            count_learned(pl, rep);
+            rep->ms_setup = now_ms() - t0;
+        }
     }
     rc = run_plan(ctx, *arena, pl, out, on_dev, rep);
     bt_plan_free(&pl);
@@ -853,6 +1065,272 @@ long bt_lists(int numTargets, int numSources, const double *targetX, const doubl
     }
     bt_plan_free(&pl);
     return cnt <= cap ? cnt : -1;
+}
+
+long bt_selector_nweights(void) { return bt::MLP_NWEIGHTS; }
+
+int bt_selector_set(const float *weights, long count)
+{
+    g_err[0] = 0;
+    if (!weights || count != bt::MLP_NWEIGHTS) {
+        set_err("selector needs %d weights", bt::MLP_NWEIGHTS);
+        return BT_ERR_PARAM;
+    }
+    std::lock_guard<std::mutex> lk(g_selector_mu);
+    g_selector.assign(weights, weights + count);
+    return BT_OK;
+}
+
+long bt_selector_training_data(int n, const double *x, const double *y, const double *z, const double *q,
+                               double theta, int leaf, int nsamples, unsigned seed, float *features, float *labels,
+                               int device)
+{
+    g_err[0] = 0;
+    if (n <= 0 || !x || !y || !z || !q || !features || !labels || nsamples <= 0 || leaf < 1) {
+        set_err("invalid arguments");
+        return -BT_ERR_PARAM;
+    }
+    DeviceCtx *ctx = nullptr;
+    int rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return -rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = ctx->stream;
+    bt_plan pl;
+    memset(&pl, 0, sizeof pl);
+    // lists as the fixed-degree-10 method builds them (the size check of the
+    // MAC depends on the degree), so training samples the interactions the
+    // selector is later asked about
+    bt_params_setup(&pl.prm, COULOMB, 0, nullptr, SKIPPING, LAGRANGE, PARTICLE_CLUSTER, theta, 10, leaf, leaf, 1.0,
+                    -1.0, 0);
+    build_plan(pl, n, n, x, y, z, x, y, z, q);
+    const bt_tree &S = pl.st, &T = pl.tt;
+    // sample particle-cluster entries (clusters up to 2e5 particles keep the
+    // exact sums affordable)
+    std::vector<int> tn_, sn_;
+    {
+        std::vector<std::pair<int, int>> all;
+        for (int u = 0; u < pl.t_approx.rows; u++)
+            for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++)
+                if (S.numpar[pl.t_approx.idx[k]] <= 200000) all.push_back({T.leaves[u], pl.t_approx.idx[k]});
+        uint64_t s = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+        int want = std::min<int>(nsamples, (int)all.size());
+        for (int i = 0; i < want; i++) {        // partial Fisher-Yates with a 64-bit LCG
+            s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+            size_t j = i + (size_t)((s >> 33) % (all.size() - i));
+            std::swap(all[i], all[j]);
+            tn_.push_back(all[i].first);
+            sn_.push_back(all[i].second);
+        }
+    }
+    const int ns_ = (int)tn_.size();
+    std::vector<double> sctr, srad, tctr, trad;
+    node_geometry(S, sctr, srad);
+    node_geometry(T, tctr, trad);
+    std::vector<std::vector<double>> grids(bt::MLP_DMAX + 1);
+    std::vector<double> slen;
+    for (int d = bt::MLP_DMIN; d <= bt::MLP_DMAX; d++) fill_grids(S, d, grids[d], slen);
+    double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx, *d_ty, *d_tz, *d_mom, *d_sctr, *d_tctr, *d_srad, *d_trad, *d_slen;
+    int *d_sibeg, *d_snum, *d_tibeg, *d_tnum, *d_snch, *d_sch, *d_sleaves, *d_slvl, *d_tn, *d_sn;
+    float *d_feat, *d_lab;
+    double *d_grid[bt::MLP_DMAX + 1] = {}, *d_Q[bt::MLP_DMAX + 1] = {};
+    Layout L;
+    L.add(&d_sx, n); L.add(&d_sy, n); L.add(&d_sz, n); L.add(&d_sq, n); L.add(&d_tx, n); L.add(&d_ty, n); L.add(&d_tz, n);
+    L.add(&d_mom, 2 * (size_t)S.n); L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
+    L.add(&d_srad, srad.size()); L.add(&d_trad, trad.size()); L.add(&d_slen, slen.size());
+    L.add(&d_sibeg, S.n); L.add(&d_snum, S.n); L.add(&d_tibeg, T.n); L.add(&d_tnum, T.n); L.add(&d_snch, S.n);
+    L.add(&d_sch, 8 * (size_t)S.n); L.add(&d_sleaves, S.nleaves); L.add(&d_slvl, S.lvl_off[S.max_depth]);
+    L.add(&d_tn, ns_); L.add(&d_sn, ns_); L.add(&d_feat, (size_t)ns_ * bt::MLP_IN); L.add(&d_lab, (size_t)ns_ * bt::MLP_OUT);
+    for (int d = bt::MLP_DMIN; d <= bt::MLP_DMAX; d++) {
+        L.add(&d_grid[d], grids[d].size());
+        L.add(&d_Q[d], (size_t)S.n * (d + 1) * (d + 1) * (d + 1));
+    }
+    long ret = ns_;
+    if (!ctx->arena.reserve(L.total())) {
+        set_err("device allocation failed");
+        bt_plan_free(&pl);
+        return -BT_ERR_CUDA;
+    }
+    L.bind(ctx->arena);
+    {
+#define UP(dst, src, cnt) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
+        UP(d_sx, pl.src.x, n); UP(d_sy, pl.src.y, n); UP(d_sz, pl.src.z, n); UP(d_sq, pl.src.q, n);
+        UP(d_tx, pl.tgt.x, n); UP(d_ty, pl.tgt.y, n); UP(d_tz, pl.tgt.z, n);
+        UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
+        UP(d_srad, srad.data(), srad.size()); UP(d_trad, trad.data(), trad.size()); UP(d_slen, slen.data(), slen.size());
+        UP(d_sibeg, S.ibeg, S.n); UP(d_snum, S.numpar, S.n); UP(d_tibeg, T.ibeg, T.n); UP(d_tnum, T.numpar, T.n);
+        UP(d_snch, S.nchild, S.n); UP(d_sch, S.child, 8 * (size_t)S.n); UP(d_sleaves, S.leaves, S.nleaves);
+        UP(d_slvl, S.lvl_nodes, S.lvl_off[S.max_depth]); UP(d_tn, tn_.data(), ns_); UP(d_sn, sn_.data(), ns_);
+        for (int d = bt::MLP_DMIN; d <= bt::MLP_DMAX; d++) UP(d_grid[d], grids[d].data(), grids[d].size());
+#undef UP
+        long long launches = 0;
+        for (int d = bt::MLP_DMIN; d <= bt::MLP_DMAX; d++) {
+            bt::launch_p2m(d, false, S.nleaves, d_sleaves, S.n, d_sibeg, d_snum, d_grid[d], d_slen, nullptr, d_sx, d_sy,
+                           d_sz, d_sq, d_Q[d], st);
+            launches++;
+            for (int l = S.max_depth - 1; l >= 0; l--) {
+                int cnt = S.lvl_off[l + 1] - S.lvl_off[l];
+                if (cnt > 0) { bt::launch_m2m(d, cnt, d_slvl + S.lvl_off[l], d_snch, d_sch, d_grid[d], d_Q[d], st); launches++; }
+            }
+        }
+        bt::launch_node_moments(S.n, d_sibeg, d_snum, d_sq, d_mom, st);
+        bt::FeatureArgs fa;
+        memset(&fa, 0, sizeof fa);
+        fa.t_ctr = d_tctr; fa.s_ctr = d_sctr; fa.t_rad = d_trad; fa.s_rad = d_srad; fa.s_mom = d_mom;
+        fa.t_numpar = d_tnum; fa.s_numpar = d_snum;
+        bt::launch_features_pairs(fa, ns_, d_tn, d_sn, d_feat, st);
+        bt::LabelArgs la;
+        memset(&la, 0, sizeof la);
+        la.tnodes = d_tn; la.snodes = d_sn; la.t_ibeg = d_tibeg; la.t_numpar = d_tnum; la.s_ibeg = d_sibeg;
+        la.s_numpar = d_snum; la.tx = d_tx; la.ty = d_ty; la.tz = d_tz; la.sx = d_sx; la.sy = d_sy; la.sz = d_sz;
+        la.sq = d_sq; la.t_ctr = d_tctr; la.s_ctr = d_sctr; la.s_mom = d_mom; la.labels = d_lab;
+        for (int d = bt::MLP_DMIN; d <= bt::MLP_DMAX; d++) { la.grid[d] = d_grid[d]; la.Q[d] = d_Q[d]; }
+        bt::launch_labels(la, ns_, st);
+        launches += 3;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(features, d_feat, sizeof(float) * (size_t)ns_ * bt::MLP_IN, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(labels, d_lab, sizeof(float) * (size_t)ns_ * bt::MLP_OUT, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        g_launches += launches;
+    }
+done:
+    bt_plan_free(&pl);
+    return rc == BT_OK ? ret : -rc;
+}
+
+int bt_mlp_loss_grad(const float *weights, const float *features, const float *labels, int n, float *grad_out,
+                     float *loss_out, int device)
+{
+    g_err[0] = 0;
+    if (!weights || !features || !labels || n <= 0 || !grad_out) { set_err("invalid arguments"); return BT_ERR_PARAM; }
+    DeviceCtx *ctx = nullptr;
+    int rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = ctx->stream;
+    float *d_w, *d_x, *d_y, *d_act, *d_yh, *d_db, *d_loss, *d_g;
+    Layout L;
+    L.add(&d_w, bt::MLP_NWEIGHTS); L.add(&d_x, (size_t)n * bt::MLP_IN); L.add(&d_y, (size_t)n * bt::MLP_OUT);
+    L.add(&d_act, 3 * (size_t)n * bt::MLP_H); L.add(&d_yh, (size_t)n * bt::MLP_OUT);
+    L.add(&d_db, 2 * (size_t)n * bt::MLP_H + (size_t)n * bt::MLP_OUT); L.add(&d_loss, n); L.add(&d_g, bt::MLP_NWEIGHTS);
+    if (!ctx->arena.reserve(L.total())) { set_err("device allocation failed"); return BT_ERR_CUDA; }
+    L.bind(ctx->arena);
+    std::vector<float> lossb(n);
+    {
+        CK(cudaMemcpyAsync(d_w, weights, sizeof(float) * bt::MLP_NWEIGHTS, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_x, features, sizeof(float) * (size_t)n * bt::MLP_IN, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_y, labels, sizeof(float) * (size_t)n * bt::MLP_OUT, cudaMemcpyHostToDevice, st));
+        bt::mlp_forward_backward(d_w, n, d_x, d_y, d_act, d_yh, d_db, d_loss, d_g, st);
+        g_launches += 12;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(grad_out, d_g, sizeof(float) * bt::MLP_NWEIGHTS, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(lossb.data(), d_loss, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (loss_out) {
+            double s = 0;
+            for (int i = 0; i < n; i++) s += lossb[i];
+            *loss_out = (float)(s / n);
+        }
+    }
+done:
+    return rc;
+}
+
+int bt_mlp_predict(const float *weights, const float *features, long n, float *out, int device)
+{
+    g_err[0] = 0;
+    if (!weights || !features || n <= 0 || !out) { set_err("invalid arguments"); return BT_ERR_PARAM; }
+    DeviceCtx *ctx = nullptr;
+    int rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = ctx->stream;
+    float *d_w, *d_x, *d_act, *d_yh;
+    Layout L;
+    L.add(&d_w, bt::MLP_NWEIGHTS); L.add(&d_x, (size_t)n * bt::MLP_IN); L.add(&d_act, 3 * (size_t)n * bt::MLP_H);
+    L.add(&d_yh, (size_t)n * bt::MLP_OUT);
+    if (!ctx->arena.reserve(L.total())) { set_err("device allocation failed"); return BT_ERR_CUDA; }
+    L.bind(ctx->arena);
+    {
+        CK(cudaMemcpyAsync(d_w, weights, sizeof(float) * bt::MLP_NWEIGHTS, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_x, features, sizeof(float) * (size_t)n * bt::MLP_IN, cudaMemcpyHostToDevice, st));
+        bt::mlp_forward(d_w, (int)n, d_x, d_act, d_yh, st);
+        g_launches += 4;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, d_yh, sizeof(float) * (size_t)n * bt::MLP_OUT, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+done:
+    return rc;
+}
+
+int bt_selector_train(const float *features, const float *labels, long n, int epochs, int batch, float lr,
+                      unsigned seed, float *weights, float *final_loss, int device)
+{
+    g_err[0] = 0;
+    if (!features || !labels || !weights || n <= 0 || epochs <= 0 || batch <= 0) {
+        set_err("invalid arguments");
+        return BT_ERR_PARAM;
+    }
+    if (batch > n) batch = (int)n;
+    DeviceCtx *ctx = nullptr;
+    int rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = ctx->stream;
+    const int NW = bt::MLP_NWEIGHTS;
+    float *d_w, *d_m, *d_v, *d_g, *d_X, *d_Y, *d_xb, *d_yb, *d_act, *d_yh, *d_db, *d_loss;
+    int *d_rows;
+    Layout L;
+    L.add(&d_w, NW); L.add(&d_m, NW); L.add(&d_v, NW); L.add(&d_g, NW);
+    L.add(&d_X, (size_t)n * bt::MLP_IN); L.add(&d_Y, (size_t)n * bt::MLP_OUT);
+    L.add(&d_xb, (size_t)batch * bt::MLP_IN); L.add(&d_yb, (size_t)batch * bt::MLP_OUT);
+    L.add(&d_act, 3 * (size_t)batch * bt::MLP_H); L.add(&d_yh, (size_t)batch * bt::MLP_OUT);
+    L.add(&d_db, 2 * (size_t)batch * bt::MLP_H + (size_t)batch * bt::MLP_OUT); L.add(&d_loss, batch);
+    L.add(&d_rows, n);
+    if (!ctx->arena.reserve(L.total())) { set_err("device allocation failed"); return BT_ERR_CUDA; }
+    L.bind(ctx->arena);
+    std::vector<int> perm(n);
+    for (long i = 0; i < n; i++) perm[i] = (int)i;
+    uint64_t s = seed * 2862933555777941757ULL + 3037000493ULL;
+    std::vector<float> lossb(batch);
+    double last = 0;
+    long long launches = 0;
+    {
+        CK(cudaMemcpyAsync(d_w, weights, sizeof(float) * NW, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(d_m, 0, sizeof(float) * NW, st));
+        CK(cudaMemsetAsync(d_v, 0, sizeof(float) * NW, st));
+        CK(cudaMemcpyAsync(d_X, features, sizeof(float) * (size_t)n * bt::MLP_IN, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_Y, labels, sizeof(float) * (size_t)n * bt::MLP_OUT, cudaMemcpyHostToDevice, st));
+        int step = 0;
+        const long nbatch = n / batch;
+        for (int ep = 0; ep < epochs; ep++) {
+            for (long i = n - 1; i > 0; i--) {      // Fisher-Yates with a 64-bit LCG
+                s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+                long j = (long)((s >> 33) % (uint64_t)(i + 1));
+                std::swap(perm[i], perm[j]);
+            }
+            CK(cudaMemcpyAsync(d_rows, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+            for (long b = 0; b < nbatch; b++) {
+                bt::gather_rows(batch, bt::MLP_IN, d_rows + b * batch, d_X, d_xb, st);
+                bt::gather_rows(batch, bt::MLP_OUT, d_rows + b * batch, d_Y, d_yb, st);
+                bt::mlp_forward_backward(d_w, batch, d_xb, d_yb, d_act, d_yh, d_db, d_loss, d_g, st);
+                // the input normalisation is fixed: keep its gradient zero
+                bt::mlp_adam(NW - 2 * bt::MLP_IN, d_w + 2 * bt::MLP_IN, d_g + 2 * bt::MLP_IN, d_m + 2 * bt::MLP_IN,
+                             d_v + 2 * bt::MLP_IN, lr, ++step, st);
+                launches += 15;
+            }
+            CK(cudaStreamSynchronize(st));
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(lossb.data(), d_loss, sizeof(float) * batch, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(weights, d_w, sizeof(float) * NW, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int i = 0; i < batch; i++) last += lossb[i];
+        if (final_loss) *final_loss = (float)(last / batch);
+        g_launches += launches;
+    }
+done:
+    return rc;
 }
 
 int bt_tree_dump(int n, const double *x, const double *y, const double *z, int maxparnode, int *ints, double *dbl, int cap)

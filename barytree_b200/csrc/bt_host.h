@@ -63,6 +63,7 @@ typedef struct {
     bt_csr t_direct;        /* per target leaf: source nodes evaluated directly (PP)     */
     bt_csr g_cc;            /* per target node: source clusters for M2L (CC)             */
     bt_csr g_cp;            /* per target node: source nodes evaluated onto the grid (CP) */
+    unsigned char *a_deg;   /* per t_approx entry: interpolation degree (NULL: prm.degree) */
 } bt_plan;
 
 /* bt_params.c */

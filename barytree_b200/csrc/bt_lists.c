@@ -224,4 +224,6 @@ void bt_plan_free(bt_plan *pl)
     bt_tree_free(&pl->tt);
     bt_csr *c[8] = {&pl->pp, &pl->ap, &pl->pc, &pl->cp, &pl->t_approx, &pl->t_direct, &pl->g_cc, &pl->g_cp};
     for (int i = 0; i < 8; i++) bt_csr_free(c[i]);
+    free(pl->a_deg);
+    pl->a_deg = NULL;
 }

@@ -49,6 +49,11 @@ CONFIGS = {
     3: dict(workload="N=4,000,000 Gaussian sigma 0.25 clipped to [-1,1]^3, charges +-1, Coulomb, particle-cluster "
                      "Hermite n=6, theta 0.7, leaf 1000, size check 4", N=4_000_000, dist="gauss", kernel=1, kp=0.0,
             approx=2, ctype=1, degree=6, theta=0.7, leaf=1000, sc=4.0, sample_n=60_000),
+    5: dict(workload="N=16,000,000: 80% in 8 Gaussian blobs (centres U[-0.7,0.7]^3, sigma log-uniform 0.05-0.3, "
+                     "clipped to [-1,1]^3), 20% uniform [-1,1]^3, charges U[-1,1], Coulomb, particle-cluster "
+                     "Lagrange, theta 0.7, leaf 2000; degree per interaction from the learned selector at 1e-6, "
+                     "against fixed degree 10", N=16_000_000, dist="blobs", kernel=1, kp=0.0, approx=1, ctype=1,
+            degree=10, theta=0.7, leaf=2000, sc=1.0, sample_n=80_000),
 }
 
 
@@ -62,6 +67,9 @@ def make_inputs(cfg, seed):
     elif cfg["dist"] == "gauss":
         x, y, z = (np.clip(rng.normal(0, 0.25, n), -1, 1) for _ in range(3))
         q = rng.choice([-1.0, 1.0], n)
+    elif cfg["dist"] == "blobs":
+        from barytree_b200.selector import blobs
+        x, y, z, q = blobs(n, seed)
     else:
         raise ValueError(cfg["dist"])
     return x, y, z, q
@@ -193,8 +201,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", type=int, default=2, choices=sorted(CONFIGS))
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--config", type=int, default=5, choices=sorted(CONFIGS))
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--degree-policy", choices=["auto", "fixed", "learned"], default="auto",
+                    help="auto: learned for the 16M clustered configuration, fixed otherwise")
+    ap.add_argument("--tolerance", type=float, default=1e-6)
+    ap.add_argument("--no-fp64-plain", action="store_true", help="skip the FP64 fixed-degree comparison step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
@@ -220,7 +232,15 @@ def main():
     x, y, z, q = make_inputs(cfg, seed=rank)
     n = len(x)
     prec = B.PRECISION_MIXED if args.precision == "mixed" else B.PRECISION_FP64
-    common = dict(kernel=cfg["kernel"], kernel_param=cfg["kp"], approximation=cfg["approx"],
+    policy = args.degree_policy
+    if policy == "auto":
+        policy = "learned" if args.config == 5 and prec == B.PRECISION_MIXED else "fixed"
+    if policy == "learned":
+        from barytree_b200 import selector
+        selector.install_default()
+    common = dict(degree_policy=B.DEGREE_LEARNED if policy == "learned" else B.DEGREE_FIXED,
+                  tolerance=args.tolerance,
+                  kernel=cfg["kernel"], kernel_param=cfg["kp"], approximation=cfg["approx"],
                   compute_type=cfg["ctype"], theta=cfg["theta"], degree=cfg["degree"], max_source_leaf=cfg["leaf"],
                   max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=local)
 
@@ -283,6 +303,29 @@ def main():
     rel_l2 = float(np.linalg.norm(pot - d) / np.linalg.norm(d))
     rel_max = float(np.max(np.abs(pot - d)) / np.max(np.abs(d)))
 
+    # the plain FP64 treecode at the configuration's fixed degree on the same
+    # system and inputs (the denominator of the mixed + learned speed-up)
+    fp64_plain = None
+    if not args.no_fp64_plain and (prec != B.PRECISION_FP64 or policy != "fixed"):
+        plain = dict(common)
+        plain.update(precision=B.PRECISION_FP64, degree_policy=B.DEGREE_FIXED)
+
+        def step_plain():
+            return B.treecode_ptr(n, n, *(t.data_ptr() for t in d_in[3:6]), *(t.data_ptr() for t in d_in[:3]),
+                                  d_in[6].data_ptr(), d_out.data_ptr(), inputs_on_device=True, **plain)
+        step_plain()
+        ms_plain, preps = timed(step_plain, 1)
+        t = torch.tensor([ms_plain], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_plain = float(t[0])
+        pp = d_out.cpu().numpy()[idx]
+        fp64_plain = {"value": world * n / (ms_plain * 1e-3), "unit": "targets/s", "ms_per_step": ms_plain,
+                      "steps": 1, "degree": cfg["degree"],
+                      "rel_l2_vs_fp64_direct": float(np.linalg.norm(pp - d) / np.linalg.norm(d)),
+                      "ms_eval_kernel": preps[-1]["ms_eval_kernel"],
+                      "interactions": preps[-1]["pp_ptwise"] + preps[-1]["pc_ptwise"]}
+
     if rank == 0:
         fp64_peak, fp32_peak, rsqrt_rate = B.measure_peaks(local)
         rep = reps[-1]
@@ -297,7 +340,8 @@ def main():
             "vs_baseline": None, "dtype": "f64" if prec == B.PRECISION_FP64 else "f32+f64",
             "data": "synthetic (seeded numpy PCG64 with the configuration's distribution)",
             "config": {"workload": cfg["workload"], "config_id": args.config, "precision": args.precision,
-                       "degree_policy": "fixed", "l2": "flushed between steps (256 MB write)",
+                       "degree_policy": policy, "tolerance": args.tolerance,
+                       "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"{world} independent system(s), one per GPU",
                        "rel_l2_vs_fp64_direct": rel_l2, "rel_max_vs_fp64_direct": rel_max,
                        "direct_sample_targets": len(idx)},
@@ -315,6 +359,10 @@ def main():
             "clocks": clock_info,
             "gpu_launches": launches,
         }
+        if fp64_plain is not None:
+            line["fp64_plain"] = fp64_plain
+            line["speedup_vs_fp64_plain"] = {"value": value / fp64_plain["value"],
+                                             "e2e": e2e / fp64_plain["value"]}
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(cfg, 1)
         print(json.dumps(line), flush=True)

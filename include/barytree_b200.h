@@ -178,6 +178,40 @@ long bt_lists(int numTargets, int numSources,
 int bt_tree_dump(int n, const double *x, const double *y, const double *z, int maxparnode,
             int *ints, double *dbl, int cap);
 
+/* ---------------------------------------------------------------------- */
+/* Learned degree selection (no counterpart in the reference).              */
+/* A small MLP (6 -> 64 -> 64 -> 64 -> 11, tanh, FP32) predicts, for each    */
+/* particle-cluster interaction, log10 of its normalised error at degrees   */
+/* 2..12; bt_eval with BT_DEGREE_LEARNED (mixed precision, particle-cluster,*/
+/* Lagrange, Coulomb) then uses the lowest degree predicted to meet the     */
+/* tolerance, or direct evaluation where that is cheaper or none does.      */
+/* Features: log10 source count, log10 target count, (r_c + r_b)/d, r_c/d,  */
+/* r_b/d, ||q||_1 / (||q||_2 sqrt(count)).                                  */
+/* Weights (floats): mean[6], std[6], W1[6][64], b1[64], W2[64][64], b2[64],*/
+/* W3[64][64], b3[64], W4[64][11], b4[11].                                  */
+/* ---------------------------------------------------------------------- */
+long bt_selector_nweights(void);
+int bt_selector_set(const float *weights, long count);
+/* Training data made by the treecode itself: builds the particle-cluster
+ * lists of the system (targets = sources), samples `nsamples` interactions
+ * and writes their features (6 floats each) and labels (11 floats each:
+ * log10 of the RMS error at degree d over up to 32 targets of the batch,
+ * divided by ||q_cluster||_2 / distance, against the exact FP64 sum over the
+ * cluster's particles).  Returns the number of samples written or -status. */
+long bt_selector_training_data(int n, const double *x, const double *y, const double *z, const double *q,
+                               double theta, int leaf, int nsamples, unsigned seed,
+                               float *features, float *labels, int device);
+/* Adam training on the GPU with the library's forward/backward kernels;
+ * `weights` holds the initial weights (with the input normalisation) and
+ * receives the trained ones. */
+int bt_selector_train(const float *features, const float *labels, long n, int epochs, int batch, float lr,
+                      unsigned seed, float *weights, float *final_loss, int device);
+/* Mean-squared-error loss and its gradient (weight layout) on one batch. */
+int bt_mlp_loss_grad(const float *weights, const float *features, const float *labels, int n,
+                     float *grad_out, float *loss_out, int device);
+/* Predicted log10 errors (11 per row). */
+int bt_mlp_predict(const float *weights, const float *features, long n, float *out, int device);
+
 /* Throughput microbenchmarks on `device` (the roofline denominators of the
  * SIMT evaluation kernels): dependent-FMA streams in FP64 and FP32 and a
  * reciprocal-square-root stream, each over all SMs.  Results in TFLOP/s
