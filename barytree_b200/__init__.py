@@ -78,10 +78,13 @@ class Report(ctypes.Structure):
                 ("num_cc", ctypes.c_longlong), ("pp_ptwise", ctypes.c_longlong), ("pc_ptwise", ctypes.c_longlong),
                 ("cp_ptwise", ctypes.c_longlong), ("cc_ptwise", ctypes.c_longlong),
                 ("ms_eval_kernel", ctypes.c_double), ("eval_flops", ctypes.c_longlong),
-                ("source_nodes", ctypes.c_int), ("target_nodes", ctypes.c_int), ("kernel_launches", ctypes.c_int)]
+                ("source_nodes", ctypes.c_int), ("target_nodes", ctypes.c_int), ("kernel_launches", ctypes.c_int),
+                ("selected", ctypes.c_longlong * 14)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["selected"] = list(self.selected)
+        return d
 
 
 class BaryTreeError(RuntimeError):

@@ -445,6 +445,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     int *d_mxdidx = nullptr, *d_mxcpidx = nullptr;
     unsigned char *d_mxdflag = nullptr, *d_adeg = nullptr;
     double *d_xgrid[BT_MAX_DEGREE + 1] = {}, *d_xQ[BT_MAX_DEGREE + 1] = {};
+    double *d_srad = nullptr, *d_trad = nullptr;
     float *d_xQ32[BT_MAX_DEGREE + 1] = {};
     if (mixed) {
         L.add(&d_spos, ns); L.add(&d_tpos, nt);
@@ -453,6 +454,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         L.add(&d_mxdoff, mx_doff.size()); L.add(&d_mxdidx, mx_didx.size()); L.add(&d_mxdflag, mx_dflag.size());
         L.add(&d_mxcpoff, mx_cpoff.size()); L.add(&d_mxcpidx, mx_cpidx.size());
         if (pl.a_deg) L.add(&d_adeg, n_approx);
+        L.add(&d_srad, S.n); L.add(&d_trad, T.n);
         for (size_t i = 0; i < xdeg.size(); i++) {
             size_t Pd = (size_t)(xdeg[i] + 1) * (xdeg[i] + 1) * (xdeg[i] + 1);
             L.add(&d_xgrid[i], xgrid[i].size());
@@ -499,6 +501,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
             UP(d_mxdflag, mx_dflag.data(), mx_dflag.size());
             if (pl.a_deg) UP(d_adeg, pl.a_deg, n_approx);
+            UP(d_srad, S.rad, S.n); UP(d_trad, T.rad, T.n);
             for (size_t i = 0; i < xdeg.size(); i++) UP(d_xgrid[i], xgrid[i].data(), xgrid[i].size());
             UP(d_mxcpoff, mx_cpoff.data(), mx_cpoff.size()); UP(d_mxcpidx, mx_cpidx.data(), mx_cpidx.size());
         }
@@ -578,6 +581,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             for (size_t i = 0; i < xdeg.size(); i++) { a.s_grid[xdeg[i]] = d_xgrid[i]; a.Q32[xdeg[i]] = d_xQ32[i]; }
             a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.d_flag = d_mxdflag; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
             a.spos = d_spos; a.kc = bt::mixed_kernel_constant(o.kernel, o.kp); a.pot = d_pot;
+            a.t_rad = d_trad; a.s_rad = d_srad;
+            a.tx64 = d_tx; a.ty64 = d_ty; a.tz64 = d_tz; a.sx64 = d_sx; a.sy64 = d_sy; a.sz64 = d_sz;
             bt::launch_eval_targets_mixed(o.kernel, a, st);
             launches++;
         } else if (nt > 0) {
@@ -735,6 +740,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol)
         aoff[0] = doff[0] = 0;
         for (int u = 0; u < rows; u++) {
             for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++) {
+                pl.sel_hist[choice[k] == bt::MLP_PP ? 13 : choice[k]]++;
                 if (choice[k] == bt::MLP_PP) didx.push_back(pl.t_approx.idx[k]);
                 else { aidx.push_back(pl.t_approx.idx[k]); adeg.push_back(choice[k]); }
             }
@@ -773,6 +779,7 @@ void count_learned(const bt_plan &pl, bt_report *r)
         }
     }
     r->pp_ptwise = pp;
+    for (int i = 0; i < 14; i++) r->selected[i] = pl.sel_hist[i];
     r->pc_ptwise = pc;
     r->eval_flops = (long long)(pp * flops_per_eval(pl.prm, false) + pc * flops_per_eval(pl.prm, true));
 }
@@ -1104,14 +1111,14 @@ long bt_selector_training_data(int n, const double *x, const double *y, const do
                     -1.0, 0);
     build_plan(pl, n, n, x, y, z, x, y, z, q);
     const bt_tree &S = pl.st, &T = pl.tt;
-    // sample particle-cluster entries (clusters up to 2e5 particles keep the
-    // exact sums affordable)
+    // sample particle-cluster entries of every size (the exact sums run over
+    // all of a cluster's particles for up to 32 targets)
     std::vector<int> tn_, sn_;
     {
         std::vector<std::pair<int, int>> all;
         for (int u = 0; u < pl.t_approx.rows; u++)
             for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++)
-                if (S.numpar[pl.t_approx.idx[k]] <= 200000) all.push_back({T.leaves[u], pl.t_approx.idx[k]});
+                all.push_back({T.leaves[u], pl.t_approx.idx[k]});
         uint64_t s = seed * 6364136223846793005ULL + 1442695040888963407ULL;
         int want = std::min<int>(nsamples, (int)all.size());
         for (int i = 0; i < want; i++) {        // partial Fisher-Yates with a 64-bit LCG

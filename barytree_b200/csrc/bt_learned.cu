@@ -154,6 +154,14 @@ k_labels(LabelArgs a)
 // ---------------------------------------------------------------------------
 // MLP: layer kernels (batch-major activations, weights [in][out])
 // ---------------------------------------------------------------------------
+// Normalised input, clipped to +-4 standard deviations so that interactions
+// outside the training range (for instance far larger clusters) are treated
+// like the most extreme ones seen in training instead of being extrapolated.
+__device__ __forceinline__ float norm_input(float x, float mean, float sd)
+{
+    return fminf(fmaxf((x - mean) / sd, -4.f), 4.f);
+}
+
 // Y[b][o] = act(sum_i X[b][i] W[i][o] + bias[o]); act: 0 none, 1 tanh.
 // The input layer first applies the stored normalisation (x - mean) / std.
 __global__ void k_linear_fwd(int B, int I, int O, const float *__restrict__ X, const float *__restrict__ W,
@@ -166,7 +174,7 @@ __global__ void k_linear_fwd(int B, int I, int O, const float *__restrict__ X, c
     float s = bias[o];
     for (int i = 0; i < I; i++) {
         float x = X[(size_t)b * I + i];
-        if (norm) x = (x - norm[i]) / norm[I + i];
+        if (norm) x = norm_input(x, norm[i], norm[I + i]);
         s = fmaf(x, W[i * O + o], s);
     }
     Y[idx] = act ? tanhf(s) : s;
@@ -196,7 +204,7 @@ __global__ void k_linear_bwd_w(int B, int I, int O, const float *__restrict__ X,
     if (i < I) {
         for (int b = 0; b < B; b++) {
             float x = X[(size_t)b * I + i];
-            if (norm) x = (x - norm[i]) / norm[I + i];
+            if (norm) x = norm_input(x, norm[i], norm[I + i]);
             s = fmaf(x, dY[(size_t)b * O + o], s);
         }
         gW[i * O + o] = s;

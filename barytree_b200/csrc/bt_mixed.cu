@@ -140,9 +140,17 @@ __device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, con
     for (int t = 0; t < NT; t++) out[t] = 0.f;
 }
 
+// Near-field tile.  FP32 leaf-relative coordinates carry an absolute error of
+// about 6e-8 of the leaf size, which is a large relative error for a pair
+// much closer than the leaf size (and such a pair dominates its target's
+// potential).  A pair with r^2 below thr2 = (quarter of the two leaves' radii)^2
+// therefore has its displacement recomputed from the FP64 coordinates before
+// the FP32 kernel evaluation; these pairs are rare, so the branch is cheap.
 template <int KT, bool SKIP>
 __device__ __forceinline__ void pp_tile(const float4 *tile, int cm, const float *x, const float *y, const float *z,
-                                        float kc, float *s)
+                                        float kc, float thr2, const double *xd, const double *yd, const double *zd,
+                                        const double *__restrict__ sx, const double *__restrict__ sy,
+                                        const double *__restrict__ sz, int base, float *s)
 {
 #pragma unroll 4
     for (int i = 0; i < cm; i++) {
@@ -150,7 +158,13 @@ __device__ __forceinline__ void pp_tile(const float4 *tile, int cm, const float 
 #pragma unroll
         for (int t = 0; t < MX_TPT; t++) {
             float dx = x[t] - p.x, dy = y[t] - p.y, dz = z[t] - p.z;
-            s[t] += kf_pp<KT, SKIP>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), p.w, kc);
+            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (r2 < thr2) {
+                const int gi = base + i;
+                float fx = (float)(xd[t] - sx[gi]), fy = (float)(yd[t] - sy[gi]), fz = (float)(zd[t] - sz[gi]);
+                r2 = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+            }
+            s[t] += kf_pp<KT, SKIP>(r2, p.w, kc);
         }
     }
 }
@@ -167,6 +181,7 @@ k_eval_targets_mixed(MixedTargetsArgs a)
     const int tnode = a.leaf_node[u];
     const int tb = a.t_ibeg[tnode], tn = a.t_numpar[tnode];
     float x[MX_TPT], y[MX_TPT], z[MX_TPT];
+    double xd[MX_TPT], yd[MX_TPT], zd[MX_TPT];
     bool act[MX_TPT];
     int tid[MX_TPT];
 #pragma unroll
@@ -176,7 +191,9 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         tid[t] = tb + (act[t] ? ti : 0);
         float4 tp = a.tpos[tid[t]];
         x[t] = tp.x; y[t] = tp.y; z[t] = tp.z;
+        xd[t] = a.tx64[tid[t]]; yd[t] = a.ty64[tid[t]]; zd[t] = a.tz64[tid[t]];
     }
+    const double trad = a.t_rad[tnode];
     const double cx = a.t_ctr[3 * tnode], cy = a.t_ctr[3 * tnode + 1], cz = a.t_ctr[3 * tnode + 2];
     const float kc = (float)a.kc;
     double acc[MX_TPT];
@@ -216,6 +233,8 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         float xs[MX_TPT], ys[MX_TPT], zs[MX_TPT];   // targets in the source leaf's frame
 #pragma unroll
         for (int t = 0; t < MX_TPT; t++) { xs[t] = x[t] - ox; ys[t] = y[t] - oy; zs[t] = z[t] - oz; }
+        const double rr = 0.25 * (trad + a.s_rad[s]);
+        const float thr2 = (float)(rr * rr);
         for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
             int cm = min(MX_TILE, sn - c0);
             for (int i = threadIdx.x; i < cm; i += blockDim.x) tile[i] = a.spos[sb + c0 + i];
@@ -223,8 +242,10 @@ k_eval_targets_mixed(MixedTargetsArgs a)
             float sum[MX_TPT];
 #pragma unroll
             for (int t = 0; t < MX_TPT; t++) sum[t] = 0.f;
-            if (skip) pp_tile<KT, true>(tile, cm, xs, ys, zs, kc, sum);
-            else pp_tile<KT, false>(tile, cm, xs, ys, zs, kc, sum);
+            if (skip)
+                pp_tile<KT, true>(tile, cm, xs, ys, zs, kc, thr2, xd, yd, zd, a.sx64, a.sy64, a.sz64, sb + c0, sum);
+            else
+                pp_tile<KT, false>(tile, cm, xs, ys, zs, kc, thr2, xd, yd, zd, a.sx64, a.sy64, a.sz64, sb + c0, sum);
 #pragma unroll
             for (int t = 0; t < MX_TPT; t++) acc[t] += (double)sum[t];
             __syncthreads();

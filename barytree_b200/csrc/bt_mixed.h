@@ -23,6 +23,9 @@ struct MixedTargetsArgs {
     const int *s_ibeg, *s_numpar;
     const double *s_ctr;                        // source node centres
     const float4 *spos;                         // sources relative to their leaf centre, with charge
+    const double *t_rad, *s_rad;                // node radii (close-pair threshold)
+    const double *tx64, *ty64, *tz64;           // FP64 coordinates for close pairs
+    const double *sx64, *sy64, *sz64;
     double kc;                                  // mixed_kernel_constant()
     double *pot;
 };

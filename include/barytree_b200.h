@@ -104,6 +104,8 @@ typedef struct bt_report {
     double ms_eval_kernel;     /* device time of the dominant evaluation kernel */
     long long eval_flops;      /* algorithmic FLOPs of that kernel               */
     int source_nodes, target_nodes, kernel_launches;
+    long long selected[14];    /* learned selection: entries per degree (index = degree),
+                                  index 13 = entries evaluated directly instead */
 } bt_report;
 
 /* Treecode evaluation with options and a report.  Same meaning of the

@@ -1,7 +1,7 @@
 """CPU FP64 oracle of the degree-selector MLP (test infrastructure).
 
 Same network and loss as the library's CUDA kernels (bt_learned.cu): input
-normalisation (x - mean) / std, three tanh layers of 64, a linear layer of 11,
+normalisation (x - mean) / std clipped to [-4, 4], three tanh layers of 64, a linear layer of 11,
 mean-squared error over all outputs.  Forward and backward in numpy FP64, for
 checking the GPU gradients.
 """
@@ -28,7 +28,7 @@ def unpack(w):
 
 def forward(w, X):
     p = unpack(w)
-    Xn = (np.asarray(X, dtype=np.float64) - p["mean"]) / p["std"]
+    Xn = np.clip((np.asarray(X, dtype=np.float64) - p["mean"]) / p["std"], -4.0, 4.0)
     A1 = np.tanh(Xn @ p["W1"] + p["b1"])
     A2 = np.tanh(A1 @ p["W2"] + p["b2"])
     A3 = np.tanh(A2 @ p["W3"] + p["b3"])
