@@ -143,9 +143,12 @@ __device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, con
 // Near-field tile.  FP32 leaf-relative coordinates carry an absolute error of
 // about 6e-8 of the leaf size, which is a large relative error for a pair
 // much closer than the leaf size (and such a pair dominates its target's
-// potential).  A pair with r^2 below thr2 = (quarter of the two leaves' radii)^2
+// potential).  A pair closer than a twentieth of the two leaves' summed radii
 // therefore has its displacement recomputed from the FP64 coordinates before
-// the FP32 kernel evaluation; these pairs are rare, so the branch is cheap.
+// the FP32 kernel evaluation.  Such pairs are rare (about 1e-5 of the near
+// field for uniform leaves), so the branch costs one compare; the pairs left
+// in FP32 carry at most about 2e-6 relative error each, which averages to
+// ~1e-7 relative in the potentials.
 template <int KT, bool SKIP>
 __device__ __forceinline__ void pp_tile(const float4 *tile, int cm, const float *x, const float *y, const float *z,
                                         float kc, float thr2, const double *xd, const double *yd, const double *zd,
@@ -233,7 +236,7 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         float xs[MX_TPT], ys[MX_TPT], zs[MX_TPT];   // targets in the source leaf's frame
 #pragma unroll
         for (int t = 0; t < MX_TPT; t++) { xs[t] = x[t] - ox; ys[t] = y[t] - oy; zs[t] = z[t] - oz; }
-        const double rr = 0.25 * (trad + a.s_rad[s]);
+        const double rr = 0.05 * (trad + a.s_rad[s]);
         const float thr2 = (float)(rr * rr);
         for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
             int cm = min(MX_TILE, sn - c0);

@@ -77,7 +77,8 @@ def test_mixed_close_pairs():
     b = B.treecode(x, y, z, x, y, z, q, degree=8, max_source_leaf=500, max_target_leaf=500,
                    precision=B.PRECISION_FP64)
     assert np.linalg.norm(a - b) / np.linalg.norm(b) <= TOL_VS_FP64_TREE
-    assert np.max(np.abs(a - b) / np.abs(b)) <= 1e-5
+    pair = np.arange(2 * k)                 # these targets' potentials are dominated by the close pair
+    assert np.max(np.abs(a[pair] - b[pair]) / np.abs(b[pair])) <= 1e-6
 
 
 def test_mixed_coincident_points():
