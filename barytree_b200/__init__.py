@@ -16,7 +16,7 @@ from enum import IntEnum
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libbarytree_b200.so")
+LIB_PATH = os.environ.get("BARYTREE_B200_LIB") or os.path.join(_HERE, "libbarytree_b200.so")
 
 
 class CEnum(IntEnum):
@@ -61,6 +61,7 @@ class ComputeType(CEnum):
 BT_OK, BT_ERR_PARAM, BT_ERR_UNSUPPORTED, BT_ERR_CUDA, BT_ERR_TIMEOUT, BT_ERR_NO_DEVICE = range(6)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 DEGREE_FIXED, DEGREE_LEARNED = 0, 1
+TREE_GPU, TREE_HOST = 0, 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -68,7 +69,7 @@ _ip = ctypes.POINTER(ctypes.c_int)
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("degree_policy", ctypes.c_int), ("tolerance", ctypes.c_double),
-                ("device", ctypes.c_int), ("inputs_on_device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("inputs_on_device", ctypes.c_int), ("tree_build", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):
@@ -105,7 +106,7 @@ _BTI_ARGS = (
 
 # every exported symbol of include/barytree_b200.h
 EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
-                    "bt_tree_dump", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
+                    "bt_tree_dump", "bt_tree_dump_ex", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
                     "bt_selector_nweights", "bt_selector_set", "bt_selector_training_data", "bt_selector_train",
                     "bt_mlp_loss_grad", "bt_mlp_predict")
 
@@ -138,6 +139,9 @@ def lib():
     L.bt_lists.restype = ctypes.c_long
     L.bt_tree_dump.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, ctypes.c_int)
     L.bt_tree_dump.restype = ctypes.c_int
+    L.bt_tree_dump_ex.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _dp,
+                                  _ip, ctypes.c_int)
+    L.bt_tree_dump_ex.restype = ctypes.c_int
     L.bt_measure_peaks.argtypes = (ctypes.c_int, _dp, _dp, _dp)
     L.bt_measure_peaks.restype = ctypes.c_int
     _fp = ctypes.POINTER(ctypes.c_float)
@@ -223,11 +227,11 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
              approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER,
              theta=0.7, degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
              precision=PRECISION_FP64, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0,
-             return_report=False):
-    """Extended entry point (bt_eval): options for precision / degree policy and a report."""
+             tree_build=TREE_GPU, return_report=False):
+    """Extended entry point (bt_eval): options for precision / degree policy / tree build and a report."""
     tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
     out = np.zeros(len(tx))
-    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0)
+    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, int(tree_build))
     rep = Report()
     rc = lib().bt_eval(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
                        int(kernel), float(kernel_param), int(approximation), int(compute_type), float(theta),
@@ -240,10 +244,12 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
 def treecode_ptr(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, kernel=Kernel.COULOMB, kernel_param=0.0,
                  approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7,
                  degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64,
-                 degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0, inputs_on_device=False):
+                 degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0, inputs_on_device=False,
+                 tree_build=TREE_GPU):
     """bt_eval on raw addresses (ints): device pointers when inputs_on_device, else host pointers."""
     cast = lambda a: ctypes.cast(ctypes.c_void_p(int(a)), _dp)  # noqa: E731
-    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), int(bool(inputs_on_device)))
+    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), int(bool(inputs_on_device)),
+                   int(tree_build))
     rep = Report()
     rc = lib().bt_eval(int(nt), int(ns), cast(tx), cast(ty), cast(tz), cast(sx), cast(sy), cast(sz), cast(sq),
                        cast(out), int(kernel), float(kernel_param), int(approximation), int(compute_type),
@@ -287,16 +293,23 @@ def interaction_lists(tx, ty, tz, sx, sy, sz, compute_type, approximation, theta
         cap *= 4
 
 
-def tree_summary(x, y, z, maxparnode):
-    """Per node (ibeg, iend, num_children, level) and (box..., radius)."""
+def tree_summary(x, y, z, maxparnode, tree_build=TREE_HOST, device=0, return_order=False):
+    """Per node (ibeg, iend, num_children, level) and (box..., radius); with
+    return_order also the particle permutation (order[i] = input index of
+    sorted particle i).  tree_build=TREE_GPU builds on the GPU."""
     x, y, z = map(_c, (x, y, z))
     cap = max(64, 4 * len(x) // max(1, maxparnode) + 64)
     ints = np.zeros(4 * cap, dtype=np.int32)
     dbl = np.zeros(7 * cap)
-    n = lib().bt_tree_dump(len(x), _p(x), _p(y), _p(z), int(maxparnode), ints.ctypes.data_as(_ip), _p(dbl), cap)
-    if n < 0:
+    order = np.zeros(max(1, len(x)), dtype=np.int32)
+    n = lib().bt_tree_dump_ex(len(x), _p(x), _p(y), _p(z), int(maxparnode), int(tree_build), int(device),
+                              ints.ctypes.data_as(_ip), _p(dbl), order.ctypes.data_as(_ip), cap)
+    if n == -1:
         raise BaryTreeError(BT_ERR_PARAM, "tree capacity")
-    return ints[: 4 * n].reshape(-1, 4), dbl[: 7 * n].reshape(-1, 7)
+    if n < 0:
+        raise BaryTreeError(BT_ERR_CUDA, last_error())
+    res = (ints[: 4 * n].reshape(-1, 4), dbl[: 7 * n].reshape(-1, 7))
+    return res + (order[: len(x)],) if return_order else res
 
 
 def kernel_launch_count() -> int:

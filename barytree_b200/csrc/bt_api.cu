@@ -25,6 +25,7 @@
 #include "bt_device.h"
 #include "bt_mixed.h"
 #include "bt_learned.h"
+#include "bt_gputree.h"
 #include "bt_host.h"
 
 namespace {
@@ -75,6 +76,7 @@ struct DeviceCtx {
     int device = -1;
     cudaStream_t stream = nullptr;
     Arena arena;
+    Arena tree_arena;       // particles in tree order (GPU tree build), kept through the call
     cudaEvent_t ev[8] = {};
     std::mutex mu;
 };
@@ -312,11 +314,94 @@ void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty,
     bt_plan_lists(&pl);
 }
 
+// Particles in tree order, resident on the device (GPU tree build).
+struct DevParts {
+    const double *sx = nullptr, *sy = nullptr, *sz = nullptr, *sq = nullptr;
+    const double *tx = nullptr, *ty = nullptr, *tz = nullptr;
+    const int *order = nullptr;     // target permutation
+};
+
+// Whether two host arrays hold the same bits (parallel compare).
+bool same_host(const double *a, const double *b, size_t n)
+{
+    if (a == b) return true;
+    const size_t CH = 1 << 16;
+    const long nch = (long)((n + CH - 1) / CH);
+    int diff = 0;
+#pragma omp parallel for schedule(static) reduction(| : diff)
+    for (long c = 0; c < nch; c++) {
+        size_t b0 = (size_t)c * CH, len = std::min(CH, n - b0);
+        diff |= memcmp(a + b0, b + b0, sizeof(double) * len) != 0;
+    }
+    return !diff;
+}
+
+// The plan with both trees built on the GPU: the same trees and particle
+// order as build_plan, the sorted particles kept in ctx->tree_arena.
+int build_plan_gpu(DeviceCtx *ctx, bt_plan &pl, int nt, int ns, const double *tx, const double *ty,
+                   const double *tz, const double *sx, const double *sy, const double *sz, const double *sq,
+                   bool inputs_on_device, DevParts &dp)
+{
+    cudaStream_t st = ctx->stream;
+    const bt_params &o = pl.prm;
+    long long launches = 0;
+    bool same = nt == ns && o.maxs == o.maxt;
+    if (same && !inputs_on_device)
+        same = same_host(tx, sx, (size_t)nt) && same_host(ty, sy, (size_t)nt) && same_host(tz, sz, (size_t)nt);
+    const bool check_on_device = same && inputs_on_device && !(tx == sx && ty == sy && tz == sz);
+    double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx = nullptr, *d_ty = nullptr, *d_tz = nullptr;
+    int *d_sord, *d_tord = nullptr;
+    unsigned long long *d_flag;
+    unsigned char *d_work;
+    const size_t wbytes = std::max(bt::gpu_tree_work_bytes(ns, o.maxs, true), bt::gpu_tree_work_bytes(nt, o.maxt, false));
+    Layout L;
+    L.add(&d_sx, ns); L.add(&d_sy, ns); L.add(&d_sz, ns); L.add(&d_sq, ns); L.add(&d_sord, ns);
+    L.add(&d_tx, nt); L.add(&d_ty, nt); L.add(&d_tz, nt); L.add(&d_tord, nt);
+    L.add(&d_flag, 1); L.add(&d_work, wbytes);
+    if (!ctx->tree_arena.reserve(L.total())) {
+        set_err("device allocation of %zu bytes for the tree build failed", L.total());
+        return BT_ERR_CUDA;
+    }
+    L.bind(ctx->tree_arena);
+    if (check_on_device) {
+        bool ex = false, ey = false, ez = false;
+        int e = bt::gpu_arrays_equal(tx, sx, (size_t)nt, d_flag, &ex, st);
+        if (!e) e = bt::gpu_arrays_equal(ty, sy, (size_t)nt, d_flag, &ey, st);
+        if (!e) e = bt::gpu_arrays_equal(tz, sz, (size_t)nt, d_flag, &ez, st);
+        if (e) { set_err("CUDA error %s in the coordinate comparison", cudaGetErrorString((cudaError_t)e)); return BT_ERR_CUDA; }
+        launches += 3;
+        same = ex && ey && ez;
+    }
+    bt::GtArrays sa{d_sx, d_sy, d_sz, d_sq, d_sord};
+    int e = bt::gpu_build_tree(ns, sx, sy, sz, sq, o.maxs, sa, d_work, wbytes, &pl.st, st, &launches);
+    if (!e && !same) {
+        bt::GtArrays ta{d_tx, d_ty, d_tz, nullptr, d_tord};
+        e = bt::gpu_build_tree(nt, tx, ty, tz, nullptr, o.maxt, ta, d_work, wbytes, &pl.tt, st, &launches);
+    }
+    g_launches += launches;
+    if (e) {
+        set_err("CUDA error %s in the tree build", cudaGetErrorString((cudaError_t)e));
+        return BT_ERR_CUDA;
+    }
+    pl.src.n = ns;
+    pl.tgt.n = nt;
+    dp.sx = d_sx; dp.sy = d_sy; dp.sz = d_sz; dp.sq = d_sq;
+    if (same) {
+        bt_tree_copy(&pl.tt, &pl.st);
+        dp.tx = d_sx; dp.ty = d_sy; dp.tz = d_sz; dp.order = d_sord;
+    } else {
+        dp.tx = d_tx; dp.ty = d_ty; dp.tz = d_tz; dp.order = d_tord;
+    }
+    bt_plan_lists(&pl);
+    return BT_OK;
+}
+
 // Device evaluation of a built plan; writes potentials in caller order to out_host.
-int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on_device, bt_report *rep)
+int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on_device, bt_report *rep,
+             const DevParts *dp = nullptr)
 {
     const bt_params &o = pl.prm;
-    const int n = o.degree, np1 = n + 1, P = o.P;
+    const int n = o.degree, P = o.P;
     const bool herm = o.approx == HERMITE;
     const int nq = herm ? 8 : 1;
     const bt_tree &S = pl.st, &T = pl.tt;
@@ -384,8 +469,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     }
     // mixed precision: Lagrange only (Hermite evaluates in FP64); node
     // centres, leaf-expanded near-field / CP lists, and per near-field entry
-    // whether the two leaves' boxes overlap (only then can a target coincide
-    // with a source, so only then is the skipping test evaluated)
+    // whether the two leaves' boxes lie within the close-pair distance (only
+    // then can a pair be close, or a target coincide with a source)
     std::vector<double> sctr, tctr;
     std::vector<int64_t> mx_doff, mx_cpoff;
     std::vector<int> mx_didx, mx_cpidx;
@@ -404,9 +489,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             int t = T.leaves[u];
             for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) {
                 int s = mx_didx[k];
-                bool ov = T.x0[t] <= S.x1[s] && S.x0[s] <= T.x1[t] && T.y0[t] <= S.y1[s] && S.y0[s] <= T.y1[t] &&
-                          T.z0[t] <= S.z1[s] && S.z0[s] <= T.z1[t];
-                mx_dflag[k] = ov ? 1 : 0;
+                double gx = std::max(0.0, std::max(S.x0[s] - T.x1[t], T.x0[t] - S.x1[s]));
+                double gy = std::max(0.0, std::max(S.y0[s] - T.y1[t], T.y0[t] - S.y1[s]));
+                double gz = std::max(0.0, std::max(S.z0[s] - T.z1[t], T.z0[t] - S.z1[s]));
+                double rr = bt::MX_CLOSE_FRAC * (T.rad[t] + S.rad[s]);
+                mx_dflag[k] = gx * gx + gy * gy + gz * gz <= 1.0625 * rr * rr ? 1 : 0;
             }
         }
     }
@@ -422,8 +509,14 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     int *d_order;
     double *d_out;
     Layout L;
-    L.add(&d_sx, ns); L.add(&d_sy, ns); L.add(&d_sz, ns); L.add(&d_sq, ns);
-    L.add(&d_tx, nt); L.add(&d_ty, nt); L.add(&d_tz, nt); L.add(&d_pot, nt);
+    if (dp) {
+        d_sx = (double *)dp->sx; d_sy = (double *)dp->sy; d_sz = (double *)dp->sz; d_sq = (double *)dp->sq;
+        d_tx = (double *)dp->tx; d_ty = (double *)dp->ty; d_tz = (double *)dp->tz; d_order = (int *)dp->order;
+    } else {
+        L.add(&d_sx, ns); L.add(&d_sy, ns); L.add(&d_sz, ns); L.add(&d_sq, ns);
+        L.add(&d_tx, nt); L.add(&d_ty, nt); L.add(&d_tz, nt); L.add(&d_order, nt);
+    }
+    L.add(&d_pot, nt);
     L.add(&d_sgrid, sgrid.size()); L.add(&d_tgrid, tgrid.size());
     L.add(&d_slen, slen.size()); L.add(&d_tlen, tlen.size()); L.add(&d_ww, BT_MAX_DEGREE + 1);
     if (need_src_clusters) L.add(&d_Q, (size_t)S.n * P * nq);
@@ -437,7 +530,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     L.add(&d_ccoff, pl.g_cc.rows + 1); L.add(&d_ccidx, pl.g_cc.off[pl.g_cc.rows]);
     L.add(&d_cpoff, pl.g_cp.rows + 1); L.add(&d_cpidx, pl.g_cp.off[pl.g_cp.rows]);
     L.add(&d_evitems, ev_items.size()); L.add(&d_griditems, grid_items.size()); L.add(&d_l2pitems, l2p_items.size());
-    L.add(&d_order, nt); L.add(&d_out, nt);
+    L.add(&d_out, nt);
     float4 *d_spos = nullptr, *d_tpos = nullptr;
     float *d_Q32 = nullptr;
     double *d_sctr = nullptr, *d_tctr = nullptr;
@@ -477,8 +570,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     {
 #define UP(dst, src, cnt)                                                                              \
     if ((cnt) > 0) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
-        UP(d_sx, pl.src.x, ns); UP(d_sy, pl.src.y, ns); UP(d_sz, pl.src.z, ns); UP(d_sq, pl.src.q, ns);
-        UP(d_tx, pl.tgt.x, nt); UP(d_ty, pl.tgt.y, nt); UP(d_tz, pl.tgt.z, nt);
+        if (!dp) {
+            UP(d_sx, pl.src.x, ns); UP(d_sy, pl.src.y, ns); UP(d_sz, pl.src.z, ns); UP(d_sq, pl.src.q, ns);
+            UP(d_tx, pl.tgt.x, nt); UP(d_ty, pl.tgt.y, nt); UP(d_tz, pl.tgt.z, nt);
+            UP(d_order, pl.tgt.order, nt);
+        }
         UP(d_sgrid, sgrid.data(), sgrid.size()); UP(d_tgrid, tgrid.data(), tgrid.size());
         UP(d_slen, slen.data(), slen.size()); UP(d_tlen, tlen.data(), tlen.size());
         UP(d_ww, ww, n + 1);
@@ -495,7 +591,6 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         UP(d_evitems, ev_items.data(), ev_items.size());
         UP(d_griditems, grid_items.data(), grid_items.size());
         UP(d_l2pitems, l2p_items.data(), l2p_items.size());
-        UP(d_order, pl.tgt.order, nt);
         if (mixed) {
             UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
@@ -582,7 +677,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.d_flag = d_mxdflag; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
             a.spos = d_spos; a.kc = bt::mixed_kernel_constant(o.kernel, o.kp); a.pot = d_pot;
             a.t_rad = d_trad; a.s_rad = d_srad;
-            a.tx64 = d_tx; a.ty64 = d_ty; a.tz64 = d_tz; a.sx64 = d_sx; a.sy64 = d_sy; a.sz64 = d_sz;
+            a.tx64 = d_tx; a.ty64 = d_ty; a.tz64 = d_tz; a.sx64 = d_sx; a.sy64 = d_sy; a.sz64 = d_sz; a.sq64 = d_sq;
+            a.kp = o.kp;
             bt::launch_eval_targets_mixed(o.kernel, a, st);
             launches++;
         } else if (nt > 0) {
@@ -663,7 +759,7 @@ void node_geometry(const bt_tree &t, std::vector<double> &ctr, std::vector<doubl
 // Predict the error of every particle-cluster entry at every degree, choose
 // the lowest degree under the budget (or direct evaluation), and rewrite the
 // plan's target-leaf lists accordingly.
-int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol)
+int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const DevParts *dp = nullptr)
 {
     std::vector<float> w;
     {
@@ -690,7 +786,9 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol)
         float *d_feat, *d_w, *d_act, *d_pred;
         unsigned char *d_choice;
         Layout L;
-        L.add(&d_sq, pl.src.n); L.add(&d_mom, 2 * (size_t)S.n); L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
+        if (dp) d_sq = (double *)dp->sq;
+        else L.add(&d_sq, pl.src.n);
+        L.add(&d_mom, 2 * (size_t)S.n); L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
         L.add(&d_srad, srad.size()); L.add(&d_trad, trad.size()); L.add(&d_sibeg, S.n); L.add(&d_snum, S.n);
         L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
         L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size()); L.add(&d_act, 3 * (size_t)CH * bt::MLP_H);
@@ -703,7 +801,8 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol)
         L.bind(arena);
         {
 #define UP(dst, src, cnt) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
-            UP(d_sq, pl.src.q, pl.src.n); UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
+            if (!dp) UP(d_sq, pl.src.q, pl.src.n);
+            UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_srad, srad.data(), srad.size()); UP(d_trad, trad.data(), trad.size());
             UP(d_sibeg, S.ibeg, S.n); UP(d_snum, S.numpar, S.n); UP(d_tnum, T.numpar, T.n);
             UP(d_idx, pl.t_approx.idx, ne); UP(d_unit, T.leaves, T.nleaves);
@@ -844,6 +943,10 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         set_err("invalid degree policy %d", opts->degree_policy);
         return BT_ERR_PARAM;
     }
+    if (opts && opts->tree_build != BT_TREE_GPU && opts->tree_build != BT_TREE_HOST) {
+        set_err("invalid tree build %d", opts->tree_build);
+        return BT_ERR_PARAM;
+    }
     if (learned && (prm.precision != BT_PRECISION_MIXED || prm.ctype != PARTICLE_CLUSTER || prm.approx != LAGRANGE ||
                     prm.kernel != COULOMB)) {
         set_err("learned degree selection is provided for mixed precision, particle-cluster, Lagrange, Coulomb");
@@ -861,30 +964,41 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
     }
     double t0 = now_ms();
     const bool on_dev = opts && opts->inputs_on_device;
-    std::vector<double> hbuf;
-    if (on_dev) {
-        // Device-resident inputs: the host builds the tree, so bring the
-        // coordinates over once.
-        hbuf.resize((size_t)3 * nt + 4 * (size_t)ns);
-        const double *src[7] = {tx, ty, tz, sx, sy, sz, sq};
-        size_t cnt[7] = {(size_t)nt, (size_t)nt, (size_t)nt, (size_t)ns, (size_t)ns, (size_t)ns, (size_t)ns};
-        double *dst = hbuf.data();
-        const double *hp[7];
-        for (int k = 0; k < 7; k++) {
-            if (cudaMemcpyAsync(dst, src[k], sizeof(double) * cnt[k], cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) {
-                set_err("copy of device inputs failed");
-                return BT_ERR_CUDA;
-            }
-            hp[k] = dst;
-            dst += cnt[k];
-        }
-        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { set_err("copy of device inputs failed"); return BT_ERR_CUDA; }
-        tx = hp[0]; ty = hp[1]; tz = hp[2]; sx = hp[3]; sy = hp[4]; sz = hp[5]; sq = hp[6];
-    }
+    const bool gpu_tree = !use_static_scratch && !(opts && opts->tree_build == BT_TREE_HOST);
     bt_plan pl;
     memset(&pl, 0, sizeof pl);
     pl.prm = prm;
-    build_plan(pl, nt, ns, tx, ty, tz, sx, sy, sz, sq);
+    DevParts dp;
+    if (gpu_tree) {
+        rc = build_plan_gpu(ctx, pl, nt, ns, tx, ty, tz, sx, sy, sz, sq, on_dev, dp);
+        if (rc != BT_OK) {
+            bt_plan_free(&pl);
+            return rc;
+        }
+    } else {
+        std::vector<double> hbuf;
+        if (on_dev) {
+            // Device-resident inputs with the host tree build: bring the
+            // coordinates over once.
+            hbuf.resize((size_t)3 * nt + 4 * (size_t)ns);
+            const double *src[7] = {tx, ty, tz, sx, sy, sz, sq};
+            size_t cnt[7] = {(size_t)nt, (size_t)nt, (size_t)nt, (size_t)ns, (size_t)ns, (size_t)ns, (size_t)ns};
+            double *dst = hbuf.data();
+            const double *hp[7];
+            for (int k = 0; k < 7; k++) {
+                if (cudaMemcpyAsync(dst, src[k], sizeof(double) * cnt[k], cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) {
+                    set_err("copy of device inputs failed");
+                    return BT_ERR_CUDA;
+                }
+                hp[k] = dst;
+                dst += cnt[k];
+            }
+            if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { set_err("copy of device inputs failed"); return BT_ERR_CUDA; }
+            tx = hp[0]; ty = hp[1]; tz = hp[2]; sx = hp[3]; sy = hp[4]; sz = hp[5]; sq = hp[6];
+        }
+        build_plan(pl, nt, ns, tx, ty, tz, sx, sy, sz, sq);
+    }
+    const DevParts *dpp = gpu_tree ? &dp : nullptr;
     double t1 = now_ms();
     if (rep) {
         rep->ms_setup = t1 - t0;
@@ -892,7 +1006,7 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         count_interactions(pl, rep);
     }
     if (learned) {
-        rc = select_degrees(ctx, *arena, pl, tol);
+        rc = select_degrees(ctx, *arena, pl, tol, dpp);
         if (rc != BT_OK) {
             bt_plan_free(&pl);
             return rc;
@@ -902,7 +1016,7 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
             rep->ms_setup = now_ms() - t0;
         }
     }
-    rc = run_plan(ctx, *arena, pl, out, on_dev, rep);
+    rc = run_plan(ctx, *arena, pl, out, on_dev, rep, dpp);
     bt_plan_free(&pl);
     if (rc != BT_OK && !on_dev) memset(out, 0, sizeof(double) * (size_t)nt);
     return rc;
@@ -1342,10 +1456,49 @@ done:
 
 int bt_tree_dump(int n, const double *x, const double *y, const double *z, int maxparnode, int *ints, double *dbl, int cap)
 {
+    return bt_tree_dump_ex(n, x, y, z, maxparnode, BT_TREE_HOST, 0, ints, dbl, nullptr, cap);
+}
+
+int bt_tree_dump_ex(int n, const double *x, const double *y, const double *z, int maxparnode, int tree_build,
+                    int device, int *ints, double *dbl, int *order, int cap)
+{
+    g_err[0] = 0;
+    if (n < 0 || maxparnode < 1 || (n > 0 && (!x || !y || !z)) || (tree_build != BT_TREE_GPU && tree_build != BT_TREE_HOST)) {
+        set_err("invalid tree arguments");
+        return -2;
+    }
     bt_parts p;
-    bt_parts_init(&p, n, x, y, z, nullptr);
+    memset(&p, 0, sizeof p);
     bt_tree t;
-    bt_tree_build(&t, &p, maxparnode);
+    if (tree_build == BT_TREE_HOST) {
+        bt_parts_init(&p, n, x, y, z, nullptr);
+        bt_tree_build(&t, &p, maxparnode);
+        if (order && n > 0) memcpy(order, p.order, sizeof(int) * (size_t)n);
+    } else {
+        DeviceCtx *ctx = nullptr;
+        if (get_ctx(device, &ctx) != BT_OK) return -2;
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaStream_t st = ctx->stream;
+        double *d_x, *d_y, *d_z;
+        int *d_ord;
+        unsigned char *d_work;
+        const size_t wbytes = bt::gpu_tree_work_bytes(n, maxparnode, false);
+        Layout L;
+        L.add(&d_x, n); L.add(&d_y, n); L.add(&d_z, n); L.add(&d_ord, n); L.add(&d_work, wbytes);
+        if (!ctx->tree_arena.reserve(L.total())) { set_err("device allocation failed"); return -2; }
+        L.bind(ctx->tree_arena);
+        long long launches = 0;
+        int e = bt::gpu_build_tree(n, x, y, z, nullptr, maxparnode, bt::GtArrays{d_x, d_y, d_z, nullptr, d_ord}, d_work,
+                                   wbytes, &t, st, &launches);
+        if (!e && order && n > 0) e = (int)cudaMemcpyAsync(order, d_ord, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st);
+        if (!e) e = (int)cudaStreamSynchronize(st);
+        g_launches += launches;
+        if (e) {
+            set_err("CUDA error %s in the tree build", cudaGetErrorString((cudaError_t)e));
+            bt_tree_free(&t);
+            return -2;
+        }
+    }
     int nn = t.n;
     if (nn <= cap) {
         for (int i = 0; i < nn; i++) {

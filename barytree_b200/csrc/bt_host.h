@@ -78,6 +78,10 @@ void bt_parts_free(bt_parts *p);
 void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode);
 void bt_tree_free(bt_tree *t);
 void bt_tree_copy(bt_tree *dst, const bt_tree *src);
+/* Node arrays for n nodes (n, cap set), and the leaf / per-level lists of a
+ * tree whose node arrays and max_depth are filled. */
+void bt_tree_alloc(bt_tree *t, int n);
+void bt_tree_finish(bt_tree *t);
 
 /* bt_lists.c */
 void bt_csr_free(bt_csr *c);

@@ -22,6 +22,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "bt_kernels.cuh"
 #include "bt_mixed.h"
 
 namespace bt {
@@ -58,17 +59,6 @@ __device__ __forceinline__ float kf_far(float r2, float q, float kc)
     } else {
         return q * rsqrt_apx(r2 + kc);
     }
-}
-
-// Near-field pair with the reference's skipping rule (r^2 <= DBL_MIN for
-// Coulomb, r <= DBL_MIN for Yukawa; the regularised kernel never skips).  In
-// FP32 a coincident pair gives r2 == 0 exactly.
-template <int KT, bool SKIP>
-__device__ __forceinline__ float kf_pp(float r2, float q, float kc)
-{
-    float v = kf_far<KT>(r2, q, kc);
-    if (SKIP && KT != 3) v = r2 > 0.0f ? v : 0.0f;
-    return v;
 }
 
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
@@ -140,36 +130,70 @@ __device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, con
     for (int t = 0; t < NT; t++) out[t] = 0.f;
 }
 
-// Near-field tile.  FP32 leaf-relative coordinates carry an absolute error of
-// about 6e-8 of the leaf size, which is a large relative error for a pair
-// much closer than the leaf size (and such a pair dominates its target's
-// potential).  A pair closer than a twentieth of the two leaves' summed radii
-// therefore has its displacement recomputed from the FP64 coordinates before
-// the FP32 kernel evaluation.  Such pairs are rare (about 1e-5 of the near
-// field for uniform leaves), so the branch costs one compare; the pairs left
-// in FP32 carry at most about 2e-6 relative error each, which averages to
-// ~1e-7 relative in the potentials.
-template <int KT, bool SKIP>
-__device__ __forceinline__ void pp_tile(const float4 *tile, int cm, const float *x, const float *y, const float *z,
-                                        float kc, float thr2, const double *xd, const double *yd, const double *zd,
-                                        const double *__restrict__ sx, const double *__restrict__ sy,
-                                        const double *__restrict__ sz, int base, float *s)
+// Near-field tiles.  FP32 leaf-relative coordinates carry an absolute error
+// of about 6e-8 of the leaf size, a large relative error for a pair much
+// closer than the leaf size, and such a pair dominates its target's
+// potential.  Pairs closer than MX_CLOSE_FRAC of the two leaves' summed
+// radii ("close pairs") are therefore left out of the FP32 sums and added in
+// FP64 from the FP64 coordinates and charges, straight into the FP64
+// per-target accumulator (an FP32 sum would also round every later term at
+// the close pair's magnitude).  Close pairs occur only between leaves whose
+// boxes lie within that distance (flagged per near-field entry); the other
+// entries run pp_tile_far with no test at all.
+__device__ __forceinline__ float pair_r2(float x, float y, float z, float4 p)
+{
+    float dx = x - p.x, dy = y - p.y, dz = z - p.z;
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+template <int KT>
+__device__ __forceinline__ void pp_tile_far(const float4 *tile, int cm, const float *x, const float *y,
+                                            const float *z, float kc, float *s)
+{
+#pragma unroll 4
+    for (int i = 0; i < cm; i++) {
+        float4 p = tile[i];
+#pragma unroll
+        for (int t = 0; t < MX_TPT; t++) s[t] += kf_far<KT>(pair_r2(x[t], y[t], z[t], p), p.w, kc);
+    }
+}
+
+// Tile of a flagged entry: FP32 sum over the pairs at or beyond the close
+// distance (which also drops coincident pairs, r2 == 0); mn = smallest r2.
+template <int KT>
+__device__ __forceinline__ void pp_tile_near(const float4 *tile, int cm, const float *x, const float *y,
+                                             const float *z, float kc, float thr2, float *s, float *mn)
 {
 #pragma unroll 4
     for (int i = 0; i < cm; i++) {
         float4 p = tile[i];
 #pragma unroll
         for (int t = 0; t < MX_TPT; t++) {
-            float dx = x[t] - p.x, dy = y[t] - p.y, dz = z[t] - p.z;
-            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            if (r2 < thr2) {
-                const int gi = base + i;
-                float fx = (float)(xd[t] - sx[gi]), fy = (float)(yd[t] - sy[gi]), fz = (float)(zd[t] - sz[gi]);
-                r2 = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
-            }
-            s[t] += kf_pp<KT, SKIP>(r2, p.w, kc);
+            float r2 = pair_r2(x[t], y[t], z[t], p);
+            mn[t] = fminf(mn[t], r2);
+            float v = kf_far<KT>(r2, p.w, kc);
+            s[t] += r2 >= thr2 ? v : 0.0f;
         }
     }
+}
+
+// The close pairs of one target in a tile, in FP64 with the reference's
+// skipping rule (k_pp).  The same FP32 test as pp_tile_near selects them.
+template <int KT>
+__device__ __forceinline__ double pp_close_fp64(const float4 *tile, int cm, float x, float y, float z, float thr2,
+                                             double xd, double yd, double zd, const double *__restrict__ sx,
+                                             const double *__restrict__ sy, const double *__restrict__ sz,
+                                             const double *__restrict__ sq, int base, double kp)
+{
+    double acc = 0.0;
+    for (int i = 0; i < cm; i++) {
+        if (pair_r2(x, y, z, tile[i]) < thr2) {
+            const int gi = base + i;
+            double dx = xd - sx[gi], dy = yd - sy[gi], dz = zd - sz[gi];
+            acc += k_pp<KT>(dx * dx + dy * dy + dz * dz, sq[gi], kp);
+        }
+    }
+    return acc;
 }
 
 // Particle-output evaluation, mixed precision.  Each thread owns MX_TPT
@@ -184,7 +208,6 @@ k_eval_targets_mixed(MixedTargetsArgs a)
     const int tnode = a.leaf_node[u];
     const int tb = a.t_ibeg[tnode], tn = a.t_numpar[tnode];
     float x[MX_TPT], y[MX_TPT], z[MX_TPT];
-    double xd[MX_TPT], yd[MX_TPT], zd[MX_TPT];
     bool act[MX_TPT];
     int tid[MX_TPT];
 #pragma unroll
@@ -194,7 +217,6 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         tid[t] = tb + (act[t] ? ti : 0);
         float4 tp = a.tpos[tid[t]];
         x[t] = tp.x; y[t] = tp.y; z[t] = tp.z;
-        xd[t] = a.tx64[tid[t]]; yd[t] = a.ty64[tid[t]]; zd[t] = a.tz64[tid[t]];
     }
     const double trad = a.t_rad[tnode];
     const double cx = a.t_ctr[3 * tnode], cy = a.t_ctr[3 * tnode + 1], cz = a.t_ctr[3 * tnode + 2];
@@ -229,14 +251,14 @@ k_eval_targets_mixed(MixedTargetsArgs a)
     float4 *tile = reinterpret_cast<float4 *>(smf);
     for (int64_t e = a.d_off[u]; e < a.d_off[u + 1]; e++) {
         const int s = a.d_idx[e];
-        const bool skip = a.d_flag[e] != 0;
+        const bool near = a.d_flag[e] != 0;
         const int sb = a.s_ibeg[s], sn = a.s_numpar[s];
         const float ox = (float)(a.s_ctr[3 * s] - cx), oy = (float)(a.s_ctr[3 * s + 1] - cy),
                     oz = (float)(a.s_ctr[3 * s + 2] - cz);
         float xs[MX_TPT], ys[MX_TPT], zs[MX_TPT];   // targets in the source leaf's frame
 #pragma unroll
         for (int t = 0; t < MX_TPT; t++) { xs[t] = x[t] - ox; ys[t] = y[t] - oy; zs[t] = z[t] - oz; }
-        const double rr = 0.05 * (trad + a.s_rad[s]);
+        const double rr = MX_CLOSE_FRAC * (trad + a.s_rad[s]);
         const float thr2 = (float)(rr * rr);
         for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
             int cm = min(MX_TILE, sn - c0);
@@ -245,10 +267,25 @@ k_eval_targets_mixed(MixedTargetsArgs a)
             float sum[MX_TPT];
 #pragma unroll
             for (int t = 0; t < MX_TPT; t++) sum[t] = 0.f;
-            if (skip)
-                pp_tile<KT, true>(tile, cm, xs, ys, zs, kc, thr2, xd, yd, zd, a.sx64, a.sy64, a.sz64, sb + c0, sum);
-            else
-                pp_tile<KT, false>(tile, cm, xs, ys, zs, kc, thr2, xd, yd, zd, a.sx64, a.sy64, a.sz64, sb + c0, sum);
+            if (near) {
+                float mn[MX_TPT];
+#pragma unroll
+                for (int t = 0; t < MX_TPT; t++) mn[t] = FLT_MAX;
+                pp_tile_near<KT>(tile, cm, xs, ys, zs, kc, thr2, sum, mn);
+                bool close = false;
+#pragma unroll
+                for (int t = 0; t < MX_TPT; t++) close |= act[t] && mn[t] < thr2;
+                if (__any_sync(0xffffffffu, close)) {
+#pragma unroll
+                    for (int t = 0; t < MX_TPT; t++)
+                        if (act[t] && mn[t] < thr2)
+                            acc[t] += pp_close_fp64<KT>(tile, cm, xs[t], ys[t], zs[t], thr2, a.tx64[tid[t]],
+                                                        a.ty64[tid[t]], a.tz64[tid[t]], a.sx64, a.sy64, a.sz64,
+                                                        a.sq64, sb + c0, a.kp);
+                }
+            } else {
+                pp_tile_far<KT>(tile, cm, xs, ys, zs, kc, sum);
+            }
 #pragma unroll
             for (int t = 0; t < MX_TPT; t++) acc[t] += (double)sum[t];
             __syncthreads();

@@ -8,6 +8,13 @@ namespace bt {
 
 constexpr int MX_MAX_DEG = 12;
 
+// Near-field pairs closer than this fraction of the two leaves' summed radii
+// are evaluated in FP64 (the rest of the mixed near field is FP32).
+#ifndef BT_CLOSE_FRAC
+#define BT_CLOSE_FRAC 0.01
+#endif
+constexpr double MX_CLOSE_FRAC = BT_CLOSE_FRAC;
+
 struct MixedTargetsArgs {
     int n, max_np1, nitems;
     const int2 *items;
@@ -19,14 +26,15 @@ struct MixedTargetsArgs {
     const double *s_grid[MX_MAX_DEG + 1];       // per degree: node grids (FP64)
     const float *Q32[MX_MAX_DEG + 1];           // per degree: proxy charges (FP32)
     const int64_t *d_off; const int *d_idx;     // source leaves per target leaf
-    const unsigned char *d_flag;                // 1: boxes overlap, apply the coincidence skip
+    const unsigned char *d_flag;                // 1: leaf boxes within the close-pair distance
     const int *s_ibeg, *s_numpar;
     const double *s_ctr;                        // source node centres
     const float4 *spos;                         // sources relative to their leaf centre, with charge
     const double *t_rad, *s_rad;                // node radii (close-pair threshold)
-    const double *tx64, *ty64, *tz64;           // FP64 coordinates for close pairs
-    const double *sx64, *sy64, *sz64;
+    const double *tx64, *ty64, *tz64;           // FP64 coordinates and charges for close pairs
+    const double *sx64, *sy64, *sz64, *sq64;
     double kc;                                  // mixed_kernel_constant()
+    double kp;                                  // kernel parameter (FP64 close pairs)
     double *pot;
 };
 

@@ -294,6 +294,38 @@ static int preorder(const bnode *nodes, int i, int next, int *pre)
     return next;
 }
 
+void bt_tree_alloc(bt_tree *t, int n)
+{
+    t->cap = 0;
+    t->n = 0;
+    while (t->cap < n) {
+        t->n = t->cap;          /* tree_grow grows when the arrays are full */
+        tree_grow(t);
+    }
+    t->n = n;
+}
+
+void bt_tree_finish(bt_tree *t)
+{
+    /* leaves and per-level non-leaf lists, DFS order (src/tree/tree.c:122-153) */
+    int nleaf = 0;
+    int *lvl_cnt = calloc((size_t)t->max_depth + 1, sizeof(int));
+    for (int i = 0; i < t->n; i++) {
+        if (t->nchild[i] == 0) nleaf++;
+        else lvl_cnt[t->level[i]]++;
+    }
+    t->nleaves = nleaf;
+    t->leaves = malloc(sizeof(int) * (size_t)(nleaf > 0 ? nleaf : 1));
+    t->lvl_off = malloc(sizeof(int) * (size_t)(t->max_depth + 1));
+    t->lvl_off[0] = 0;
+    for (int l = 0; l < t->max_depth; l++) t->lvl_off[l + 1] = t->lvl_off[l] + lvl_cnt[l];
+    t->lvl_nodes = malloc(sizeof(int) * (size_t)(t->lvl_off[t->max_depth] + 1));
+    memset(lvl_cnt, 0, sizeof(int) * (size_t)(t->max_depth + 1));
+    int nl = 0;
+    collect(t, 0, &nl, lvl_cnt);
+    free(lvl_cnt);
+}
+
 void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
 {
     memset(t, 0, sizeof(*t));
@@ -338,13 +370,7 @@ void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
     /* pre-order numbering (TreeLinkedList_SetIndex, src/tree/tree_linked_list.c:284-293) */
     int *pre = malloc(sizeof(int) * (size_t)n);
     preorder(nodes, 0, 0, pre);
-    t->cap = 0;
-    t->n = 0;
-    while (t->cap < n) {
-        t->n = t->cap;          /* tree_grow grows when the arrays are full */
-        tree_grow(t);
-    }
-    t->n = n;
+    bt_tree_alloc(t, n);
     t->max_depth = depth;
     for (int i = 0; i < n; i++) {
         const bnode *nd = &nodes[i];
@@ -362,23 +388,7 @@ void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
     free(pre);
     free(nodes);
 
-    /* leaves and per-level non-leaf lists, DFS order (src/tree/tree.c:122-153) */
-    int nleaf = 0;
-    int *lvl_cnt = calloc((size_t)t->max_depth + 1, sizeof(int));
-    for (int i = 0; i < t->n; i++) {
-        if (t->nchild[i] == 0) nleaf++;
-        else lvl_cnt[t->level[i]]++;
-    }
-    t->nleaves = nleaf;
-    t->leaves = malloc(sizeof(int) * (size_t)(nleaf > 0 ? nleaf : 1));
-    t->lvl_off = malloc(sizeof(int) * (size_t)(t->max_depth + 1));
-    t->lvl_off[0] = 0;
-    for (int l = 0; l < t->max_depth; l++) t->lvl_off[l + 1] = t->lvl_off[l] + lvl_cnt[l];
-    t->lvl_nodes = malloc(sizeof(int) * (size_t)(t->lvl_off[t->max_depth] + 1));
-    memset(lvl_cnt, 0, sizeof(int) * (size_t)(t->max_depth + 1));
-    int nl = 0;
-    collect(t, 0, &nl, lvl_cnt);
-    free(lvl_cnt);
+    bt_tree_finish(t);
 }
 
 void bt_tree_copy(bt_tree *dst, const bt_tree *src)

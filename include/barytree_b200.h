@@ -92,7 +92,11 @@ typedef struct bt_options {
     int device;           /* CUDA device ordinal                                      */
     int inputs_on_device; /* 1: the x,y,z,q pointers passed to bt_eval are device
                              pointers (FP64) and output is a device pointer          */
+    int tree_build;       /* BT_TREE_GPU (default) or BT_TREE_HOST: where the trees
+                             are built; both give the same trees and particle order  */
 } bt_options;
+
+enum { BT_TREE_GPU = 0, BT_TREE_HOST = 1 };
 
 /* Per-call report (all optional: pass NULL). */
 typedef struct bt_report {
@@ -179,6 +183,15 @@ long bt_lists(int numTargets, int numSources,
  * Mirrors Tree_Sources_Construct (src/tree/tree.c:19-59). */
 int bt_tree_dump(int n, const double *x, const double *y, const double *z, int maxparnode,
             int *ints, double *dbl, int cap);
+
+/* bt_tree_dump with the build location (BT_TREE_HOST / BT_TREE_GPU on
+ * `device`, inputs in host memory) and, if order is not NULL, the particle
+ * permutation (order[i] = input index of sorted particle i; n entries).
+ * Returns the node count, -1 if `cap` is too small, -2 on other errors
+ * (bt_last_error).  No counterpart in the reference: it checks that both
+ * builds give the reference's tree. */
+int bt_tree_dump_ex(int n, const double *x, const double *y, const double *z, int maxparnode,
+                    int tree_build, int device, int *ints, double *dbl, int *order, int cap);
 
 /* ---------------------------------------------------------------------- */
 /* Learned degree selection (no counterpart in the reference).              */

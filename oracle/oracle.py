@@ -186,3 +186,14 @@ def tree(x, y, z, maxpar):
 
 def ref_tree(x, y, z, maxpar):
     return _tree(reflists_lib().refl_tree, x, y, z, maxpar)
+
+
+def ref_tree_order(x, y, z, maxpar):
+    """The reference's particle permutation (0-based input index per sorted slot)."""
+    x, y, z = map(_c, (x, y, z))
+    L = reflists_lib()
+    L.refl_tree_order.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip)
+    L.refl_tree_order.restype = ctypes.c_int
+    order = np.zeros(max(1, len(x)), dtype=np.int32)
+    L.refl_tree_order(len(x), _p(x), _p(y), _p(z), int(maxpar), order.ctypes.data_as(_ip))
+    return order[: len(x)]

@@ -66,6 +66,24 @@ int refl_tree(int n, const double *x, const double *y, const double *z, int maxp
     return nn <= cap ? nn : -1;
 }
 
+/* The reference's particle permutation after its tree build: order[i] =
+ * 0-based input index of sorted particle i (Particles_ConstructOrder,
+ * src/particles/particles.c:138-144, permuted by the partition). */
+int refl_tree_order(int n, const double *x, const double *y, const double *z, int maxparnode, int *order)
+{
+    struct Particles *p = mkpart(n, x, y, z);
+    struct RunParams *rp = NULL;
+    RunParams_Setup(&rp, COULOMB, 0, NULL, LAGRANGE, SKIPPING, PARTICLE_CLUSTER,
+                    0.5, 1, maxparnode, maxparnode, 1.0, -1.0, 0);
+    struct Tree *t = NULL;
+    Tree_Sources_Construct(&t, p, rp);
+    for (int i = 0; i < n; i++) order[i] = p->order[i] - 1;
+    Tree_Free(&t);
+    RunParams_Free(&rp);
+    freepart(p);
+    return 0;
+}
+
 long refl_lists(int numTargets, int numSources,
                 const double *targetX, const double *targetY, const double *targetZ,
                 const double *sourceX, const double *sourceY, const double *sourceZ,

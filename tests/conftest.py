@@ -38,3 +38,12 @@ def uniform_inputs(seed, n, targets="same"):
 def golden_files():
     d = os.path.join(ROOT, "tests", "golden")
     return sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith(".npz"))
+
+
+def same_members(ints, order_a, order_b):
+    """Whether two particle permutations put the same particles in every
+    leaf of the tree summary `ints` (1-based ibeg, iend, children, level)."""
+    for b, e, nch, _ in ints:
+        if nch == 0 and not np.array_equal(np.sort(order_a[b - 1:e]), np.sort(order_b[b - 1:e])):
+            return False
+    return True

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import barytree_b200 as B
-from conftest import ROOT, golden_files, uniform_inputs
+from conftest import ROOT, golden_files, same_members, uniform_inputs
 from oracle import oracle as O
 
 
@@ -96,6 +96,19 @@ def test_tree_matches_reference_build():
     b_int, b_dbl = O.ref_tree(sx, sy, sz, 50)
     assert np.array_equal(a_int[:, :3], b_int[:, :3])    # ibeg, iend, children
     assert np.array_equal(a_dbl, b_dbl)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_tree_membership_matches_reference_build():
+    """Every node holds the same particles as in the reference's build.  The
+    order inside a node differs: the reference partitions in place by swaps
+    (src/tree/partition.c:14-120), the builds here keep input order."""
+    sx, sy, sz, _ = _clustered(8, 12000)
+    ints, _, order = B.tree_summary(sx, sy, sz, 50, return_order=True)
+    ref = O.ref_tree_order(sx, sy, sz, 50)
+    assert same_members(ints, order, ref)
+    leaf = ints[ints[:, 2] == 0]
+    assert all(np.array_equal(order[b - 1:e], np.sort(order[b - 1:e])) for b, e, _, _ in leaf)
 
 
 def _bti(**over):
