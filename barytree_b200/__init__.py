@@ -62,14 +62,17 @@ BT_OK, BT_ERR_PARAM, BT_ERR_UNSUPPORTED, BT_ERR_CUDA, BT_ERR_TIMEOUT, BT_ERR_NO_
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 DEGREE_FIXED, DEGREE_LEARNED = 0, 1
 TREE_GPU, TREE_HOST = 0, 1
+DISPATCH_AUTO, DISPATCH_QUEUE, DISPATCH_GRID = 0, 1, 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
+_llp = ctypes.POINTER(ctypes.c_longlong)
 
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("degree_policy", ctypes.c_int), ("tolerance", ctypes.c_double),
-                ("device", ctypes.c_int), ("inputs_on_device", ctypes.c_int), ("tree_build", ctypes.c_int)]
+                ("device", ctypes.c_int), ("inputs_on_device", ctypes.c_int), ("tree_build", ctypes.c_int),
+                ("dispatch", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):
@@ -106,7 +109,7 @@ _BTI_ARGS = (
 
 # every exported symbol of include/barytree_b200.h
 EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
-                    "bt_tree_dump", "bt_tree_dump_ex", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
+                    "bt_tree_dump", "bt_tree_dump_ex", "bt_eval_batch", "bt_session_create", "bt_session_eval", "bt_session_destroy", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
                     "bt_selector_nweights", "bt_selector_set", "bt_selector_training_data", "bt_selector_train",
                     "bt_mlp_loss_grad", "bt_mlp_predict")
 
@@ -139,6 +142,20 @@ def lib():
     L.bt_lists.restype = ctypes.c_long
     L.bt_tree_dump.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, ctypes.c_int)
     L.bt_tree_dump.restype = ctypes.c_int
+    L.bt_eval_batch.argtypes = (ctypes.c_int, _llp, _llp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                ctypes.POINTER(Options), ctypes.POINTER(Report))
+    L.bt_eval_batch.restype = ctypes.c_int
+    L.bt_session_create.argtypes = (ctypes.c_int, _llp, _llp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(Options),
+                                    ctypes.POINTER(ctypes.c_void_p))
+    L.bt_session_create.restype = ctypes.c_int
+    L.bt_session_eval.argtypes = (ctypes.c_void_p, _dp, _dp, ctypes.POINTER(Report))
+    L.bt_session_eval.restype = ctypes.c_int
+    L.bt_session_destroy.argtypes = (ctypes.c_void_p,)
+    L.bt_session_destroy.restype = ctypes.c_int
     L.bt_tree_dump_ex.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _dp,
                                   _ip, ctypes.c_int)
     L.bt_tree_dump_ex.restype = ctypes.c_int
@@ -227,11 +244,11 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
              approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER,
              theta=0.7, degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
              precision=PRECISION_FP64, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0,
-             tree_build=TREE_GPU, return_report=False):
+             tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, return_report=False):
     """Extended entry point (bt_eval): options for precision / degree policy / tree build and a report."""
     tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
     out = np.zeros(len(tx))
-    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, int(tree_build))
+    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, int(tree_build), int(dispatch))
     rep = Report()
     rc = lib().bt_eval(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
                        int(kernel), float(kernel_param), int(approximation), int(compute_type), float(theta),
@@ -241,15 +258,101 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
     return (out, rep.as_dict()) if return_report else out
 
 
+def treecode_batch(systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
+                   compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
+                   max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64, degree_policy=DEGREE_FIXED,
+                   tolerance=1e-6, device=0, tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, return_report=False):
+    """bt_eval_batch over a list of systems (tx, ty, tz, sx, sy, sz, sq); returns one potential array per system."""
+    systems = [tuple(map(_c, s)) for s in systems]
+    toff = np.concatenate([[0], np.cumsum([len(s[0]) for s in systems])]).astype(np.int64)
+    soff = np.concatenate([[0], np.cumsum([len(s[3]) for s in systems])]).astype(np.int64)
+    cat = [_c(np.concatenate([s[i] for s in systems]) if systems else np.zeros(0)) for i in range(7)]
+    out = np.zeros(int(toff[-1]))
+    rep = treecode_batch_ptr(len(systems), toff, soff, *(a.ctypes.data for a in cat), out.ctypes.data,
+                             kernel=kernel, kernel_param=kernel_param, approximation=approximation,
+                             compute_type=compute_type, theta=theta, degree=degree, max_source_leaf=max_source_leaf,
+                             max_target_leaf=max_target_leaf, size_check=size_check, precision=precision,
+                             degree_policy=degree_policy, tolerance=tolerance, device=device, tree_build=tree_build,
+                             dispatch=dispatch)
+    pots = [out[toff[k]:toff[k + 1]].copy() for k in range(len(systems))]
+    return (pots, rep) if return_report else pots
+
+
+def treecode_batch_ptr(nsys, target_offsets, source_offsets, tx, ty, tz, sx, sy, sz, sq, out,
+                       kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
+                       compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
+                       max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64, degree_policy=DEGREE_FIXED,
+                       tolerance=1e-6, device=0, inputs_on_device=False, tree_build=TREE_GPU,
+                       dispatch=DISPATCH_AUTO):
+    """bt_eval_batch on raw addresses; offsets are host int64 arrays of nsys+1 entries."""
+    cast = lambda a: ctypes.cast(ctypes.c_void_p(int(a)), _dp)  # noqa: E731
+    toff = np.ascontiguousarray(target_offsets, dtype=np.int64)
+    soff = np.ascontiguousarray(source_offsets, dtype=np.int64)
+    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), int(bool(inputs_on_device)),
+                   int(tree_build), int(dispatch))
+    rep = Report()
+    rc = lib().bt_eval_batch(int(nsys), toff.ctypes.data_as(_llp), soff.ctypes.data_as(_llp), cast(tx), cast(ty),
+                             cast(tz), cast(sx), cast(sy), cast(sz), cast(sq), cast(out), int(kernel),
+                             float(kernel_param), int(approximation), int(compute_type), float(theta), int(degree),
+                             int(max_source_leaf), int(max_target_leaf), float(size_check), ctypes.byref(opts),
+                             ctypes.byref(rep))
+    _check(rc)
+    return rep.as_dict()
+
+
+class Session:
+    """bt_session_*: trees, lists and the device sequence built once for fixed
+    particle positions; evaluate(charges) replays the captured CUDA graph.
+
+    systems: a list of (tx, ty, tz, sx, sy, sz, sq); sq are the charges used
+    for a learned degree selection (and need not be passed again)."""
+
+    def __init__(self, systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
+                 compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
+                 max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64, degree_policy=DEGREE_FIXED,
+                 tolerance=1e-6, device=0, dispatch=DISPATCH_AUTO):
+        systems = [tuple(map(_c, s)) for s in systems]
+        self.toff = np.concatenate([[0], np.cumsum([len(s[0]) for s in systems])]).astype(np.int64)
+        self.soff = np.concatenate([[0], np.cumsum([len(s[3]) for s in systems])]).astype(np.int64)
+        cat = [_c(np.concatenate([s[i] for s in systems])) for i in range(7)]
+        opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, TREE_GPU, int(dispatch))
+        h = ctypes.c_void_p()
+        rc = lib().bt_session_create(len(systems), self.toff.ctypes.data_as(_llp), self.soff.ctypes.data_as(_llp),
+                                     *(_p(a) for a in cat), int(kernel), float(kernel_param), int(approximation),
+                                     int(compute_type), float(theta), int(degree), int(max_source_leaf),
+                                     int(max_target_leaf), float(size_check), ctypes.byref(opts), ctypes.byref(h))
+        _check(rc)
+        self._h = h
+
+    def evaluate(self, charges, return_report=False):
+        """Potentials per system for new source charges (one array per system, or concatenated)."""
+        q = _c(np.concatenate(charges) if isinstance(charges, (list, tuple)) else charges)
+        if len(q) != self.soff[-1]:
+            raise BaryTreeError(BT_ERR_PARAM, f"expected {self.soff[-1]} charges, got {len(q)}")
+        out = np.zeros(int(self.toff[-1]))
+        rep = Report()
+        _check(lib().bt_session_eval(self._h, _p(q), _p(out), ctypes.byref(rep)))
+        pots = [out[self.toff[k]:self.toff[k + 1]].copy() for k in range(len(self.toff) - 1)]
+        return (pots, rep.as_dict()) if return_report else pots
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bt_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
 def treecode_ptr(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, kernel=Kernel.COULOMB, kernel_param=0.0,
                  approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7,
                  degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64,
                  degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0, inputs_on_device=False,
-                 tree_build=TREE_GPU):
+                 tree_build=TREE_GPU, dispatch=DISPATCH_AUTO):
     """bt_eval on raw addresses (ints): device pointers when inputs_on_device, else host pointers."""
     cast = lambda a: ctypes.cast(ctypes.c_void_p(int(a)), _dp)  # noqa: E731
     opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), int(bool(inputs_on_device)),
-                   int(tree_build))
+                   int(tree_build), int(dispatch))
     rep = Report()
     rc = lib().bt_eval(int(nt), int(ns), cast(tx), cast(ty), cast(tz), cast(sx), cast(sy), cast(sz), cast(sq),
                        cast(out), int(kernel), float(kernel_param), int(approximation), int(compute_type),

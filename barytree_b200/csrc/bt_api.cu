@@ -17,6 +17,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <climits>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -293,32 +294,13 @@ void expand_to_leaves(const bt_csr &in, const bt_tree &t, const std::vector<int>
 }
 
 // Build the host plan: copies, trees, lists.
-void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty, const double *tz,
-                const double *sx, const double *sy, const double *sz, const double *sq)
-{
-    bt_parts_init(&pl.src, ns, sx, sy, sz, sq);
-    bt_tree_build(&pl.st, &pl.src, pl.prm.maxs);
-    // Targets at exactly the source positions with the same leaf size give
-    // the same node sets (the build depends only on coordinates and leaf
-    // size), so the target tree and permutation are copies of the source's.
-    bool same = nt == ns && pl.prm.maxs == pl.prm.maxt && (tx == sx || !memcmp(tx, sx, sizeof(double) * nt)) &&
-                (ty == sy || !memcmp(ty, sy, sizeof(double) * nt)) && (tz == sz || !memcmp(tz, sz, sizeof(double) * nt));
-    if (same && nt > 0) {
-        bt_parts_init(&pl.tgt, nt, pl.src.x, pl.src.y, pl.src.z, nullptr);
-        memcpy(pl.tgt.order, pl.src.order, sizeof(int) * (size_t)nt);
-        bt_tree_copy(&pl.tt, &pl.st);
-    } else {
-        bt_parts_init(&pl.tgt, nt, tx, ty, tz, nullptr);
-        bt_tree_build(&pl.tt, &pl.tgt, pl.prm.maxt);
-    }
-    bt_plan_lists(&pl);
-}
-
-// Particles in tree order, resident on the device (GPU tree build).
-struct DevParts {
-    const double *sx = nullptr, *sy = nullptr, *sz = nullptr, *sq = nullptr;
-    const double *tx = nullptr, *ty = nullptr, *tz = nullptr;
-    const int *order = nullptr;     // target permutation
+// Systems of a call: nsys and the target / source offsets (a single system
+// unless the call is batched).
+struct Systems {
+    int n = 1;
+    std::vector<int64_t> toff, soff;
+    Systems(int nt, int ns) : toff{0, nt}, soff{0, ns} {}
+    Systems(int nsys, const long long *t, const long long *s) : n(nsys), toff(t, t + nsys + 1), soff(s, s + nsys + 1) {}
 };
 
 // Whether two host arrays hold the same bits (parallel compare).
@@ -336,16 +318,54 @@ bool same_host(const double *a, const double *b, size_t n)
     return !diff;
 }
 
+// Build the host plan: copies, trees, lists.
+void build_plan(bt_plan &pl, const Systems &sys, const double *tx, const double *ty, const double *tz,
+                const double *sx, const double *sy, const double *sz, const double *sq)
+{
+    const int nt = (int)sys.toff[sys.n], ns = (int)sys.soff[sys.n];
+    bt_parts_init(&pl.src, ns, sx, sy, sz, sq);
+    bt_forest_build(&pl.st, &pl.src, sys.n, sys.soff.data(), pl.prm.maxs);
+    // Targets at exactly the source positions with the same leaf size give
+    // the same node sets (the build depends only on coordinates and leaf
+    // size), so the target tree and permutation are copies of the source's.
+    bool same = sys.toff == sys.soff && pl.prm.maxs == pl.prm.maxt && same_host(tx, sx, (size_t)nt) &&
+                same_host(ty, sy, (size_t)nt) && same_host(tz, sz, (size_t)nt);
+    if (same && nt > 0) {
+        bt_parts_init(&pl.tgt, nt, pl.src.x, pl.src.y, pl.src.z, nullptr);
+        memcpy(pl.tgt.order, pl.src.order, sizeof(int) * (size_t)nt);
+        bt_tree_copy(&pl.tt, &pl.st);
+    } else {
+        bt_parts_init(&pl.tgt, nt, tx, ty, tz, nullptr);
+        bt_forest_build(&pl.tt, &pl.tgt, sys.n, sys.toff.data(), pl.prm.maxt);
+    }
+    bt_plan_lists(&pl);
+}
+
+void build_plan(bt_plan &pl, int nt, int ns, const double *tx, const double *ty, const double *tz,
+                const double *sx, const double *sy, const double *sz, const double *sq)
+{
+    build_plan(pl, Systems(nt, ns), tx, ty, tz, sx, sy, sz, sq);
+}
+
+// Particles in tree order, resident on the device (GPU tree build).
+struct DevParts {
+    const double *sx = nullptr, *sy = nullptr, *sz = nullptr, *sq = nullptr;
+    const double *tx = nullptr, *ty = nullptr, *tz = nullptr;
+    const int *order = nullptr;     // target permutation
+    const int *sorder = nullptr;    // source permutation
+};
+
 // The plan with both trees built on the GPU: the same trees and particle
-// order as build_plan, the sorted particles kept in ctx->tree_arena.
-int build_plan_gpu(DeviceCtx *ctx, bt_plan &pl, int nt, int ns, const double *tx, const double *ty,
-                   const double *tz, const double *sx, const double *sy, const double *sz, const double *sq,
-                   bool inputs_on_device, DevParts &dp)
+// order as build_plan, the sorted particles kept in `tarena`.
+int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sys, const double *tx,
+                   const double *ty, const double *tz, const double *sx, const double *sy, const double *sz,
+                   const double *sq, bool inputs_on_device, DevParts &dp)
 {
     cudaStream_t st = ctx->stream;
     const bt_params &o = pl.prm;
+    const int nt = (int)sys.toff[sys.n], ns = (int)sys.soff[sys.n];
     long long launches = 0;
-    bool same = nt == ns && o.maxs == o.maxt;
+    bool same = sys.toff == sys.soff && o.maxs == o.maxt;
     if (same && !inputs_on_device)
         same = same_host(tx, sx, (size_t)nt) && same_host(ty, sy, (size_t)nt) && same_host(tz, sz, (size_t)nt);
     const bool check_on_device = same && inputs_on_device && !(tx == sx && ty == sy && tz == sz);
@@ -353,16 +373,17 @@ int build_plan_gpu(DeviceCtx *ctx, bt_plan &pl, int nt, int ns, const double *tx
     int *d_sord, *d_tord = nullptr;
     unsigned long long *d_flag;
     unsigned char *d_work;
-    const size_t wbytes = std::max(bt::gpu_tree_work_bytes(ns, o.maxs, true), bt::gpu_tree_work_bytes(nt, o.maxt, false));
+    const size_t wbytes = std::max(bt::gpu_tree_work_bytes(ns, o.maxs, true, sys.n),
+                                   bt::gpu_tree_work_bytes(nt, o.maxt, false, sys.n));
     Layout L;
     L.add(&d_sx, ns); L.add(&d_sy, ns); L.add(&d_sz, ns); L.add(&d_sq, ns); L.add(&d_sord, ns);
     L.add(&d_tx, nt); L.add(&d_ty, nt); L.add(&d_tz, nt); L.add(&d_tord, nt);
     L.add(&d_flag, 1); L.add(&d_work, wbytes);
-    if (!ctx->tree_arena.reserve(L.total())) {
+    if (!tarena.reserve(L.total())) {
         set_err("device allocation of %zu bytes for the tree build failed", L.total());
         return BT_ERR_CUDA;
     }
-    L.bind(ctx->tree_arena);
+    L.bind(tarena);
     if (check_on_device) {
         bool ex = false, ey = false, ez = false;
         int e = bt::gpu_arrays_equal(tx, sx, (size_t)nt, d_flag, &ex, st);
@@ -373,10 +394,12 @@ int build_plan_gpu(DeviceCtx *ctx, bt_plan &pl, int nt, int ns, const double *tx
         same = ex && ey && ez;
     }
     bt::GtArrays sa{d_sx, d_sy, d_sz, d_sq, d_sord};
-    int e = bt::gpu_build_tree(ns, sx, sy, sz, sq, o.maxs, sa, d_work, wbytes, &pl.st, st, &launches);
+    int e = bt::gpu_build_forest(sys.n, sys.soff.data(), sx, sy, sz, sq, o.maxs, sa, d_work, wbytes, &pl.st, st,
+                                 &launches);
     if (!e && !same) {
         bt::GtArrays ta{d_tx, d_ty, d_tz, nullptr, d_tord};
-        e = bt::gpu_build_tree(nt, tx, ty, tz, nullptr, o.maxt, ta, d_work, wbytes, &pl.tt, st, &launches);
+        e = bt::gpu_build_forest(sys.n, sys.toff.data(), tx, ty, tz, nullptr, o.maxt, ta, d_work, wbytes, &pl.tt, st,
+                                 &launches);
     }
     g_launches += launches;
     if (e) {
@@ -385,7 +408,7 @@ int build_plan_gpu(DeviceCtx *ctx, bt_plan &pl, int nt, int ns, const double *tx
     }
     pl.src.n = ns;
     pl.tgt.n = nt;
-    dp.sx = d_sx; dp.sy = d_sy; dp.sz = d_sz; dp.sq = d_sq;
+    dp.sx = d_sx; dp.sy = d_sy; dp.sz = d_sz; dp.sq = d_sq; dp.sorder = d_sord;
     if (same) {
         bt_tree_copy(&pl.tt, &pl.st);
         dp.tx = d_sx; dp.ty = d_sy; dp.tz = d_sz; dp.order = d_sord;
@@ -396,9 +419,219 @@ int build_plan_gpu(DeviceCtx *ctx, bt_plan &pl, int nt, int ns, const double *tx
     return BT_OK;
 }
 
+// Everything the device sequence of one evaluation needs: the device arrays
+// of a prepared plan and the few host-side sizes that shape the launches.
+struct DevPlan {
+    bool mixed = false, herm = false, need_src_clusters = false, need_tgt_grids = false;
+    bool queue = false;     // mixed kernels on a device work queue
+    int n = 0, P = 0, ns = 0, nt = 0, max_np1 = 0, kernel = 0;
+    double kp = 0.0;
+    int S_n = 0, S_nleaves = 0, S_max_depth = 0, T_n = 0, T_nleaves = 0, T_max_depth = 0;
+    std::vector<int> S_lvl_off, T_lvl_off, xdeg;
+    int n_grid_items = 0, n_ev_items = 0, n_l2p_items = 0;
+    double *d_sx = nullptr, *d_sy = nullptr, *d_sz = nullptr, *d_sq = nullptr, *d_tx = nullptr, *d_ty = nullptr, *d_tz = nullptr, *d_pot = nullptr, *d_sgrid = nullptr, *d_tgrid = nullptr, *d_slen = nullptr, *d_tlen = nullptr, *d_ww = nullptr, *d_Q = nullptr, *d_Phi = nullptr, *d_srad = nullptr, *d_trad = nullptr, *d_sctr = nullptr, *d_tctr = nullptr;
+    int *d_sibeg = nullptr, *d_snum = nullptr, *d_snch = nullptr, *d_sch = nullptr, *d_sleaves = nullptr, *d_slvl = nullptr, *d_tibeg = nullptr, *d_tnum = nullptr, *d_tnch = nullptr, *d_tch = nullptr, *d_tpar = nullptr, *d_tleaves = nullptr, *d_tlvl = nullptr, *d_aidx = nullptr, *d_didx = nullptr, *d_ccidx = nullptr, *d_cpidx = nullptr, *d_order = nullptr, *d_queue = nullptr, *d_mxdidx = nullptr, *d_mxcpidx = nullptr;
+    int64_t *d_aoff = nullptr, *d_doff = nullptr, *d_ccoff = nullptr, *d_cpoff = nullptr, *d_mxdoff = nullptr, *d_mxcpoff = nullptr;
+    int2 *d_evitems = nullptr, *d_griditems = nullptr, *d_l2pitems = nullptr;
+    float4 *d_spos = nullptr, *d_tpos = nullptr;
+    float *d_Q32 = nullptr;
+    unsigned char *d_mxdflag = nullptr, *d_adeg = nullptr;
+    double *d_xgrid[BT_MAX_DEGREE + 1] = {}, *d_xQ[BT_MAX_DEGREE + 1] = {};
+    float *d_xQ32[BT_MAX_DEGREE + 1] = {};
+    double *d_out = nullptr;    // potentials in caller order (run_plan's own buffer)
+};
+
+// The device sequence of one evaluation (stream-ordered, no host
+// synchronisation, so it can be captured into a CUDA graph): relative
+// positions, upward pass, grid-output and particle-output kernels, downward
+// pass, and the scatter of the potentials into caller order at scatter_out.
+// ev: 5 events bracketing the phases, or nullptr.
+int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatter_out, long long &launches)
+{
+    int rc = BT_OK;
+    const bool mixed = v.mixed, herm = v.herm, need_src_clusters = v.need_src_clusters, need_tgt_grids = v.need_tgt_grids;
+    const int n = v.n, P = v.P, ns = v.ns, nt = v.nt, max_np1 = v.max_np1;
+    const std::vector<int> &xdeg = v.xdeg;
+    auto d_sx = v.d_sx;
+    auto d_sy = v.d_sy;
+    auto d_sz = v.d_sz;
+    auto d_sq = v.d_sq;
+    auto d_tx = v.d_tx;
+    auto d_ty = v.d_ty;
+    auto d_tz = v.d_tz;
+    auto d_pot = v.d_pot;
+    auto d_sgrid = v.d_sgrid;
+    auto d_tgrid = v.d_tgrid;
+    auto d_slen = v.d_slen;
+    auto d_tlen = v.d_tlen;
+    auto d_ww = v.d_ww;
+    auto d_Q = v.d_Q;
+    auto d_Phi = v.d_Phi;
+    auto d_srad = v.d_srad;
+    auto d_trad = v.d_trad;
+    auto d_sctr = v.d_sctr;
+    auto d_tctr = v.d_tctr;
+    auto d_sibeg = v.d_sibeg;
+    auto d_snum = v.d_snum;
+    auto d_snch = v.d_snch;
+    auto d_sch = v.d_sch;
+    auto d_sleaves = v.d_sleaves;
+    auto d_slvl = v.d_slvl;
+    auto d_tibeg = v.d_tibeg;
+    auto d_tnum = v.d_tnum;
+    auto d_tnch = v.d_tnch;
+    auto d_tch = v.d_tch;
+    auto d_tpar = v.d_tpar;
+    auto d_tleaves = v.d_tleaves;
+    auto d_tlvl = v.d_tlvl;
+    auto d_aidx = v.d_aidx;
+    auto d_didx = v.d_didx;
+    auto d_ccidx = v.d_ccidx;
+    auto d_cpidx = v.d_cpidx;
+    auto d_order = v.d_order;
+    auto d_queue = v.d_queue;
+    auto d_mxdidx = v.d_mxdidx;
+    auto d_mxcpidx = v.d_mxcpidx;
+    auto d_aoff = v.d_aoff;
+    auto d_doff = v.d_doff;
+    auto d_ccoff = v.d_ccoff;
+    auto d_cpoff = v.d_cpoff;
+    auto d_mxdoff = v.d_mxdoff;
+    auto d_mxcpoff = v.d_mxcpoff;
+    auto d_evitems = v.d_evitems;
+    auto d_griditems = v.d_griditems;
+    auto d_l2pitems = v.d_l2pitems;
+    auto d_spos = v.d_spos;
+    auto d_tpos = v.d_tpos;
+    auto d_Q32 = v.d_Q32;
+    auto d_mxdflag = v.d_mxdflag;
+    auto d_adeg = v.d_adeg;
+    auto &d_xgrid = v.d_xgrid;
+    auto &d_xQ = v.d_xQ;
+    auto &d_xQ32 = v.d_xQ32;
+    if (mixed) {
+        bt::launch_rel_positions(v.S_nleaves, d_sleaves, d_sibeg, d_snum, d_sctr, d_sx, d_sy, d_sz, d_sq, d_spos, st);
+        bt::launch_rel_positions(v.T_nleaves, d_tleaves, d_tibeg, d_tnum, d_tctr, d_tx, d_ty, d_tz, nullptr, d_tpos, st);
+        launches += 2;
+    }
+    if (ev) CK(cudaEventRecord(ev[0], st));
+    // upward pass
+    if (need_src_clusters && ns > 0) {
+        bt::launch_p2m(n, herm, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
+                       d_sz, d_sq, d_Q, st);
+        launches++;
+        if (!herm) {
+            for (int l = v.S_max_depth - 1; l >= 0; l--) {
+                int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
+                if (cnt > 0) {
+                    bt::launch_m2m(n, cnt, d_slvl + v.S_lvl_off[l], d_snch, d_sch, d_sgrid, d_Q, st);
+                    launches++;
+                }
+            }
+        }
+        if (mixed) {
+            bt::launch_to_f32((size_t)v.S_n * P, d_Q, d_Q32, st);
+            launches++;
+        }
+        // proxy charges at the other degrees chosen per interaction
+        for (size_t i = 0; i < xdeg.size(); i++) {
+            const int d = xdeg[i];
+            bt::launch_p2m(d, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww, d_sx,
+                           d_sy, d_sz, d_sq, d_xQ[i], st);
+            launches++;
+            for (int l = v.S_max_depth - 1; l >= 0; l--) {
+                int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
+                if (cnt > 0) {
+                    bt::launch_m2m(d, cnt, d_slvl + v.S_lvl_off[l], d_snch, d_sch, d_xgrid[i], d_xQ[i], st);
+                    launches++;
+                }
+            }
+            bt::launch_to_f32((size_t)v.S_n * (d + 1) * (d + 1) * (d + 1), d_xQ[i], d_xQ32[i], st);
+            launches++;
+        }
+    }
+    CK(cudaGetLastError());
+    if (ev) CK(cudaEventRecord(ev[1], st));
+    // grid-output evaluation (CP, M2L) and L2L
+    if (mixed && v.queue) CK(cudaMemsetAsync(d_queue, 0, 2 * sizeof(int), st));
+    if (need_tgt_grids && nt > 0 && mixed) {
+        bt::MixedGridsArgs g;
+        g.n = n; g.nitems = v.n_grid_items; g.items = d_griditems; g.t_grid = d_tgrid; g.t_ctr = d_tctr;
+        g.queue = v.queue ? d_queue : nullptr;
+        g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_mxcpoff; g.p_idx = d_mxcpidx;
+        g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.s_ctr = d_sctr; g.Q32 = d_Q32;
+        g.spos = d_spos; g.kc = bt::mixed_kernel_constant(v.kernel, v.kp); g.Phi = d_Phi;
+        bt::launch_eval_grids_mixed(v.kernel, g, st);
+        launches++;
+    } else if (need_tgt_grids && nt > 0) {
+        bt::EvalGridsArgs g;
+        g.n = n; g.nitems = v.n_grid_items; g.items = d_griditems; g.t_grid = d_tgrid;
+        g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_cpoff; g.p_idx = d_cpidx;
+        g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.Q = d_Q;
+        g.sx = d_sx; g.sy = d_sy; g.sz = d_sz; g.sq = d_sq; g.kp = v.kp; g.Phi = d_Phi;
+        bt::launch_eval_grids(v.kernel, herm, g, st);
+        launches++;
+    }
+    CK(cudaGetLastError());
+    if (ev) CK(cudaEventRecord(ev[2], st));
+    // particle-output evaluation (PC, PP)
+    if (nt > 0 && mixed) {
+        bt::MixedTargetsArgs a;
+        memset(&a, 0, sizeof a);
+        a.n = n; a.max_np1 = max_np1; a.nitems = v.n_ev_items; a.items = d_evitems;
+        a.queue = v.queue ? d_queue + 1 : nullptr;
+        a.leaf_node = d_tleaves; a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.t_ctr = d_tctr; a.tpos = d_tpos;
+        a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = d_adeg;
+        a.s_grid[n] = d_sgrid; a.Q32[n] = d_Q32;
+        for (size_t i = 0; i < xdeg.size(); i++) { a.s_grid[xdeg[i]] = d_xgrid[i]; a.Q32[xdeg[i]] = d_xQ32[i]; }
+        a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.d_flag = d_mxdflag; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
+        a.spos = d_spos; a.kc = bt::mixed_kernel_constant(v.kernel, v.kp); a.pot = d_pot;
+        a.t_rad = d_trad; a.s_rad = d_srad;
+        a.tx64 = d_tx; a.ty64 = d_ty; a.tz64 = d_tz; a.sx64 = d_sx; a.sy64 = d_sy; a.sz64 = d_sz; a.sq64 = d_sq;
+        a.kp = v.kp;
+        bt::launch_eval_targets_mixed(v.kernel, a, st);
+        launches++;
+    } else if (nt > 0) {
+        bt::EvalTargetsArgs a;
+        a.n = n; a.nitems = v.n_ev_items; a.items = d_evitems; a.leaf_node = d_tleaves;
+        a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.a_off = d_aoff; a.a_idx = d_aidx; a.d_off = d_doff; a.d_idx = d_didx;
+        a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_grid = d_sgrid; a.Q = d_Q;
+        a.sx = d_sx; a.sy = d_sy; a.sz = d_sz; a.sq = d_sq; a.tx = d_tx; a.ty = d_ty; a.tz = d_tz;
+        a.kp = v.kp; a.pot = d_pot;
+        bt::launch_eval_targets(v.kernel, herm, a, st);
+        launches++;
+    }
+    CK(cudaGetLastError());
+    if (ev) CK(cudaEventRecord(ev[3], st));
+    // downward pass
+    if (need_tgt_grids && nt > 0) {
+        if (!herm) {
+            for (int l = 0; l < v.T_max_depth; l++) {
+                int cnt = v.T_lvl_off[l + 1] - v.T_lvl_off[l];
+                if (cnt > 0) {
+                    bt::launch_l2l(n, cnt, d_tlvl + v.T_lvl_off[l], d_tnch, d_tch, d_tgrid, d_Phi, st);
+                    launches++;
+                }
+            }
+        }
+        bt::launch_l2p(n, herm, v.n_l2p_items, d_l2pitems, d_tleaves, d_tpar, d_tibeg, d_tnum, d_tgrid,
+                       d_tlen, d_ww, d_Phi, d_tx, d_ty, d_tz, d_pot, st);
+        launches++;
+    }
+    CK(cudaGetLastError());
+    if (ev) CK(cudaEventRecord(ev[4], st));
+    bt::launch_scatter(nt, d_order, d_pot, scatter_out, st);
+    launches++;
+    CK(cudaGetLastError());
+done:
+    return rc;
+}
+
 // Device evaluation of a built plan; writes potentials in caller order to out_host.
+// execute = false: prepare only (uploads done, the device sequence not
+// issued), for capture into a graph by the caller.
 int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on_device, bt_report *rep,
-             const DevParts *dp = nullptr)
+             const DevParts *dp = nullptr, bool queue = false, DevPlan *dv_out = nullptr, bool execute = true)
 {
     const bt_params &o = pl.prm;
     const int n = o.degree, P = o.P;
@@ -531,6 +764,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     L.add(&d_cpoff, pl.g_cp.rows + 1); L.add(&d_cpidx, pl.g_cp.off[pl.g_cp.rows]);
     L.add(&d_evitems, ev_items.size()); L.add(&d_griditems, grid_items.size()); L.add(&d_l2pitems, l2p_items.size());
     L.add(&d_out, nt);
+    int *d_queue;           // work-queue counters of the two evaluation kernels
+    L.add(&d_queue, 2);
     float4 *d_spos = nullptr, *d_tpos = nullptr;
     float *d_Q32 = nullptr;
     double *d_sctr = nullptr, *d_tctr = nullptr;
@@ -602,117 +837,83 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         }
 #undef UP
         cudaEvent_t *ev = ctx->ev;
-        if (mixed) {
-            bt::launch_rel_positions(S.nleaves, d_sleaves, d_sibeg, d_snum, d_sctr, d_sx, d_sy, d_sz, d_sq, d_spos, st);
-            bt::launch_rel_positions(T.nleaves, d_tleaves, d_tibeg, d_tnum, d_tctr, d_tx, d_ty, d_tz, nullptr, d_tpos, st);
-            launches += 2;
+        DevPlan v;
+        v.mixed = mixed; v.herm = herm; v.need_src_clusters = need_src_clusters; v.need_tgt_grids = need_tgt_grids;
+        v.queue = queue;
+        v.n = n; v.P = P; v.ns = ns; v.nt = nt; v.max_np1 = max_np1; v.kernel = o.kernel; v.kp = o.kp;
+        v.S_n = S.n; v.S_nleaves = S.nleaves; v.S_max_depth = S.max_depth;
+        v.T_n = T.n; v.T_nleaves = T.nleaves; v.T_max_depth = T.max_depth;
+        if (S.lvl_off) v.S_lvl_off.assign(S.lvl_off, S.lvl_off + S.max_depth + 1);
+        else v.S_lvl_off.assign(S.max_depth + 1, 0);
+        if (T.lvl_off) v.T_lvl_off.assign(T.lvl_off, T.lvl_off + T.max_depth + 1);
+        else v.T_lvl_off.assign(T.max_depth + 1, 0);
+        v.xdeg = xdeg;
+        v.n_grid_items = (int)grid_items.size(); v.n_ev_items = (int)ev_items.size(); v.n_l2p_items = (int)l2p_items.size();
+        v.d_sx = d_sx;
+        v.d_sy = d_sy;
+        v.d_sz = d_sz;
+        v.d_sq = d_sq;
+        v.d_tx = d_tx;
+        v.d_ty = d_ty;
+        v.d_tz = d_tz;
+        v.d_pot = d_pot;
+        v.d_sgrid = d_sgrid;
+        v.d_tgrid = d_tgrid;
+        v.d_slen = d_slen;
+        v.d_tlen = d_tlen;
+        v.d_ww = d_ww;
+        v.d_Q = d_Q;
+        v.d_Phi = d_Phi;
+        v.d_srad = d_srad;
+        v.d_trad = d_trad;
+        v.d_sctr = d_sctr;
+        v.d_tctr = d_tctr;
+        v.d_sibeg = d_sibeg;
+        v.d_snum = d_snum;
+        v.d_snch = d_snch;
+        v.d_sch = d_sch;
+        v.d_sleaves = d_sleaves;
+        v.d_slvl = d_slvl;
+        v.d_tibeg = d_tibeg;
+        v.d_tnum = d_tnum;
+        v.d_tnch = d_tnch;
+        v.d_tch = d_tch;
+        v.d_tpar = d_tpar;
+        v.d_tleaves = d_tleaves;
+        v.d_tlvl = d_tlvl;
+        v.d_aidx = d_aidx;
+        v.d_didx = d_didx;
+        v.d_ccidx = d_ccidx;
+        v.d_cpidx = d_cpidx;
+        v.d_order = d_order;
+        v.d_queue = d_queue;
+        v.d_mxdidx = d_mxdidx;
+        v.d_mxcpidx = d_mxcpidx;
+        v.d_aoff = d_aoff;
+        v.d_doff = d_doff;
+        v.d_ccoff = d_ccoff;
+        v.d_cpoff = d_cpoff;
+        v.d_mxdoff = d_mxdoff;
+        v.d_mxcpoff = d_mxcpoff;
+        v.d_evitems = d_evitems;
+        v.d_griditems = d_griditems;
+        v.d_l2pitems = d_l2pitems;
+        v.d_spos = d_spos;
+        v.d_tpos = d_tpos;
+        v.d_Q32 = d_Q32;
+        v.d_mxdflag = d_mxdflag;
+        v.d_adeg = d_adeg;
+        for (int k = 0; k <= BT_MAX_DEGREE; k++) { v.d_xgrid[k] = d_xgrid[k]; v.d_xQ[k] = d_xQ[k]; v.d_xQ32[k] = d_xQ32[k]; }
+        if (dv_out) {
+            *dv_out = v;
+            dv_out->d_out = d_out;
         }
-        CK(cudaEventRecord(ev[0], st));
-        // upward pass
-        if (need_src_clusters && ns > 0) {
-            bt::launch_p2m(n, herm, S.nleaves, d_sleaves, S.n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
-                           d_sz, d_sq, d_Q, st);
-            launches++;
-            if (!herm) {
-                for (int l = S.max_depth - 1; l >= 0; l--) {
-                    int cnt = S.lvl_off[l + 1] - S.lvl_off[l];
-                    if (cnt > 0) {
-                        bt::launch_m2m(n, cnt, d_slvl + S.lvl_off[l], d_snch, d_sch, d_sgrid, d_Q, st);
-                        launches++;
-                    }
-                }
-            }
-            if (mixed) {
-                bt::launch_to_f32((size_t)S.n * P, d_Q, d_Q32, st);
-                launches++;
-            }
-            // proxy charges at the other degrees chosen per interaction
-            for (size_t i = 0; i < xdeg.size(); i++) {
-                const int d = xdeg[i];
-                bt::launch_p2m(d, false, S.nleaves, d_sleaves, S.n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww, d_sx,
-                               d_sy, d_sz, d_sq, d_xQ[i], st);
-                launches++;
-                for (int l = S.max_depth - 1; l >= 0; l--) {
-                    int cnt = S.lvl_off[l + 1] - S.lvl_off[l];
-                    if (cnt > 0) {
-                        bt::launch_m2m(d, cnt, d_slvl + S.lvl_off[l], d_snch, d_sch, d_xgrid[i], d_xQ[i], st);
-                        launches++;
-                    }
-                }
-                bt::launch_to_f32((size_t)S.n * (d + 1) * (d + 1) * (d + 1), d_xQ[i], d_xQ32[i], st);
-                launches++;
-            }
+        if (!execute) {
+            CK(cudaStreamSynchronize(st));
+            goto done;
         }
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(ev[1], st));
-        // grid-output evaluation (CP, M2L) and L2L
-        if (need_tgt_grids && nt > 0 && mixed) {
-            bt::MixedGridsArgs g;
-            g.n = n; g.nitems = (int)grid_items.size(); g.items = d_griditems; g.t_grid = d_tgrid; g.t_ctr = d_tctr;
-            g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_mxcpoff; g.p_idx = d_mxcpidx;
-            g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.s_ctr = d_sctr; g.Q32 = d_Q32;
-            g.spos = d_spos; g.kc = bt::mixed_kernel_constant(o.kernel, o.kp); g.Phi = d_Phi;
-            bt::launch_eval_grids_mixed(o.kernel, g, st);
-            launches++;
-        } else if (need_tgt_grids && nt > 0) {
-            bt::EvalGridsArgs g;
-            g.n = n; g.nitems = (int)grid_items.size(); g.items = d_griditems; g.t_grid = d_tgrid;
-            g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_cpoff; g.p_idx = d_cpidx;
-            g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.Q = d_Q;
-            g.sx = d_sx; g.sy = d_sy; g.sz = d_sz; g.sq = d_sq; g.kp = o.kp; g.Phi = d_Phi;
-            bt::launch_eval_grids(o.kernel, herm, g, st);
-            launches++;
-        }
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(ev[2], st));
-        // particle-output evaluation (PC, PP)
-        if (nt > 0 && mixed) {
-            bt::MixedTargetsArgs a;
-            memset(&a, 0, sizeof a);
-            a.n = n; a.max_np1 = max_np1; a.nitems = (int)ev_items.size(); a.items = d_evitems;
-            a.leaf_node = d_tleaves; a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.t_ctr = d_tctr; a.tpos = d_tpos;
-            a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = d_adeg;
-            a.s_grid[n] = d_sgrid; a.Q32[n] = d_Q32;
-            for (size_t i = 0; i < xdeg.size(); i++) { a.s_grid[xdeg[i]] = d_xgrid[i]; a.Q32[xdeg[i]] = d_xQ32[i]; }
-            a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.d_flag = d_mxdflag; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
-            a.spos = d_spos; a.kc = bt::mixed_kernel_constant(o.kernel, o.kp); a.pot = d_pot;
-            a.t_rad = d_trad; a.s_rad = d_srad;
-            a.tx64 = d_tx; a.ty64 = d_ty; a.tz64 = d_tz; a.sx64 = d_sx; a.sy64 = d_sy; a.sz64 = d_sz; a.sq64 = d_sq;
-            a.kp = o.kp;
-            bt::launch_eval_targets_mixed(o.kernel, a, st);
-            launches++;
-        } else if (nt > 0) {
-            bt::EvalTargetsArgs a;
-            a.n = n; a.nitems = (int)ev_items.size(); a.items = d_evitems; a.leaf_node = d_tleaves;
-            a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.a_off = d_aoff; a.a_idx = d_aidx; a.d_off = d_doff; a.d_idx = d_didx;
-            a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_grid = d_sgrid; a.Q = d_Q;
-            a.sx = d_sx; a.sy = d_sy; a.sz = d_sz; a.sq = d_sq; a.tx = d_tx; a.ty = d_ty; a.tz = d_tz;
-            a.kp = o.kp; a.pot = d_pot;
-            bt::launch_eval_targets(o.kernel, herm, a, st);
-            launches++;
-        }
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(ev[3], st));
-        // downward pass
-        if (need_tgt_grids && nt > 0) {
-            if (!herm) {
-                for (int l = 0; l < T.max_depth; l++) {
-                    int cnt = T.lvl_off[l + 1] - T.lvl_off[l];
-                    if (cnt > 0) {
-                        bt::launch_l2l(n, cnt, d_tlvl + T.lvl_off[l], d_tnch, d_tch, d_tgrid, d_Phi, st);
-                        launches++;
-                    }
-                }
-            }
-            bt::launch_l2p(n, herm, (int)l2p_items.size(), d_l2pitems, d_tleaves, d_tpar, d_tibeg, d_tnum, d_tgrid,
-                           d_tlen, d_ww, d_Phi, d_tx, d_ty, d_tz, d_pot, st);
-            launches++;
-        }
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(ev[4], st));
-        bt::launch_scatter(nt, d_order, d_pot, out_on_device ? out : d_out, st);
-        launches++;
-        CK(cudaGetLastError());
+        rc = issue_plan(v, st, ev, out_on_device ? out : d_out, launches);
+        if (rc != BT_OK) goto done;
         if (!out_on_device && nt > 0)
             CK(cudaMemcpyAsync(out, d_out, sizeof(double) * nt, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -781,7 +982,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         node_geometry(T, tctr, trad);
         const int64_t CH = 1 << 18;
         double *d_sq, *d_mom, *d_sctr, *d_tctr, *d_srad, *d_trad;
-        int *d_sibeg, *d_snum, *d_tnum, *d_idx, *d_unit;
+        int *d_sibeg, *d_snum, *d_tnum, *d_idx, *d_unit, *d_snch, *d_sch, *d_sleaves, *d_slvl;
         int64_t *d_off;
         float *d_feat, *d_w, *d_act, *d_pred;
         unsigned char *d_choice;
@@ -790,6 +991,8 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         else L.add(&d_sq, pl.src.n);
         L.add(&d_mom, 2 * (size_t)S.n); L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
         L.add(&d_srad, srad.size()); L.add(&d_trad, trad.size()); L.add(&d_sibeg, S.n); L.add(&d_snum, S.n);
+        L.add(&d_snch, S.n); L.add(&d_sch, 8 * (size_t)S.n); L.add(&d_sleaves, S.nleaves);
+        L.add(&d_slvl, S.lvl_off ? S.lvl_off[S.max_depth] : 0);
         L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
         L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size()); L.add(&d_act, 3 * (size_t)CH * bt::MLP_H);
         L.add(&d_pred, (size_t)ne * bt::MLP_OUT); L.add(&d_choice, ne);
@@ -805,16 +1008,19 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_srad, srad.data(), srad.size()); UP(d_trad, trad.data(), trad.size());
             UP(d_sibeg, S.ibeg, S.n); UP(d_snum, S.numpar, S.n); UP(d_tnum, T.numpar, T.n);
+            UP(d_snch, S.nchild, S.n); UP(d_sch, S.child, 8 * (size_t)S.n); UP(d_sleaves, S.leaves, S.nleaves);
+            if (S.lvl_off && S.lvl_off[S.max_depth] > 0) UP(d_slvl, S.lvl_nodes, S.lvl_off[S.max_depth]);
             UP(d_idx, pl.t_approx.idx, ne); UP(d_unit, T.leaves, T.nleaves);
             UP(d_off, pl.t_approx.off, pl.t_approx.rows + 1); UP(d_w, w.data(), w.size());
 #undef UP
-            bt::launch_node_moments(S.n, d_sibeg, d_snum, d_sq, d_mom, st);
+            bt::MomentTree mt{S.n, S.nleaves, S.max_depth, d_sleaves, d_sibeg, d_snum, d_snch, d_sch, d_slvl, S.lvl_off};
+            long long launches = bt::launch_node_moments(mt, d_sq, d_mom, st);
             bt::FeatureArgs fa;
             fa.units = pl.t_approx.rows; fa.off = d_off; fa.idx = d_idx; fa.unit_node = d_unit;
             fa.t_ctr = d_tctr; fa.s_ctr = d_sctr; fa.t_rad = d_trad; fa.s_rad = d_srad; fa.s_mom = d_mom;
             fa.t_numpar = d_tnum; fa.s_numpar = d_snum;
             bt::launch_features(fa, ne, d_feat, st);
-            long long launches = 2;
+            launches++;
             for (int64_t c0 = 0; c0 < ne; c0 += CH) {
                 int B = (int)std::min<int64_t>(CH, ne - c0);
                 bt::mlp_forward(d_w, B, d_feat + c0 * bt::MLP_IN, d_act, d_pred + c0 * bt::MLP_OUT, st);
@@ -917,11 +1123,49 @@ int static_scratch_arena(int device, Arena **out)
     return BT_OK;
 }
 
-int eval_common(int nt, int ns, const double *tx, const double *ty, const double *tz, const double *sx,
+// Checks the options and applies them to prm: precision, learned degree
+// policy and its tolerance, dispatch of the mixed evaluation kernels.
+int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double &tol, bool &queue)
+{
+    if (opts && opts->precision != BT_PRECISION_FP64 && opts->precision != BT_PRECISION_MIXED) {
+        set_err("invalid precision %d", opts->precision);
+        return BT_ERR_PARAM;
+    }
+    prm.precision = opts ? opts->precision : BT_PRECISION_FP64;
+    learned = opts && opts->degree_policy == BT_DEGREE_LEARNED;
+    if (opts && opts->degree_policy != BT_DEGREE_FIXED && !learned) {
+        set_err("invalid degree policy %d", opts->degree_policy);
+        return BT_ERR_PARAM;
+    }
+    if (opts && opts->tree_build != BT_TREE_GPU && opts->tree_build != BT_TREE_HOST) {
+        set_err("invalid tree build %d", opts->tree_build);
+        return BT_ERR_PARAM;
+    }
+    if (opts && (opts->dispatch < BT_DISPATCH_AUTO || opts->dispatch > BT_DISPATCH_GRID)) {
+        set_err("invalid dispatch %d", opts->dispatch);
+        return BT_ERR_PARAM;
+    }
+    // AUTO: one block per work item.  Persistent blocks on a device counter
+    // measured 2.5 % slower for the 16M clustered system (cost-sorted items
+    // are already dispatched longest first by the block scheduler).
+    queue = opts && opts->dispatch == BT_DISPATCH_QUEUE;
+    if (learned && (prm.precision != BT_PRECISION_MIXED || prm.ctype != PARTICLE_CLUSTER || prm.approx != LAGRANGE ||
+                    prm.kernel != COULOMB)) {
+        set_err("learned degree selection is provided for mixed precision, particle-cluster, Lagrange, Coulomb");
+        return BT_ERR_UNSUPPORTED;
+    }
+    tol = (opts && opts->tolerance > 0) ? opts->tolerance : 1e-6;
+    return BT_OK;
+}
+
+int eval_common(const Systems &sys, const double *tx, const double *ty, const double *tz, const double *sx,
                 const double *sy, const double *sz, const double *sq, double *out, bt_params &prm,
                 const bt_options *opts, bt_report *rep, bool use_static_scratch = false)
 {
     g_err[0] = 0;
+    const int64_t nt64 = sys.toff[sys.n], ns64 = sys.soff[sys.n];
+    if (nt64 > INT_MAX || ns64 > INT_MAX) { set_err("more than 2^31-1 particles"); return BT_ERR_PARAM; }
+    const int nt = (int)nt64, ns = (int)ns64;
     int rc = validate(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, prm);
     if (rc != BT_OK) return rc;
     const bool out_dev = opts && opts->inputs_on_device;
@@ -933,26 +1177,10 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
         return BT_OK;
     }
     int device = opts ? opts->device : 0;
-    if (opts && opts->precision != BT_PRECISION_FP64 && opts->precision != BT_PRECISION_MIXED) {
-        set_err("invalid precision %d", opts->precision);
-        return BT_ERR_PARAM;
-    }
-    prm.precision = opts ? opts->precision : BT_PRECISION_FP64;
-    const bool learned = opts && opts->degree_policy == BT_DEGREE_LEARNED;
-    if (opts && opts->degree_policy != BT_DEGREE_FIXED && !learned) {
-        set_err("invalid degree policy %d", opts->degree_policy);
-        return BT_ERR_PARAM;
-    }
-    if (opts && opts->tree_build != BT_TREE_GPU && opts->tree_build != BT_TREE_HOST) {
-        set_err("invalid tree build %d", opts->tree_build);
-        return BT_ERR_PARAM;
-    }
-    if (learned && (prm.precision != BT_PRECISION_MIXED || prm.ctype != PARTICLE_CLUSTER || prm.approx != LAGRANGE ||
-                    prm.kernel != COULOMB)) {
-        set_err("learned degree selection is provided for mixed precision, particle-cluster, Lagrange, Coulomb");
-        return BT_ERR_UNSUPPORTED;
-    }
-    const double tol = (opts && opts->tolerance > 0) ? opts->tolerance : 1e-6;
+    bool learned = false, queue = false;
+    double tol = 1e-6;
+    rc = parse_options(opts, prm, learned, tol, queue);
+    if (rc != BT_OK) return rc;
     DeviceCtx *ctx = nullptr;
     rc = get_ctx(device, &ctx);
     if (rc != BT_OK) return rc;
@@ -970,7 +1198,7 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
     pl.prm = prm;
     DevParts dp;
     if (gpu_tree) {
-        rc = build_plan_gpu(ctx, pl, nt, ns, tx, ty, tz, sx, sy, sz, sq, on_dev, dp);
+        rc = build_plan_gpu(ctx, ctx->tree_arena, pl, sys, tx, ty, tz, sx, sy, sz, sq, on_dev, dp);
         if (rc != BT_OK) {
             bt_plan_free(&pl);
             return rc;
@@ -996,7 +1224,7 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
             if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { set_err("copy of device inputs failed"); return BT_ERR_CUDA; }
             tx = hp[0]; ty = hp[1]; tz = hp[2]; sx = hp[3]; sy = hp[4]; sz = hp[5]; sq = hp[6];
         }
-        build_plan(pl, nt, ns, tx, ty, tz, sx, sy, sz, sq);
+        build_plan(pl, sys, tx, ty, tz, sx, sy, sz, sq);
     }
     const DevParts *dpp = gpu_tree ? &dp : nullptr;
     double t1 = now_ms();
@@ -1016,10 +1244,42 @@ int eval_common(int nt, int ns, const double *tx, const double *ty, const double
             rep->ms_setup = now_ms() - t0;
         }
     }
-    rc = run_plan(ctx, *arena, pl, out, on_dev, rep, dpp);
+    rc = run_plan(ctx, *arena, pl, out, on_dev, rep, dpp, queue);
     bt_plan_free(&pl);
     if (rc != BT_OK && !on_dev) memset(out, 0, sizeof(double) * (size_t)nt);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Sessions: fixed geometry, new charges per evaluation, replayed as a graph
+// ---------------------------------------------------------------------------
+struct Session {
+    int device = 0;
+    DeviceCtx *ctx = nullptr;
+    Arena tree_arena, arena;        // owned by the session
+    DevPlan v;
+    bool on_dev = false;
+    int ns = 0, nt = 0;
+    double *d_qin = nullptr;        // charges in caller order
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev[5] = {};
+    long long graph_kernels = 0;    // kernel launches per replay
+    bt_report base{};               // interaction counts, node counts, setup time
+};
+
+void session_free(Session *s)
+{
+    if (!s) return;
+    if (s->ctx) cudaSetDevice(s->device);
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    for (auto &e : s->ev)
+        if (e) cudaEventDestroy(e);
+    if (s->d_qin) cudaFree(s->d_qin);
+    if (s->arena.base) cudaFree(s->arena.base);
+    if (s->tree_arena.base) cudaFree(s->tree_arena.base);
+    delete s;
 }
 
 }  // namespace
@@ -1043,7 +1303,7 @@ int BaryTreeInterface_ex(int numTargets, int numSources, const double *targetX, 
     bt_params_setup(&prm, kernel, numKernelParams, kernelParams, singularity, approximation, compute_type, theta,
                     interpOrder, maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, beta, verbosity);
     bt_report rep;
-    int rc = eval_common(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+    int rc = eval_common(Systems(numTargets, numSources), targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
                          outputArray, prm, nullptr, verbosity > 0 ? &rep : nullptr);
     if (verbosity > 0 && rc == BT_OK) {
         printf("[BaryTree] barytree_b200: %d targets, %d sources, setup %.3f ms, upward %.3f ms, "
@@ -1076,7 +1336,7 @@ int bt_eval(int numTargets, int numSources, const double *targetX, const double 
     bt_params prm;
     bt_params_setup(&prm, kernel, 1, &kernelParam, SKIPPING, approximation, compute_type, theta, interpOrder,
                     maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
-    return eval_common(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+    return eval_common(Systems(numTargets, numSources), targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
                        outputArray, prm, opts, report);
 }
 
@@ -1094,8 +1354,36 @@ int bt_eval_noalloc(int numTargets, int numSources, const double *targetX, const
     opts.precision = precision;
     opts.device = device;
     opts.inputs_on_device = 1;
-    return eval_common(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+    return eval_common(Systems(numTargets, numSources), targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
                        outputArray, prm, &opts, nullptr, true);
+}
+
+int bt_eval_batch(int numSystems, const long long *targetOffsets, const long long *sourceOffsets,
+                  const double *targetX, const double *targetY, const double *targetZ, const double *sourceX,
+                  const double *sourceY, const double *sourceZ, const double *sourceValue, double *outputArray,
+                  int kernel, double kernelParam, int approximation, int compute_type, double theta,
+                  int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck,
+                  const bt_options *opts, bt_report *report)
+{
+    g_err[0] = 0;
+    if (numSystems < 1 || !targetOffsets || !sourceOffsets) {
+        set_err("a batch needs at least one system and both offset arrays");
+        return BT_ERR_PARAM;
+    }
+    if (targetOffsets[0] != 0 || sourceOffsets[0] != 0) {
+        set_err("offsets must start at 0");
+        return BT_ERR_PARAM;
+    }
+    for (int k = 0; k < numSystems; k++)
+        if (targetOffsets[k + 1] < targetOffsets[k] || sourceOffsets[k + 1] < sourceOffsets[k]) {
+            set_err("offsets must not decrease (system %d)", k);
+            return BT_ERR_PARAM;
+        }
+    bt_params prm;
+    bt_params_setup(&prm, kernel, 1, &kernelParam, SKIPPING, approximation, compute_type, theta, interpOrder,
+                    maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
+    return eval_common(Systems(numSystems, targetOffsets, sourceOffsets), targetX, targetY, targetZ, sourceX, sourceY,
+                       sourceZ, sourceValue, outputArray, prm, opts, report);
 }
 
 int bt_direct(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,
@@ -1293,7 +1581,10 @@ long bt_selector_training_data(int n, const double *x, const double *y, const do
                 if (cnt > 0) { bt::launch_m2m(d, cnt, d_slvl + S.lvl_off[l], d_snch, d_sch, d_grid[d], d_Q[d], st); launches++; }
             }
         }
-        bt::launch_node_moments(S.n, d_sibeg, d_snum, d_sq, d_mom, st);
+        {
+            bt::MomentTree mt{S.n, S.nleaves, S.max_depth, d_sleaves, d_sibeg, d_snum, d_snch, d_sch, d_slvl, S.lvl_off};
+            launches += bt::launch_node_moments(mt, d_sq, d_mom, st);
+        }
         bt::FeatureArgs fa;
         memset(&fa, 0, sizeof fa);
         fa.t_ctr = d_tctr; fa.s_ctr = d_sctr; fa.t_rad = d_trad; fa.s_rad = d_srad; fa.s_mom = d_mom;
@@ -1511,6 +1802,165 @@ int bt_tree_dump_ex(int n, const double *x, const double *y, const double *z, in
     bt_tree_free(&t);
     bt_parts_free(&p);
     return nn <= cap ? nn : -1;
+}
+
+int bt_session_create(int numSystems, const long long *targetOffsets, const long long *sourceOffsets,
+                      const double *targetX, const double *targetY, const double *targetZ, const double *sourceX,
+                      const double *sourceY, const double *sourceZ, const double *sourceValue, int kernel,
+                      double kernelParam, int approximation, int compute_type, double theta, int interpOrder,
+                      int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck, const bt_options *opts,
+                      bt_session **session)
+{
+    g_err[0] = 0;
+    if (!session) { set_err("session pointer is NULL"); return BT_ERR_PARAM; }
+    *session = nullptr;
+    if (numSystems < 1 || (numSystems > 1 && (!targetOffsets || !sourceOffsets))) {
+        set_err("a session needs at least one system (offsets for more than one)");
+        return BT_ERR_PARAM;
+    }
+    std::vector<long long> tdef, sdef;
+    if (!targetOffsets || !sourceOffsets) {
+        set_err("offsets are required (numSystems+1 entries, from 0)");
+        return BT_ERR_PARAM;
+    }
+    if (targetOffsets[0] != 0 || sourceOffsets[0] != 0) { set_err("offsets must start at 0"); return BT_ERR_PARAM; }
+    for (int k = 0; k < numSystems; k++)
+        if (targetOffsets[k + 1] < targetOffsets[k] || sourceOffsets[k + 1] < sourceOffsets[k]) {
+            set_err("offsets must not decrease (system %d)", k);
+            return BT_ERR_PARAM;
+        }
+    const Systems sys(numSystems, targetOffsets, sourceOffsets);
+    const int64_t nt64 = sys.toff[sys.n], ns64 = sys.soff[sys.n];
+    if (nt64 > INT_MAX || ns64 > INT_MAX) { set_err("more than 2^31-1 particles"); return BT_ERR_PARAM; }
+    const int nt = (int)nt64, ns = (int)ns64;
+    if (nt < 1 || ns < 1) { set_err("a session needs at least one target and one source"); return BT_ERR_PARAM; }
+    bt_params prm;
+    bt_params_setup(&prm, kernel, 1, &kernelParam, SKIPPING, approximation, compute_type, theta, interpOrder,
+                    maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
+    int rc = validate(nt, ns, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue, sourceX, prm);
+    if (rc != BT_OK) return rc;
+    if (opts && opts->tree_build == BT_TREE_HOST) {
+        set_err("sessions build their trees on the GPU");
+        return BT_ERR_UNSUPPORTED;
+    }
+    bool learned = false, queue = false;
+    double tol = 1e-6;
+    rc = parse_options(opts, prm, learned, tol, queue);
+    if (rc != BT_OK) return rc;
+    const int device = opts ? opts->device : 0;
+    DeviceCtx *ctx = nullptr;
+    rc = get_ctx(device, &ctx);
+    if (rc != BT_OK) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t st = ctx->stream;
+    Session *S = new Session;
+    S->device = device;
+    S->ctx = ctx;
+    S->on_dev = opts && opts->inputs_on_device;
+    S->ns = ns;
+    S->nt = nt;
+    double t0 = now_ms();
+    bt_plan pl;
+    memset(&pl, 0, sizeof pl);
+    pl.prm = prm;
+    DevParts dp;
+    rc = build_plan_gpu(ctx, S->tree_arena, pl, sys, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+                        S->on_dev, dp);
+    if (rc == BT_OK) {
+        count_interactions(pl, &S->base);
+        if (learned) {
+            rc = select_degrees(ctx, S->arena, pl, tol, &dp);
+            if (rc == BT_OK) count_learned(pl, &S->base);
+        }
+    }
+    if (rc == BT_OK)
+        rc = run_plan(ctx, S->arena, pl, nullptr, true, nullptr, &dp, queue, &S->v, false);
+    const int *sorder = dp.sorder;
+    bt_plan_free(&pl);
+    if (rc == BT_OK && cudaMalloc(&S->d_qin, sizeof(double) * (size_t)ns) != cudaSuccess) {
+        cudaGetLastError();
+        set_err("device allocation for the session's charges failed");
+        rc = BT_ERR_CUDA;
+    }
+    for (int i = 0; rc == BT_OK && i < 5; i++)
+        if (cudaEventCreate(&S->ev[i]) != cudaSuccess) { set_err("event creation failed"); rc = BT_ERR_CUDA; }
+    if (rc == BT_OK) {
+        // capture: charges into tree order, then the whole device sequence
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            bt::launch_gather(ns, sorder, S->d_qin, (double *)S->v.d_sq, st);
+            long long launches = 1;
+            int rc2 = issue_plan(S->v, st, S->ev, S->v.d_out, launches);
+            e = cudaStreamEndCapture(st, &S->graph);
+            if (rc2 != BT_OK) rc = rc2;
+            S->graph_kernels = launches;
+        }
+        if (rc == BT_OK && e == cudaSuccess) e = cudaGraphInstantiate(&S->exec, S->graph, 0);
+        if (rc == BT_OK && e != cudaSuccess) {
+            set_err("graph capture failed: %s", cudaGetErrorString(e));
+            rc = BT_ERR_CUDA;
+        }
+    }
+    if (rc != BT_OK) {
+        cudaGetLastError();
+        session_free(S);
+        return rc;
+    }
+    S->base.ms_setup = now_ms() - t0;
+    S->base.source_nodes = S->v.S_n;
+    S->base.target_nodes = S->v.T_n;
+    S->base.kernel_launches = (int)S->graph_kernels;
+    *session = reinterpret_cast<bt_session *>(S);
+    return BT_OK;
+}
+
+int bt_session_eval(bt_session *session, const double *sourceValue, double *outputArray, bt_report *report)
+{
+    g_err[0] = 0;
+    Session *S = reinterpret_cast<Session *>(session);
+    if (!S || !sourceValue || !outputArray) { set_err("session, charges and output are required"); return BT_ERR_PARAM; }
+    std::lock_guard<std::mutex> lk(S->ctx->mu);
+    if (cudaSetDevice(S->device) != cudaSuccess) { set_err("cudaSetDevice failed"); return BT_ERR_CUDA; }
+    cudaStream_t st = S->ctx->stream;
+    const double t0 = now_ms();
+    const cudaMemcpyKind in = S->on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out = S->on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    cudaError_t e = cudaMemcpyAsync(S->d_qin, sourceValue, sizeof(double) * (size_t)S->ns, in, st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(S->exec, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(outputArray, S->v.d_out, sizeof(double) * (size_t)S->nt, out, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        set_err("session evaluation failed: %s", cudaGetErrorString(e));
+        return BT_ERR_CUDA;
+    }
+    g_launches += S->graph_kernels;
+    if (report) {
+        *report = S->base;
+        float a = 0, b = 0, c = 0, d = 0;
+        cudaEventElapsedTime(&a, S->ev[0], S->ev[1]);
+        cudaEventElapsedTime(&b, S->ev[1], S->ev[2]);
+        cudaEventElapsedTime(&c, S->ev[2], S->ev[3]);
+        cudaEventElapsedTime(&d, S->ev[3], S->ev[4]);
+        report->ms_upward = a;
+        report->ms_compute = b + c;
+        report->ms_downward = d;
+        report->ms_eval_kernel = c;
+        report->ms_total = now_ms() - t0;
+        report->ms_transfer = report->ms_total - (a + b + c + d);
+        report->ms_setup = 0.0;
+    }
+    return BT_OK;
+}
+
+int bt_session_destroy(bt_session *session)
+{
+    Session *S = reinterpret_cast<Session *>(session);
+    if (!S) return BT_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->ctx->mu);
+        session_free(S);
+    }
+    return BT_OK;
 }
 
 }  // extern "C"

@@ -81,6 +81,76 @@ k_p2m_lagrange(int n, const int *__restrict__ leaves, const int *__restrict__ ib
     }
 }
 
+// P2M in separable form.  Q[k1,k2,k3] = sum_i (q_i Lx_i[k1]) (Ly_i[k2] Lz_i[k3]):
+// each thread owns whole (k2,k3) columns with all n+1 k1 entries in
+// registers, so per particle it forms one product Ly*Lz and n+1 FMAs against
+// q*Lx values that every thread of the warp reads from the same shared
+// address.  FP64, with the exact-node rule inside lagrange_basis.
+constexpr int P2S_THREADS = 128;
+constexpr int P2S_CHUNK = 64;
+
+template <int NP1>
+__global__ void __launch_bounds__(P2S_THREADS)
+k_p2m_sep(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int *__restrict__ numpar,
+          const double *__restrict__ grid, const double *__restrict__ sx, const double *__restrict__ sy,
+          const double *__restrict__ sz, const double *__restrict__ sq, double *__restrict__ Q)
+{
+    constexpr int n = NP1 - 1, COLS = NP1 * NP1, P = COLS * NP1;
+    constexpr int CPT = (COLS + P2S_THREADS - 1) / P2S_THREADS;
+    const int node = leaves[blockIdx.x];
+    __shared__ double nodes[3 * NP1];
+    __shared__ double A[P2S_CHUNK][NP1], Ly[P2S_CHUNK][NP1], Lz[P2S_CHUNK][NP1];
+    for (int i = threadIdx.x; i < 3 * NP1; i += blockDim.x) nodes[i] = grid[(size_t)node * 3 * NP1 + i];
+    double acc[CPT][NP1];
+    int k2[CPT], k3[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        const int col = threadIdx.x + c * P2S_THREADS;
+        k2[c] = col < COLS ? col % NP1 : 0;
+        k3[c] = col < COLS ? col / NP1 : 0;
+#pragma unroll
+        for (int k = 0; k < NP1; k++) acc[c][k] = 0.0;
+    }
+    __syncthreads();
+    const int b = ibeg[node], m = numpar[node];
+    for (int c0 = 0; c0 < m; c0 += P2S_CHUNK) {
+        const int cm = min(P2S_CHUNK, m - c0);
+        for (int w = threadIdx.x; w < cm * 3; w += blockDim.x) {
+            const int i = w / 3, ax = w % 3;
+            const double *src = ax == 0 ? sx : ax == 1 ? sy : sz;
+            double L[MAXNP];
+            lagrange_basis(n, nodes + ax * NP1, src[b + c0 + i], L);
+            if (ax == 0) {
+                const double qi = sq[b + c0 + i];
+#pragma unroll
+                for (int k = 0; k < NP1; k++) A[i][k] = qi * L[k];
+            } else {
+                double *dst = ax == 1 ? Ly[i] : Lz[i];
+#pragma unroll
+                for (int k = 0; k < NP1; k++) dst[k] = L[k];
+            }
+        }
+        __syncthreads();
+        for (int i = 0; i < cm; i++) {
+#pragma unroll
+            for (int c = 0; c < CPT; c++) {
+                const double bb = Ly[i][k2[c]] * Lz[i][k3[c]];
+#pragma unroll
+                for (int k = 0; k < NP1; k++) acc[c][k] = fma(A[i][k], bb, acc[c][k]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        const int col = threadIdx.x + c * P2S_THREADS;
+        if (col < COLS) {
+#pragma unroll
+            for (int k = 0; k < NP1; k++) Q[(size_t)node * P + k + NP1 * col] = acc[c][k];
+        }
+    }
+}
+
 // Per-axis basis matrix M[i][k] = L_k(child node i) of a parent grid
 // evaluated at a child's grid coordinates, for all three axes, into smem.
 __device__ void axis_matrices(int n, const double *pnodes, const double *cnodes, double *M)
@@ -615,6 +685,17 @@ void launch_scatter(int n, const int *order, const double *src, double *dst, cud
     if (n > 0) k_scatter<<<(n + 255) / 256, 256, 0, st>>>(n, order, src, dst);
 }
 
+__global__ void k_gather(int n, const int *__restrict__ order, const double *__restrict__ src, double *__restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[order[i]];
+}
+
+void launch_gather(int n, const int *order, const double *src, double *dst, cudaStream_t st)
+{
+    if (n > 0) k_gather<<<(n + 255) / 256, 256, 0, st>>>(n, order, src, dst);
+}
+
 // Returns device milliseconds of one probe launch; ops = launched FMA/rsqrt count.
 float run_probe(int which, int sms, double *ops, void *scratch, cudaStream_t st)
 {
@@ -652,8 +733,14 @@ void launch_p2m(int n, bool hermite, int nleaves, const int *leaves, int nnodes,
                 const double *sz, const double *sq, double *Q, cudaStream_t st)
 {
     if (!hermite) {
-        if (nleaves > 0)
-            k_p2m_lagrange<<<nleaves, P2M_THREADS, 0, st>>>(n, leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q);
+        if (nleaves <= 0) return;
+        switch (n + 1) {
+#define BT_P2S(N) case N: k_p2m_sep<N><<<nleaves, P2S_THREADS, 0, st>>>(leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q); return;
+            BT_P2S(2) BT_P2S(3) BT_P2S(4) BT_P2S(5) BT_P2S(6) BT_P2S(7) BT_P2S(8)
+            BT_P2S(9) BT_P2S(10) BT_P2S(11) BT_P2S(12) BT_P2S(13)
+#undef BT_P2S
+        }
+        k_p2m_lagrange<<<nleaves, P2M_THREADS, 0, st>>>(n, leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q);
     } else {
         if (nnodes > 0)
             k_p2m_hermite<<<nnodes, HP2M_THREADS, 0, st>>>(n, ibeg, numpar, grid, box_len, ww, sx, sy, sz, sq, Q);

@@ -48,6 +48,8 @@ void launch_l2p(int n, bool hermite, int nitems, const int2 *items, const int *l
                 const double *ww, const double *Phi, const double *tx, const double *ty, const double *tz,
                 double *pot, cudaStream_t st);
 void launch_scatter(int n, const int *order, const double *src, double *dst, cudaStream_t st);
+// dst[i] = src[order[i]] (inputs in caller order -> tree order)
+void launch_gather(int n, const int *order, const double *src, double *dst, cudaStream_t st);
 float run_probe(int which, int sms, double *ops, void *scratch, cudaStream_t st);
 void launch_direct(int kernel, int nt, int ns, const double *tx, const double *ty, const double *tz,
                    const double *sx, const double *sy, const double *sz, const double *sq, double kp, double *out,

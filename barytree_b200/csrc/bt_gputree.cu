@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -234,17 +235,17 @@ int preorder(const std::vector<HNode> &nodes, int i, int next, std::vector<int> 
 
 // Nodes of one level: at most 8 per split node of the level above, and a
 // split node holds more than maxpar particles.
-size_t level_nodes_max(int n, int maxpar)
+size_t level_nodes_max(int n, int maxpar, int nsys)
 {
     size_t split = (size_t)n / ((size_t)(maxpar > 0 ? maxpar : 1) + 1);
-    return std::min((size_t)n, 8 * split + 8) + 1;
+    return std::max((size_t)nsys, std::min((size_t)n, 8 * split + 8)) + 1;
 }
 
 }  // namespace
 
-size_t gpu_tree_work_bytes(int n, int maxpar, bool with_q)
+size_t gpu_tree_work_bytes(int n, int maxpar, bool with_q, int nsys)
 {
-    const size_t L = level_nodes_max(n, maxpar), C = (size_t)n / GT_CHUNK + L;
+    const size_t L = level_nodes_max(n, maxpar, nsys), C = (size_t)n / GT_CHUNK + L;
     const size_t per = (with_q ? 4 : 3) * sizeof(double) + sizeof(int);
     return per * (size_t)n + (size_t)n            // second copy of the particles, slot codes
            + L * (2 * 3 * 8 + 4 * 8 * 4 + 3 * 8 + 3)  // boxes, part counts, mids, axes
@@ -255,11 +256,24 @@ size_t gpu_tree_work_bytes(int n, int maxpar, bool with_q)
 int gpu_build_tree(int n, const double *x, const double *y, const double *z, const double *q, int maxpar,
                    GtArrays A, void *work, size_t work_bytes, bt_tree *t, cudaStream_t st, long long *launches)
 {
+    int64_t off[2] = {0, n};
+    return gpu_build_forest(1, off, x, y, z, q, maxpar, A, work, work_bytes, t, st, launches);
+}
+
+int gpu_build_forest(int nsys, const int64_t *sys_off, const double *x, const double *y, const double *z,
+                     const double *q, int maxpar, GtArrays A, void *work, size_t work_bytes, bt_tree *t,
+                     cudaStream_t st, long long *launches)
+{
     memset(t, 0, sizeof(*t));
     t->max_depth = 1;
-    if (n <= 0) return 0;
+    bt_tree_set_roots(t, nsys);
+    const int n = (int)sys_off[nsys];
+    if (n <= 0) {
+        t->leaf_off = (int *)calloc((size_t)nsys + 1, sizeof(int));
+        return 0;
+    }
     const bool with_q = q != nullptr;
-    if (gpu_tree_work_bytes(n, maxpar, with_q) > work_bytes) return (int)cudaErrorMemoryAllocation;
+    if (gpu_tree_work_bytes(n, maxpar, with_q, nsys) > work_bytes) return (int)cudaErrorMemoryAllocation;
     char *p = (char *)work;
     auto take = [&](size_t bytes) { char *r = p; p += (bytes + 255) & ~size_t(255); return (void *)r; };
     GtArrays B;
@@ -267,7 +281,7 @@ int gpu_build_tree(int n, const double *x, const double *y, const double *z, con
     B.q = with_q ? (double *)take(8 * (size_t)n) : nullptr; B.order = (int *)take(4 * (size_t)n);
     if (!with_q) A.q = nullptr;
     unsigned char *code = (unsigned char *)take((size_t)n);
-    const size_t nodes_max = level_nodes_max(n, maxpar), chunks_max = (size_t)n / GT_CHUNK + nodes_max;
+    const size_t nodes_max = level_nodes_max(n, maxpar, nsys), chunks_max = (size_t)n / GT_CHUNK + nodes_max;
     unsigned long long *kmin = (unsigned long long *)take(3 * 8 * nodes_max);
     unsigned long long *kmax = (unsigned long long *)take(3 * 8 * nodes_max);
     int *cnt[3];
@@ -287,8 +301,13 @@ int gpu_build_tree(int n, const double *x, const double *y, const double *z, con
     (*launches)++;
 
     std::vector<HNode> nodes;
-    nodes.push_back(HNode{0, n, 0, -1, 0, {0}, {0}});
-    int lo = 0, hi = 1, depth = 1;
+    std::vector<int> root_node(nsys, -1);
+    for (int k = 0; k < nsys; k++) {
+        if (sys_off[k + 1] <= sys_off[k]) continue;
+        root_node[k] = (int)nodes.size();
+        nodes.push_back(HNode{(int)sys_off[k], (int)(sys_off[k + 1] - sys_off[k]), 0, -1, 0, {0}, {0}});
+    }
+    int lo = 0, hi = (int)nodes.size(), depth = 1;
     std::vector<int> hc_node, hc_begin, hc_len, hc_off;
     std::vector<unsigned long long> hkmin, hkmax;
     std::vector<int> hcnt, hchist;
@@ -435,7 +454,11 @@ int gpu_build_tree(int n, const double *x, const double *y, const double *z, con
     // pre-order numbering and the flattened tree (as bt_tree.c)
     const int nn = (int)nodes.size();
     std::vector<int> pre(nn);
-    preorder(nodes, 0, 0, pre);
+    for (int k = 0, next = 0; k < nsys; k++)
+        if (root_node[k] >= 0) {
+            t->roots[k] = next;
+            next = preorder(nodes, root_node[k], next, pre);
+        }
     std::vector<HNode> pn(nn);
     for (int i = 0; i < nn; i++) pn[pre[i]] = nodes[i];
     bt_tree_alloc(t, nn);

@@ -23,7 +23,9 @@ typedef struct {
     int *order;
 } bt_parts;
 
-/* Flattened tree (struct Tree, src/tree/struct_tree.h:4-43).  ibeg is 0-based. */
+/* Flattened tree (struct Tree, src/tree/struct_tree.h:4-43).  ibeg is 0-based.
+ * A forest of independent systems' trees (batched evaluation) is one bt_tree
+ * whose systems' nodes are numbered consecutively, each system in pre-order. */
 typedef struct {
     int n, cap, max_depth;
     int *ibeg, *numpar, *nchild, *child, *parent, *level;
@@ -32,6 +34,9 @@ typedef struct {
     int *leaves;          /* DFS order (Tree_Fill_Levels, src/tree/tree.c:122-153)  */
     int *lvl_off;         /* max_depth+1 offsets into lvl_nodes                         */
     int *lvl_nodes;       /* non-leaf nodes grouped by level, DFS order within a level  */
+    int nroots;           /* systems                                                    */
+    int *roots;           /* per system: its root node, -1 for a system with no particles */
+    int *leaf_off;        /* nroots+1 offsets: system k's leaves are leaves[leaf_off[k] ..) */
 } bt_tree;
 
 /* Compressed row storage: row r holds idx[off[r] .. off[r+1]). */
@@ -76,12 +81,16 @@ void bt_params_setup(bt_params *o, int kernel, int nkp, const double *kp, int si
 void bt_parts_init(bt_parts *p, int n, const double *x, const double *y, const double *z, const double *q);
 void bt_parts_free(bt_parts *p);
 void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode);
+/* Forest of nsys systems: system k holds particles [sys_off[k], sys_off[k+1]). */
+void bt_forest_build(bt_tree *t, bt_parts *p, int nsys, const int64_t *sys_off, int maxparnode);
 void bt_tree_free(bt_tree *t);
 void bt_tree_copy(bt_tree *dst, const bt_tree *src);
 /* Node arrays for n nodes (n, cap set), and the leaf / per-level lists of a
- * tree whose node arrays and max_depth are filled. */
+ * tree whose node arrays, max_depth and roots are filled. */
 void bt_tree_alloc(bt_tree *t, int n);
 void bt_tree_finish(bt_tree *t);
+/* The roots array for nsys systems (all -1). */
+void bt_tree_set_roots(bt_tree *t, int nsys);
 
 /* bt_lists.c */
 void bt_csr_free(bt_csr *c);

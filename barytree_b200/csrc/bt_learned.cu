@@ -24,10 +24,14 @@ namespace bt {
 // ---------------------------------------------------------------------------
 // node charge moments and interaction features
 // ---------------------------------------------------------------------------
-__global__ void k_node_moments(int nnodes, const int *__restrict__ ibeg, const int *__restrict__ numpar,
-                               const double *__restrict__ q, double *__restrict__ mom)
+// Charge moments of every node: sum |q| and sqrt(sum q^2).  Leaves sum their
+// particles (one block per leaf); every other node sums its children, level
+// by level from the deepest (a fixed order, so the features are the same
+// bits on every call).
+__global__ void k_leaf_moments(int nleaves, const int *__restrict__ leaves, const int *__restrict__ ibeg,
+                               const int *__restrict__ numpar, const double *__restrict__ q, double *__restrict__ mom)
 {
-    const int node = blockIdx.x;
+    const int node = leaves[blockIdx.x];
     double a = 0.0, b = 0.0;
     for (int i = ibeg[node] + threadIdx.x; i < ibeg[node] + numpar[node]; i += blockDim.x) {
         double v = q[i];
@@ -42,7 +46,29 @@ __global__ void k_node_moments(int nnodes, const int *__restrict__ ibeg, const i
         if (threadIdx.x < s) { sa[threadIdx.x] += sa[threadIdx.x + s]; sb[threadIdx.x] += sb[threadIdx.x + s]; }
         __syncthreads();
     }
-    if (threadIdx.x == 0) { mom[2 * node] = sa[0]; mom[2 * node + 1] = sqrt(sb[0]); }
+    if (threadIdx.x == 0) { mom[2 * node] = sa[0]; mom[2 * node + 1] = sb[0]; }
+}
+
+__global__ void k_moments_up(int cnt, const int *__restrict__ nodes, const int *__restrict__ nchild,
+                             const int *__restrict__ child, double *__restrict__ mom)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cnt) return;
+    const int node = nodes[k];
+    double a = 0.0, b = 0.0;
+    for (int c = 0; c < nchild[node]; c++) {
+        const int ch = child[8 * node + c];
+        a += mom[2 * ch];
+        b += mom[2 * ch + 1];
+    }
+    mom[2 * node] = a;
+    mom[2 * node + 1] = b;
+}
+
+__global__ void k_moments_sqrt(int n, double *__restrict__ mom)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) mom[2 * k + 1] = sqrt(mom[2 * k + 1]);
 }
 
 __device__ __forceinline__ void features_of(const FeatureArgs &a, int tnode, int snode, float *f)
@@ -334,9 +360,23 @@ void gather_rows(int B, int width, const int *rows, const float *src, float *dst
     k_gather_rows<<<nb((long long)B * width, 256), 256, 0, st>>>(B, width, rows, src, dst);
 }
 
-void launch_node_moments(int nnodes, const int *ibeg, const int *numpar, const double *q, double *mom, cudaStream_t st)
+int launch_node_moments(const MomentTree &t, const double *q, double *mom, cudaStream_t st)
 {
-    if (nnodes > 0) k_node_moments<<<nnodes, 256, 0, st>>>(nnodes, ibeg, numpar, q, mom);
+    if (t.nnodes <= 0) return 0;
+    int launches = 0;
+    if (t.nleaves > 0) {
+        k_leaf_moments<<<t.nleaves, 256, 0, st>>>(t.nleaves, t.leaves, t.ibeg, t.numpar, q, mom);
+        launches++;
+    }
+    for (int l = t.max_depth - 1; l >= 0; l--) {
+        const int cnt = t.lvl_off[l + 1] - t.lvl_off[l];
+        if (cnt > 0) {
+            k_moments_up<<<nb(cnt, 128), 128, 0, st>>>(cnt, t.lvl_nodes + t.lvl_off[l], t.nchild, t.child, mom);
+            launches++;
+        }
+    }
+    k_moments_sqrt<<<nb(t.nnodes, 256), 256, 0, st>>>(t.nnodes, mom);
+    return launches + 1;
 }
 
 void launch_features(const FeatureArgs &a, int64_t nentries, float *out, cudaStream_t st)

@@ -45,7 +45,15 @@ void mlp_forward_backward(const float *w, int B, const float *X, const float *Y,
                           float *lossb, float *grad, cudaStream_t st);
 void mlp_adam(int n, float *w, const float *g, float *m, float *v, float lr, int step, cudaStream_t st);
 void gather_rows(int B, int width, const int *rows, const float *src, float *dst, cudaStream_t st);
-void launch_node_moments(int nnodes, const int *ibeg, const int *numpar, const double *q, double *mom, cudaStream_t st);
+// Source tree on the device for the node moments (lvl_off is a host array).
+struct MomentTree {
+    int nnodes, nleaves, max_depth;
+    const int *leaves, *ibeg, *numpar, *nchild, *child, *lvl_nodes;
+    const int *lvl_off;
+};
+// mom[2 i] = sum |q|, mom[2 i + 1] = sqrt(sum q^2) over node i's particles.
+// Returns the number of kernel launches.
+int launch_node_moments(const MomentTree &t, const double *q, double *mom, cudaStream_t st);
 void launch_features(const FeatureArgs &a, int64_t nentries, float *out, cudaStream_t st);
 void launch_features_pairs(const FeatureArgs &a, int n, const int *tnodes, const int *snodes, float *out,
                            cudaStream_t st);

@@ -51,11 +51,12 @@ static void csr_from_vecs(bt_csr *c, ivec *v, int rows)
 
 /* pc_compute_interaction_list: depth-first, children in order; an explicit
  * stack visits nodes in the same order as the reference's recursion. */
-static void pc_traverse(const bt_tree *t, double br, double bx, double by, double bz,
+static void pc_traverse(const bt_tree *t, int root, double br, double bx, double by, double bz,
                         const bt_params *o, ivec *ap, ivec *pp, int *stack)
 {
     int sp = 0;
-    stack[sp++] = 0;
+    if (root < 0) return;
+    stack[sp++] = root;
     double thr = o->size_check * o->P;
     while (sp) {
         int node = stack[--sp];
@@ -135,8 +136,15 @@ void bt_plan_lists(bt_plan *pl)
             int *stack = malloc(sizeof(int) * (size_t)(8 * trav->n + 8));
 #pragma omp for schedule(dynamic, 8)
             for (int i = 0; i < nb; i++) {
+                /* the batch's system: the other side's tree of the same system */
+                int lo = 0, hi = bat->nroots;
+                while (hi - lo > 1) {
+                    int m = (lo + hi) / 2;
+                    if (bat->leaf_off[m] <= i) lo = m; else hi = m;
+                }
                 int b = bat->leaves[i];
-                pc_traverse(trav, bat->rad[b], bat->xm[b], bat->ym[b], bat->zm[b], o, &ap[i], &pp[i], stack);
+                pc_traverse(trav, trav->roots[lo], bat->rad[b], bat->xm[b], bat->ym[b], bat->zm[b], o, &ap[i],
+                            &pp[i], stack);
             }
             free(stack);
         }
@@ -147,7 +155,11 @@ void bt_plan_lists(bt_plan *pl)
     } else {
         int nt = pl->tt.n;
         cc_out L = {vecs(nt), vecs(nt), vecs(nt), vecs(nt)};
-        if (pl->st.n > 0 && nt > 0) cc_traverse(&pl->st, 0, &pl->tt, 0, o, &L);
+        /* one dual traversal per system (src/interaction_lists/interaction_lists.c:537-748) */
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int k = 0; k < pl->st.nroots; k++)
+            if (pl->st.roots[k] >= 0 && pl->tt.roots[k] >= 0)
+                cc_traverse(&pl->st, pl->st.roots[k], &pl->tt, pl->tt.roots[k], o, &L);
         csr_from_vecs(&pl->pp, L.pp, nt);
         csr_from_vecs(&pl->ap, L.ap, nt);
         csr_from_vecs(&pl->pc, L.pc, nt);

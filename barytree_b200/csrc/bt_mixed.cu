@@ -70,6 +70,13 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
 }
 
 constexpr int MX_THREADS = 128;
+// Register budget of the evaluation kernels: BT_MX_MIN_BLOCKS resident blocks
+// per SM (unset: the compiler's choice).
+#ifdef BT_MX_MIN_BLOCKS
+#define BT_MX_BOUNDS __launch_bounds__(MX_THREADS, BT_MX_MIN_BLOCKS)
+#else
+#define BT_MX_BOUNDS __launch_bounds__(MX_THREADS)
+#endif
 constexpr int MX_TPT = 2;                       // targets per thread
 constexpr int MX_CHUNK = MX_THREADS * MX_TPT;   // targets per work item
 constexpr int MX_TILE = 1024;
@@ -140,70 +147,159 @@ __device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, con
 // the close pair's magnitude).  Close pairs occur only between leaves whose
 // boxes lie within that distance (flagged per near-field entry); the other
 // entries run pp_tile_far with no test at all.
-__device__ __forceinline__ float pair_r2(float x, float y, float z, float4 p)
+// Packed FP32 pairs (sm_100 f32x2 instructions): one instruction applies the
+// same operation to two FP32 values held in a 64-bit register pair, which
+// halves the issue slots of the near-field arithmetic.  Flush-to-zero like
+// the rest of this file.
+typedef unsigned long long f2_t;
+
+__device__ __forceinline__ f2_t f2_make(float lo, float hi)
 {
-    float dx = x - p.x, dy = y - p.y, dz = z - p.z;
-    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    f2_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_split(f2_t v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b)
+{
+    f2_t r;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b)
+{
+    f2_t r;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c)
+{
+    f2_t r;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
 }
 
+// Near-field source tile in shared memory, structure of arrays (x', y', z'
+// relative to the source leaf centre, q), padded to a multiple of 4 with
+// charge-free sources far away.
+struct Tile {
+    float *x, *y, *z, *q;
+};
+
+constexpr float MX_PAD_POS = 1.0e18f;   // r2 ~ 1e36 < FLT_MAX; with q = 0 it adds nothing
+
+// Two sources (a pair) against one target, accumulated into the pair sum S.
+// kc: mixed_kernel_constant(); kc2 = {kc, kc}.
 template <int KT>
-__device__ __forceinline__ void pp_tile_far(const float4 *tile, int cm, const float *x, const float *y,
-                                            const float *z, float kc, float *s)
+__device__ __forceinline__ f2_t kf2_acc(f2_t r2, f2_t q, f2_t S, f2_t kc2)
 {
-#pragma unroll 4
-    for (int i = 0; i < cm; i++) {
-        float4 p = tile[i];
+    if (KT == 3) r2 = f2_fma(f2_make(1.0f, 1.0f), kc2, r2);   // r2 + eps^2
+    float a, b;
+    f2_split(r2, a, b);
+    const f2_t rinv = f2_make(rsqrt_apx(a), rsqrt_apx(b));
+    if (KT != 2) return f2_fma(q, rinv, S);
+    // Yukawa as kf_far: one Newton step on 1/r, then exp(-kappa r) by ex2
+    const f2_t h = f2_mul(r2, rinv);
+    const f2_t t = f2_fma(f2_mul(h, f2_make(-0.5f, -0.5f)), rinv, f2_make(1.5f, 1.5f));
+    float e0, e1;
+    f2_split(f2_mul(kc2, f2_mul(h, t)), e0, e1);
+    const f2_t e = f2_make(ex2_apx(e0), ex2_apx(e1));
+    return f2_fma(q, f2_mul(f2_mul(rinv, t), e), S);
+}
+
+// One tile against the thread's MX_TPT targets (x, y, z in the source
+// leaf's frame).  NEAR: also the smallest r2 per target (mn), which tells
+// whether the tile holds a close pair.
+template <int KT, bool NEAR>
+__device__ __forceinline__ void pp_tile(const Tile tl, int cm4, const float *x, const float *y, const float *z,
+                                        float kc, float *s, float *mn)
+{
+    f2_t X[MX_TPT], Y[MX_TPT], Z[MX_TPT], S[MX_TPT];
 #pragma unroll
-        for (int t = 0; t < MX_TPT; t++) s[t] += kf_far<KT>(pair_r2(x[t], y[t], z[t], p), p.w, kc);
+    for (int t = 0; t < MX_TPT; t++) {
+        X[t] = f2_make(x[t], x[t]);
+        Y[t] = f2_make(y[t], y[t]);
+        Z[t] = f2_make(z[t], z[t]);
+        S[t] = f2_make(0.0f, 0.0f);
     }
-}
-
-// Tile of a flagged entry: FP32 sum over the pairs at or beyond the close
-// distance (which also drops coincident pairs, r2 == 0); mn = smallest r2.
-template <int KT>
-__device__ __forceinline__ void pp_tile_near(const float4 *tile, int cm, const float *x, const float *y,
-                                             const float *z, float kc, float thr2, float *s, float *mn)
-{
-#pragma unroll 4
-    for (int i = 0; i < cm; i++) {
-        float4 p = tile[i];
+    const f2_t kc2 = f2_make(kc, kc);
+#pragma unroll 2
+    for (int i = 0; i < cm4; i += 4) {
+        const ulonglong2 PX = *reinterpret_cast<const ulonglong2 *>(tl.x + i);
+        const ulonglong2 PY = *reinterpret_cast<const ulonglong2 *>(tl.y + i);
+        const ulonglong2 PZ = *reinterpret_cast<const ulonglong2 *>(tl.z + i);
+        const ulonglong2 PQ = *reinterpret_cast<const ulonglong2 *>(tl.q + i);
 #pragma unroll
-        for (int t = 0; t < MX_TPT; t++) {
-            float r2 = pair_r2(x[t], y[t], z[t], p);
-            mn[t] = fminf(mn[t], r2);
-            float v = kf_far<KT>(r2, p.w, kc);
-            s[t] += r2 >= thr2 ? v : 0.0f;
+        for (int hh = 0; hh < 2; hh++) {
+            const f2_t px = hh ? PX.y : PX.x, py = hh ? PY.y : PY.x, pz = hh ? PZ.y : PZ.x, pq = hh ? PQ.y : PQ.x;
+#pragma unroll
+            for (int t = 0; t < MX_TPT; t++) {
+                const f2_t dx = f2_sub(X[t], px), dy = f2_sub(Y[t], py), dz = f2_sub(Z[t], pz);
+                const f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
+                if (NEAR) {
+                    float a, b;
+                    f2_split(r2, a, b);
+                    mn[t] = fminf(mn[t], fminf(a, b));
+                }
+                S[t] = kf2_acc<KT>(r2, pq, S[t], kc2);
+            }
         }
     }
+#pragma unroll
+    for (int t = 0; t < MX_TPT; t++) {
+        float a, b;
+        f2_split(S[t], a, b);
+        s[t] = a + b;
+    }
 }
 
-// The close pairs of one target in a tile, in FP64 with the reference's
-// skipping rule (k_pp).  The same FP32 test as pp_tile_near selects them.
+// A tile holding a close pair for this target, again in scalar form: the
+// FP32 sum over the pairs at or beyond the close distance (which also drops
+// coincident pairs, r2 == 0), and the close pairs in FP64 from the FP64
+// coordinates and charges with the reference's skipping rule (k_pp).
 template <int KT>
-__device__ __forceinline__ double pp_close_fp64(const float4 *tile, int cm, float x, float y, float z, float thr2,
-                                             double xd, double yd, double zd, const double *__restrict__ sx,
-                                             const double *__restrict__ sy, const double *__restrict__ sz,
-                                             const double *__restrict__ sq, int base, double kp)
+__device__ __noinline__ float pp_tile_close(const Tile tl, int cm, float x, float y, float z, float kc, float thr2,
+                                            double xd, double yd, double zd, const double *__restrict__ sx,
+                                            const double *__restrict__ sy, const double *__restrict__ sz,
+                                            const double *__restrict__ sq, int base, double kp, double *acc)
 {
-    double acc = 0.0;
+    float s = 0.0f;
+    double a = 0.0;
     for (int i = 0; i < cm; i++) {
-        if (pair_r2(x, y, z, tile[i]) < thr2) {
+        const float dx = x - tl.x[i], dy = y - tl.y[i], dz = z - tl.z[i];
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (r2 >= thr2) {
+            s += kf_far<KT>(r2, tl.q[i], kc);
+        } else {
             const int gi = base + i;
-            double dx = xd - sx[gi], dy = yd - sy[gi], dz = zd - sz[gi];
-            acc += k_pp<KT>(dx * dx + dy * dy + dz * dz, sq[gi], kp);
+            const double ex = xd - sx[gi], ey = yd - sy[gi], ez = zd - sz[gi];
+            a += k_pp<KT>(ex * ex + ey * ey + ez * ez, sq[gi], kp);
         }
     }
-    return acc;
+    *acc += a;
+    return s;
 }
 
 // Particle-output evaluation, mixed precision.  Each thread owns MX_TPT
 // targets of a work item (target leaf, chunk of MX_CHUNK targets).
-template <int KT>
-__global__ void __launch_bounds__(MX_THREADS)
-k_eval_targets_mixed(MixedTargetsArgs a)
+// Blocks of a work-queue launch take items (cost-sorted, longest first) from
+// a device counter until the queue is empty; without a queue, block b
+// evaluates item b.
+__device__ __forceinline__ int next_item(int *queue, int *slot)
 {
-    extern __shared__ float smf[];
-    const int2 it = a.items[blockIdx.x];
+    if (threadIdx.x == 0) *slot = atomicAdd(queue, 1);
+    __syncthreads();
+    const int w = *slot;
+    __syncthreads();
+    return w;
+}
+
+template <int KT>
+__device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const int2 it, float *smf)
+{
     const int u = it.x;
     const int tnode = a.leaf_node[u];
     const int tb = a.t_ibeg[tnode], tn = a.t_numpar[tnode];
@@ -248,7 +344,7 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         __syncthreads();
     }
     // near field: source leaves, particles relative to their leaf centre
-    float4 *tile = reinterpret_cast<float4 *>(smf);
+    const Tile tl{smf, smf + MX_TILE, smf + 2 * MX_TILE, smf + 3 * MX_TILE};
     for (int64_t e = a.d_off[u]; e < a.d_off[u + 1]; e++) {
         const int s = a.d_idx[e];
         const bool near = a.d_flag[e] != 0;
@@ -261,17 +357,17 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         const double rr = MX_CLOSE_FRAC * (trad + a.s_rad[s]);
         const float thr2 = (float)(rr * rr);
         for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
-            int cm = min(MX_TILE, sn - c0);
-            for (int i = threadIdx.x; i < cm; i += blockDim.x) tile[i] = a.spos[sb + c0 + i];
+            const int cm = min(MX_TILE, sn - c0), cm4 = (cm + 3) & ~3;
+            for (int i = threadIdx.x; i < cm4; i += blockDim.x) {
+                const float4 p = i < cm ? a.spos[sb + c0 + i] : make_float4(MX_PAD_POS, MX_PAD_POS, MX_PAD_POS, 0.0f);
+                tl.x[i] = p.x; tl.y[i] = p.y; tl.z[i] = p.z; tl.q[i] = p.w;
+            }
             __syncthreads();
-            float sum[MX_TPT];
-#pragma unroll
-            for (int t = 0; t < MX_TPT; t++) sum[t] = 0.f;
+            float sum[MX_TPT], mn[MX_TPT];
             if (near) {
-                float mn[MX_TPT];
 #pragma unroll
                 for (int t = 0; t < MX_TPT; t++) mn[t] = FLT_MAX;
-                pp_tile_near<KT>(tile, cm, xs, ys, zs, kc, thr2, sum, mn);
+                pp_tile<KT, true>(tl, cm4, xs, ys, zs, kc, sum, mn);
                 bool close = false;
 #pragma unroll
                 for (int t = 0; t < MX_TPT; t++) close |= act[t] && mn[t] < thr2;
@@ -279,12 +375,12 @@ k_eval_targets_mixed(MixedTargetsArgs a)
 #pragma unroll
                     for (int t = 0; t < MX_TPT; t++)
                         if (act[t] && mn[t] < thr2)
-                            acc[t] += pp_close_fp64<KT>(tile, cm, xs[t], ys[t], zs[t], thr2, a.tx64[tid[t]],
-                                                        a.ty64[tid[t]], a.tz64[tid[t]], a.sx64, a.sy64, a.sz64,
-                                                        a.sq64, sb + c0, a.kp);
+                            sum[t] = pp_tile_close<KT>(tl, cm, xs[t], ys[t], zs[t], kc, thr2, a.tx64[tid[t]],
+                                                       a.ty64[tid[t]], a.tz64[tid[t]], a.sx64, a.sy64, a.sz64,
+                                                       a.sq64, sb + c0, a.kp, &acc[t]);
                 }
             } else {
-                pp_tile_far<KT>(tile, cm, xs, ys, zs, kc, sum);
+                pp_tile<KT, false>(tl, cm4, xs, ys, zs, kc, sum, mn);
             }
 #pragma unroll
             for (int t = 0; t < MX_TPT; t++) acc[t] += (double)sum[t];
@@ -296,15 +392,26 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         if (act[t]) a.pot[tid[t]] = acc[t];
 }
 
+template <int KT>
+__global__ void BT_MX_BOUNDS
+k_eval_targets_mixed(MixedTargetsArgs a)
+{
+    extern __shared__ float smf[];
+    __shared__ int slot;
+    int w = a.queue ? next_item(a.queue, &slot) : blockIdx.x;
+    while (w < a.nitems) {
+        targets_item<KT>(a, a.items[w], smf);
+        if (!a.queue) break;
+        w = next_item(a.queue, &slot);
+    }
+}
+
 // Grid-output evaluation (M2L from source clusters + CP from source leaves)
 // onto the grid of a target node, mixed precision, Lagrange.  One thread per
 // target grid point.
 template <int KT>
-__global__ void __launch_bounds__(MX_THREADS)
-k_eval_grids_mixed(MixedGridsArgs a)
+__device__ __forceinline__ void grids_item(const MixedGridsArgs &a, const int2 it, float *smf)
 {
-    extern __shared__ float smf[];
-    const int2 it = a.items[blockIdx.x];
     const int T = it.x;
     const int np1 = a.n + 1, P = np1 * np1 * np1;
     const int j0 = it.y * MX_THREADS + threadIdx.x;
@@ -358,6 +465,20 @@ k_eval_grids_mixed(MixedGridsArgs a)
     if (active) a.Phi[(size_t)T * P + j0] = acc;
 }
 
+template <int KT>
+__global__ void BT_MX_BOUNDS
+k_eval_grids_mixed(MixedGridsArgs a)
+{
+    extern __shared__ float smf[];
+    __shared__ int slot;
+    int w = a.queue ? next_item(a.queue, &slot) : blockIdx.x;
+    while (w < a.nitems) {
+        grids_item<KT>(a, a.items[w], smf);
+        if (!a.queue) break;
+        w = next_item(a.queue, &slot);
+    }
+}
+
 // Particles relative to the centre of their leaf, FP32 (x', y', z', q).
 __global__ void k_rel_positions(int nleaves, const int *__restrict__ leaves, const int *__restrict__ ibeg,
                                 const int *__restrict__ numpar, const double *__restrict__ ctr,
@@ -397,12 +518,25 @@ static size_t mixed_smem(int max_np1)
     return far > near ? far : near;
 }
 
+// Grid of a work-queue launch: as many blocks as are resident at once.
+template <typename K>
+static int queue_grid(K kernel, size_t smem, int nitems)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, MX_THREADS, smem);
+    int g = sms * (per_sm > 0 ? per_sm : 1);
+    return g < nitems ? g : nitems;
+}
+
 template <int KT>
 static void eval_targets_mixed_t(const MixedTargetsArgs &a, cudaStream_t st)
 {
     size_t sm = mixed_smem(a.max_np1);
     cudaFuncSetAttribute(k_eval_targets_mixed<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_eval_targets_mixed<KT><<<a.nitems, MX_THREADS, sm, st>>>(a);
+    int grid = a.queue ? queue_grid(k_eval_targets_mixed<KT>, sm, a.nitems) : a.nitems;
+    k_eval_targets_mixed<KT><<<grid, MX_THREADS, sm, st>>>(a);
 }
 
 void launch_eval_targets_mixed(int kernel, const MixedTargetsArgs &a, cudaStream_t st)
@@ -418,7 +552,8 @@ static void eval_grids_mixed_t(const MixedGridsArgs &a, cudaStream_t st)
 {
     size_t sm = mixed_smem(a.n + 1);
     cudaFuncSetAttribute(k_eval_grids_mixed<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_eval_grids_mixed<KT><<<a.nitems, MX_THREADS, sm, st>>>(a);
+    int grid = a.queue ? queue_grid(k_eval_grids_mixed<KT>, sm, a.nitems) : a.nitems;
+    k_eval_grids_mixed<KT><<<grid, MX_THREADS, sm, st>>>(a);
 }
 
 void launch_eval_grids_mixed(int kernel, const MixedGridsArgs &a, cudaStream_t st)

@@ -18,6 +18,7 @@ constexpr double MX_CLOSE_FRAC = BT_CLOSE_FRAC;
 struct MixedTargetsArgs {
     int n, max_np1, nitems;
     const int2 *items;
+    int *queue;                                 // work-queue counter (zeroed), or nullptr: one block per item
     const int *leaf_node, *t_ibeg, *t_numpar;
     const double *t_ctr;                        // target node centres (FP64, 3 per node)
     const float4 *tpos;                         // targets relative to their leaf centre
@@ -41,6 +42,7 @@ struct MixedTargetsArgs {
 struct MixedGridsArgs {
     int n, nitems;
     const int2 *items;
+    int *queue;                                 // work-queue counter (zeroed), or nullptr: one block per item
     const double *t_grid, *t_ctr;
     const int64_t *c_off; const int *c_idx;     // M2L source clusters per target node
     const int64_t *p_off; const int *p_idx;     // CP source leaves per target node

@@ -99,7 +99,16 @@ void bt_tree_free(bt_tree *t)
     free(t->x0); free(t->x1); free(t->y0); free(t->y1); free(t->z0); free(t->z1);
     free(t->xm); free(t->ym); free(t->zm); free(t->rad);
     free(t->leaves); free(t->lvl_off); free(t->lvl_nodes);
+    free(t->roots); free(t->leaf_off);
     memset(t, 0, sizeof(*t));
+}
+
+void bt_tree_set_roots(bt_tree *t, int nsys)
+{
+    free(t->roots);
+    t->nroots = nsys;
+    t->roots = malloc(sizeof(int) * (size_t)(nsys > 0 ? nsys : 1));
+    for (int k = 0; k < nsys; k++) t->roots[k] = -1;
 }
 
 typedef struct {
@@ -322,15 +331,30 @@ void bt_tree_finish(bt_tree *t)
     t->lvl_nodes = malloc(sizeof(int) * (size_t)(t->lvl_off[t->max_depth] + 1));
     memset(lvl_cnt, 0, sizeof(int) * (size_t)(t->max_depth + 1));
     int nl = 0;
-    collect(t, 0, &nl, lvl_cnt);
+    t->leaf_off = malloc(sizeof(int) * (size_t)(t->nroots + 1));
+    for (int k = 0; k < t->nroots; k++) {
+        t->leaf_off[k] = nl;
+        if (t->roots[k] >= 0) collect(t, t->roots[k], &nl, lvl_cnt);
+    }
+    t->leaf_off[t->nroots] = nl;
     free(lvl_cnt);
 }
 
 void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
 {
+    int64_t off[2] = {0, p->n};
+    bt_forest_build(t, p, 1, off, maxparnode);
+}
+
+void bt_forest_build(bt_tree *t, bt_parts *p, int nsys, const int64_t *sys_off, int maxparnode)
+{
     memset(t, 0, sizeof(*t));
     t->max_depth = 1;
-    if (p->n <= 0) return;
+    bt_tree_set_roots(t, nsys);
+    if (p->n <= 0) {
+        t->leaf_off = calloc((size_t)nsys + 1, sizeof(int));
+        return;
+    }
     build_ctx c;
     size_t m = (size_t)p->n;
     c.p = p;
@@ -340,11 +364,18 @@ void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
     c.code = malloc(m);
     c.maxpar = maxparnode;
 
-    int cap = 1024, n = 1;
+    int cap = 1024 + nsys, n = 0;
     bnode *nodes = malloc(sizeof(bnode) * (size_t)cap);
-    memset(&nodes[0], 0, sizeof(bnode));
-    nodes[0].ibeg = 0; nodes[0].np = p->n; nodes[0].level = 0; nodes[0].parent = -1;
-    int lo = 0, hi = 1, depth = 1;
+    int *root_node = malloc(sizeof(int) * (size_t)nsys);
+    for (int k = 0; k < nsys; k++) {
+        root_node[k] = -1;
+        if (sys_off[k + 1] <= sys_off[k]) continue;
+        memset(&nodes[n], 0, sizeof(bnode));
+        nodes[n].ibeg = (int)sys_off[k]; nodes[n].np = (int)(sys_off[k + 1] - sys_off[k]);
+        nodes[n].level = 0; nodes[n].parent = -1;
+        root_node[k] = n++;
+    }
+    int lo = 0, hi = n, depth = 1;
     while (lo < hi) {
         for (int i = lo; i < hi; i++)
             if (nodes[i].np >= BT_PAR_NODE) split_node(&nodes[i], &c, 1);
@@ -367,9 +398,18 @@ void bt_tree_build(bt_tree *t, bt_parts *p, int maxparnode)
     }
     free(c.tx); free(c.ty); free(c.tz); free(c.tq); free(c.to); free(c.code);
 
-    /* pre-order numbering (TreeLinkedList_SetIndex, src/tree/tree_linked_list.c:284-293) */
-    int *pre = malloc(sizeof(int) * (size_t)n);
-    preorder(nodes, 0, 0, pre);
+    /* pre-order numbering (TreeLinkedList_SetIndex, src/tree/tree_linked_list.c:284-293),
+     * system after system */
+    int *pre = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    {
+        int next = 0;
+        for (int k = 0; k < nsys; k++)
+            if (root_node[k] >= 0) {
+                t->roots[k] = next;
+                next = preorder(nodes, root_node[k], next, pre);
+            }
+    }
+    free(root_node);
     bt_tree_alloc(t, n);
     t->max_depth = depth;
     for (int i = 0; i < n; i++) {
@@ -395,6 +435,12 @@ void bt_tree_copy(bt_tree *dst, const bt_tree *src)
 {
     memset(dst, 0, sizeof(*dst));
     dst->max_depth = 1;
+    if (src->roots) {
+        bt_tree_set_roots(dst, src->nroots);
+        memcpy(dst->roots, src->roots, sizeof(int) * (size_t)src->nroots);
+        dst->leaf_off = malloc(sizeof(int) * (size_t)(src->nroots + 1));
+        memcpy(dst->leaf_off, src->leaf_off, sizeof(int) * (size_t)(src->nroots + 1));
+    }
     if (src->n <= 0 || !src->lvl_off) return;
     int n = src->n;
     while (dst->cap < n) {

@@ -49,6 +49,11 @@ CONFIGS = {
     3: dict(workload="N=4,000,000 Gaussian sigma 0.25 clipped to [-1,1]^3, charges +-1, Coulomb, particle-cluster "
                      "Hermite n=6, theta 0.7, leaf 1000, size check 4", N=4_000_000, dist="gauss", kernel=1, kp=0.0,
             approx=2, ctype=1, degree=6, theta=0.7, leaf=1000, sc=4.0, sample_n=60_000),
+    4: dict(workload="256 independent systems in one bt_eval_batch call: N log-uniform 1,000-200,000, uniform in "
+                     "the unit cube [0,1]^3, charges U[-1,1], regularized Coulomb eps=1e-3 (self term q/eps "
+                     "included), particle-cluster Lagrange n=7, theta 0.7, leaf 2000, mixed precision",
+            N=None, dist="batch", nsys=256, nmin=1_000, nmax=200_000, kernel=3, kp=1e-3, approx=1, ctype=1,
+            degree=7, theta=0.7, leaf=2000, sc=1.0, sample_n=300_000),
     5: dict(workload="N=16,000,000: 80% in 8 Gaussian blobs (centres U[-0.7,0.7]^3, sigma log-uniform 0.05-0.3, "
                      "clipped to [-1,1]^3), 20% uniform [-1,1]^3, charges U[-1,1], Coulomb, particle-cluster "
                      "Lagrange, theta 0.7, leaf 2000; degree per interaction from the learned selector at 1e-6, "
@@ -57,9 +62,23 @@ CONFIGS = {
 }
 
 
-def make_inputs(cfg, seed):
-    """Seeded synthetic inputs with the configuration's distribution (numpy PCG64)."""
+def batch_sizes(cfg, seed):
+    """Particle counts of a batch: log-uniform between nmin and nmax."""
     rng = np.random.default_rng(seed)
+    nsys = cfg.get("nsys_override", cfg["nsys"])
+    return np.round(np.exp(rng.uniform(np.log(cfg["nmin"]), np.log(cfg["nmax"]), nsys))).astype(np.int64)
+
+
+def make_inputs(cfg, seed):
+    """Seeded synthetic inputs with the configuration's distribution (numpy
+    PCG64): x, y, z, q and, for a batch, the system offsets (else None)."""
+    rng = np.random.default_rng(seed)
+    if cfg["dist"] == "batch":
+        sizes = batch_sizes(cfg, seed)
+        n = int(sizes.sum())
+        x, y, z = (rng.uniform(0, 1, n) for _ in range(3))
+        q = rng.uniform(-1, 1, n)
+        return x, y, z, q, np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
     n = cfg["N"] if "n_override" not in cfg else cfg["n_override"]
     if cfg["dist"] == "uniform":
         x, y, z = (rng.uniform(-1, 1, n) for _ in range(3))
@@ -72,7 +91,7 @@ def make_inputs(cfg, seed):
         x, y, z, q = blobs(n, seed)
     else:
         raise ValueError(cfg["dist"])
-    return x, y, z, q
+    return x, y, z, q, None
 
 
 class ClockSampler:
@@ -127,12 +146,23 @@ def reference_sample_worker(args):
     cfg, seed, n = args
     from oracle import oracle as O
     c = dict(cfg)
-    c["n_override"] = n
-    x, y, z, q = make_inputs(c, seed)
+    if c["dist"] == "batch":
+        # systems of the batch distribution, one after another, up to about n particles
+        sizes = batch_sizes(dict(c, nsys_override=64), seed)
+        sizes = sizes[: max(1, int(np.searchsorted(np.cumsum(sizes), n)))]
+        c["nsys_override"] = len(sizes)
+    else:
+        c["n_override"] = n
+    x, y, z, q, off = make_inputs(c, seed)
+    if off is None:
+        off = np.array([0, len(x)])
     t0 = time.perf_counter()
-    O.ref_treecode(x.copy(), y.copy(), z.copy(), None, x, y, z, q, None, c["kernel"], [c["kp"]], 1, c["approx"],
-                   c["ctype"], c["theta"], c["degree"], c["leaf"], c["leaf"], c["sc"], -1.0, 0)
-    return n, time.perf_counter() - t0
+    for k in range(len(off) - 1):
+        a, b = off[k], off[k + 1]
+        O.ref_treecode(x[a:b].copy(), y[a:b].copy(), z[a:b].copy(), None, x[a:b], y[a:b], z[a:b], q[a:b], None,
+                       c["kernel"], [c["kp"]], 1, c["approx"], c["ctype"], c["theta"], c["degree"], c["leaf"],
+                       c["leaf"], c["sc"], -1.0, 0)
+    return int(off[-1]), time.perf_counter() - t0, len(off) - 1
 
 
 def cpu_baseline(cfg, cores=1):
@@ -142,8 +172,9 @@ def cpu_baseline(cfg, cores=1):
         return None
     n = cfg["sample_n"]
     if cores == 1:
-        done, secs = reference_sample_worker((cfg, 1000, n))
+        done, secs, nsys = reference_sample_worker((cfg, 1000, n))
         value = done / secs
+        n = done
     else:
         import multiprocessing as mp
         ctx = mp.get_context("spawn")
@@ -152,9 +183,12 @@ def cpu_baseline(cfg, cores=1):
             res = pool.map(reference_sample_worker, [(cfg, 1000 + i, n) for i in range(cores)])
         secs = time.perf_counter() - t0
         value = sum(r[0] for r in res) / secs
+        nsys = res[0][2]
+        n = res[0][0]
     return {"value": value, "unit": "targets/s", "cores": cores, "kind": "reference",
-            "sample": f"reference BaryTree CPU build (gcc -O3, serial) on {cores} independent system(s) of "
-                      f"N={n} with this configuration's distribution and parameters; {secs:.1f} s wall"}
+            "sample": f"reference BaryTree CPU build (gcc -O3, serial) on {cores} independent sample(s) of "
+                      f"N={n} particles" + (f" in {nsys} systems" if cfg["dist"] == "batch" else "") +
+                      f" with this configuration's distribution and parameters; {secs:.1f} s wall"}
 
 
 def traffic_from_profiles(config_id):
@@ -169,6 +203,30 @@ def traffic_from_profiles(config_id):
             except ValueError:
                 return None
     return None
+
+
+def roofline(sfu, tflops, fma_peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_rate, traffic):
+    """Roofline of the particle-output kernel (PC + PP onto targets).
+
+    Neither HBM nor the tensor cores bind it: source tiles are reused from
+    shared memory and the work is kernel evaluations.  Mixed Lagrange: the
+    special-function (MUFU) pipe binds (one rsqrt per evaluation, two MUFU ops
+    for Yukawa), peak = the rsqrt rate measured on this GPU by the library's
+    probe.  FP64: the FP64 FMA pipe, peak = the measured DFMA rate."""
+    evals = rep["eval_flops"] / w
+    r = {"kernel": "k_eval_targets(_mixed) (PC + PP)", "ms_per_launch": ev_ms,
+         "evaluations_per_launch": evals, "flops_per_launch": rep["eval_flops"], "traffic": traffic,
+         "simt_tflops": tflops, "simt_peak_tflops": fma_peak,
+         "simt_frac": tflops / fma_peak if tflops else None,
+         "peak_source": "measured by bt_measure_peaks on this GPU (rsqrt probe; FMA = 2 FLOP)"}
+    if sfu:
+        ach = evals * mufu_per_eval / (ev_ms * 1e-3) / 1e9 if ev_ms > 0 else None
+        r.update(bound="sfu (MUFU rsqrt/ex2)", achieved=ach, peak=rsqrt_rate, unit="Gop/s",
+                 frac=ach / rsqrt_rate if ach else None)
+    else:
+        r.update(bound="fp64-simt" if prec == 0 else "fp32-simt", achieved=tflops, peak=fma_peak, unit="TFLOP/s",
+                 frac=tflops / fma_peak if tflops else None)
+    return r
 
 
 def run_reference_arm(args, cfg, rank, world):
@@ -208,8 +266,17 @@ def main():
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--no-fp64-plain", action="store_true", help="skip the FP64 fixed-degree comparison step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="skip the session (graph replay) measurement")
+    ap.add_argument("--dispatch", choices=["auto", "queue", "grid"], default="auto",
+                    help="mixed evaluation kernels: persistent blocks on a device work queue, or one block per item")
+    ap.add_argument("--n", type=int, default=None,
+                    help="particles (default: the configuration's N); smaller systems of the same "
+                         "distribution for profiling captures")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.n:
+        cfg["n_override"] = args.n
+        cfg["workload"] = f"{cfg['workload']} [reduced to N={args.n:,}]"
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -229,8 +296,9 @@ def main():
     B.lib()
 
     dev = torch.device("cuda", local)
-    x, y, z, q = make_inputs(cfg, seed=rank)
+    x, y, z, q, off = make_inputs(cfg, seed=rank)
     n = len(x)
+    batch = off is not None
     prec = B.PRECISION_MIXED if args.precision == "mixed" else B.PRECISION_FP64
     policy = args.degree_policy
     if policy == "auto":
@@ -242,24 +310,28 @@ def main():
                   tolerance=args.tolerance,
                   kernel=cfg["kernel"], kernel_param=cfg["kp"], approximation=cfg["approx"],
                   compute_type=cfg["ctype"], theta=cfg["theta"], degree=cfg["degree"], max_source_leaf=cfg["leaf"],
-                  max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=local)
+                  max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=local,
+                  dispatch={"auto": B.DISPATCH_AUTO, "queue": B.DISPATCH_QUEUE, "grid": B.DISPATCH_GRID}[args.dispatch])
 
     # device-resident inputs (targets are separate arrays with the same coordinates)
     d_in = [torch.from_numpy(a).to(dev) for a in (x, y, z, x.copy(), y.copy(), z.copy(), q)]
     d_out = torch.empty(n, dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)     # > L2 (126 MB)
 
+    def call(ptrs, out_ptr, on_device, **kw):
+        if batch:
+            return B.treecode_batch_ptr(len(off) - 1, off, off, *ptrs, out_ptr, inputs_on_device=on_device, **kw)
+        return B.treecode_ptr(n, n, *ptrs, out_ptr, inputs_on_device=on_device, **kw)
+
     def step_device():
-        return B.treecode_ptr(n, n, *(t.data_ptr() for t in d_in[3:6]), *(t.data_ptr() for t in d_in[:3]),
-                              d_in[6].data_ptr(), d_out.data_ptr(), inputs_on_device=True, **common)
+        return call([t.data_ptr() for t in d_in[3:6] + d_in[:3] + d_in[6:]], d_out.data_ptr(), True, **common)
 
     # pinned host buffers for the end-to-end path
     h_in = [torch.from_numpy(a.copy()).pin_memory() for a in (x, y, z, x, y, z, q)]
     h_out = torch.empty(n, dtype=torch.float64).pin_memory()
 
     def step_host():
-        return B.treecode_ptr(n, n, *(t.data_ptr() for t in h_in[3:6]), *(t.data_ptr() for t in h_in[:3]),
-                              h_in[6].data_ptr(), h_out.data_ptr(), inputs_on_device=False, **common)
+        return call([t.data_ptr() for t in h_in[3:6] + h_in[:3] + h_in[6:]], h_out.data_ptr(), False, **common)
 
     def timed(step, k):
         """K steps, each bracketed by CUDA events on the current stream; L2 flushed between steps."""
@@ -296,35 +368,72 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_dev, ms_e2e = float(t[0]), float(t[1])
 
-    # accuracy of the last step vs the FP64 direct sum on 10,000 strided targets (outside timing)
-    idx = np.arange(0, n, max(1, n // 10000))
-    d = B.direct(x[idx], y[idx], z[idx], x, y, z, q, cfg["kernel"], cfg["kp"], device=local)
-    pot = d_out.cpu().numpy()[idx]
-    rel_l2 = float(np.linalg.norm(pot - d) / np.linalg.norm(d))
-    rel_max = float(np.max(np.abs(pot - d)) / np.max(np.abs(d)))
+    # accuracy of the last step vs the FP64 direct sum (outside timing): 10,000
+    # strided targets; for a batch, per system (every target up to 20,000
+    # particles, else 10,000 strided) and the worst system reported
+    def accuracy(pot_all):
+        if not batch:
+            idx = np.arange(0, n, max(1, n // 10000))
+            d = B.direct(x[idx], y[idx], z[idx], x, y, z, q, cfg["kernel"], cfg["kp"], device=local)
+            e = pot_all[idx] - d
+            return (float(np.linalg.norm(e) / np.linalg.norm(d)), float(np.max(np.abs(e)) / np.max(np.abs(d))),
+                    len(idx))
+        l2, mx, cnt = [], [], 0
+        for k in range(len(off) - 1):
+            a, b = int(off[k]), int(off[k + 1])
+            m = b - a
+            idx = a + (np.arange(m) if m <= 20000 else np.arange(0, m, m // 10000))
+            d = B.direct(x[idx], y[idx], z[idx], x[a:b], y[a:b], z[a:b], q[a:b], cfg["kernel"], cfg["kp"],
+                         device=local)
+            e = pot_all[idx] - d
+            l2.append(float(np.linalg.norm(e) / np.linalg.norm(d)))
+            mx.append(float(np.max(np.abs(e)) / np.max(np.abs(d))))
+            cnt += len(idx)
+        return max(l2), max(mx), cnt
+
+    rel_l2, rel_max, n_checked = accuracy(d_out.cpu().numpy())
 
     # the plain FP64 treecode at the configuration's fixed degree on the same
     # system and inputs (the denominator of the mixed + learned speed-up)
     fp64_plain = None
     if not args.no_fp64_plain and (prec != B.PRECISION_FP64 or policy != "fixed"):
         plain = dict(common)
-        plain.update(precision=B.PRECISION_FP64, degree_policy=B.DEGREE_FIXED)
+        plain.update(precision=B.PRECISION_FP64, degree_policy=B.DEGREE_FIXED, dispatch=B.DISPATCH_AUTO)
 
         def step_plain():
-            return B.treecode_ptr(n, n, *(t.data_ptr() for t in d_in[3:6]), *(t.data_ptr() for t in d_in[:3]),
-                                  d_in[6].data_ptr(), d_out.data_ptr(), inputs_on_device=True, **plain)
+            return call([t.data_ptr() for t in d_in[3:6] + d_in[:3] + d_in[6:]], d_out.data_ptr(), True, **plain)
         step_plain()
         ms_plain, preps = timed(step_plain, 1)
         t = torch.tensor([ms_plain], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_plain = float(t[0])
-        pp = d_out.cpu().numpy()[idx]
         fp64_plain = {"value": world * n / (ms_plain * 1e-3), "unit": "targets/s", "ms_per_step": ms_plain,
                       "steps": 1, "degree": cfg["degree"],
-                      "rel_l2_vs_fp64_direct": float(np.linalg.norm(pp - d) / np.linalg.norm(d)),
+                      "rel_l2_vs_fp64_direct": accuracy(d_out.cpu().numpy())[0],
                       "ms_eval_kernel": preps[-1]["ms_eval_kernel"],
                       "interactions": preps[-1]["pp_ptwise"] + preps[-1]["pc_ptwise"]}
+
+    # the same evaluation through a session: trees, lists and degree selection
+    # built once, then per evaluation the charges go host->device, one CUDA
+    # graph replays the whole device sequence, potentials come back
+    graph = None
+    if not args.no_graph:
+        bounds = off if batch else np.array([0, n])
+        systems = [(x[a:b], y[a:b], z[a:b], x[a:b], y[a:b], z[a:b], q[a:b]) for a, b in zip(bounds[:-1], bounds[1:])]
+        sess = B.Session(systems, **common)
+        sess.evaluate(q)
+        ms_graph, greps = timed(lambda: sess.evaluate(q, return_report=True)[1], args.steps)
+        sess.close()
+        t = torch.tensor([ms_graph], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_graph = float(t[0]) / args.steps
+        graph = {"value": world * n / (ms_graph * 1e-3), "unit": "targets/s", "ms_per_step": ms_graph,
+                 "kernels_per_graph": greps[-1]["kernel_launches"], "ms_eval_kernel": greps[-1]["ms_eval_kernel"],
+                 "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                 "what": "bt_session_eval with host charges and potentials: one CUDA graph replay of the whole "
+                         "device sequence; trees, lists and degree selection made once by bt_session_create"}
 
     if rank == 0:
         fp64_peak, fp32_peak, rsqrt_rate = B.measure_peaks(local)
@@ -332,6 +441,11 @@ def main():
         ev_ms = statistics.mean(r["ms_eval_kernel"] for r in reps)
         achieved = rep["eval_flops"] / (ev_ms * 1e-3) / 1e12 if ev_ms > 0 else None
         peak = fp64_peak if prec == B.PRECISION_FP64 else fp32_peak
+        # the binding pipe of the mixed Lagrange kernels is the special-function
+        # unit: one rsqrt per evaluation (Yukawa: rsqrt + ex2)
+        w = {1: 10.0, 2: 13.0, 3: 11.0}[cfg["kernel"]]
+        mufu_per_eval = 2 if cfg["kernel"] == 2 else 1
+        sfu = prec == B.PRECISION_MIXED and cfg["approx"] == 1
         value = world * n / (ms_dev / args.steps * 1e-3)
         e2e = world * n / (ms_e2e / args.steps * 1e-3)
         line = {
@@ -340,25 +454,25 @@ def main():
             "vs_baseline": None, "dtype": "f64" if prec == B.PRECISION_FP64 else "f32+f64",
             "data": "synthetic (seeded numpy PCG64 with the configuration's distribution)",
             "config": {"workload": cfg["workload"], "config_id": args.config, "precision": args.precision,
-                       "degree_policy": policy, "tolerance": args.tolerance,
+                       "degree_policy": policy, "tolerance": args.tolerance, "dispatch": args.dispatch,
                        "l2": "flushed between steps (256 MB write)",
-                       "parallelism": f"{world} independent system(s), one per GPU",
+                       "parallelism": f"{world} independent " + ("batch(es)" if batch else "system(s)") + ", one per GPU",
+                       "systems": len(off) - 1 if batch else 1,
                        "rel_l2_vs_fp64_direct": rel_l2, "rel_max_vs_fp64_direct": rel_max,
-                       "direct_sample_targets": len(idx)},
-            "e2e": {"value": e2e, "unit": "targets/s", "h2d_bytes_per_step": 7 * 8 * n,
+                       "direct_sample_targets": n_checked},
+            # the target arrays hold the sources' coordinates, which the library
+            # detects and copies once: x, y, z, q go host->device, potentials back
+            "e2e": {"value": e2e, "unit": "targets/s", "h2d_bytes_per_step": 4 * 8 * n,
                     "d2h_bytes_per_step": 8 * n, "ms_per_step": ms_e2e / args.steps},
-            "roofline": {"bound": "fp64-simt" if prec == B.PRECISION_FP64 else "fp32-simt",
-                         "kernel": "k_eval_targets (PC + PP)", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak if achieved else None,
-                         "peak_source": "measured by bt_measure_peaks on this GPU (FMA=2 FLOP)",
-                         "traffic": traffic_from_profiles(args.config),
-                         "flops_per_launch": rep["eval_flops"], "ms_per_launch": ev_ms,
-                         "rsqrt_gops_measured": rsqrt_rate},
+            "roofline": roofline(sfu, achieved, peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_rate,
+                                 traffic_from_profiles(args.config)),
             "phases_ms": {k: rep[k] for k in ("ms_setup", "ms_upward", "ms_compute", "ms_downward", "ms_transfer")},
             "interactions": {k: rep[k] for k in ("pp_ptwise", "pc_ptwise", "cp_ptwise", "cc_ptwise")},
             "clocks": clock_info,
             "gpu_launches": launches,
         }
+        if graph is not None:
+            line["graph_replay"] = graph
         if fp64_plain is not None:
             line["fp64_plain"] = fp64_plain
             line["speedup_vs_fp64_plain"] = {"value": value / fp64_plain["value"],

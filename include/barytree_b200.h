@@ -94,9 +94,14 @@ typedef struct bt_options {
                              pointers (FP64) and output is a device pointer          */
     int tree_build;       /* BT_TREE_GPU (default) or BT_TREE_HOST: where the trees
                              are built; both give the same trees and particle order  */
+    int dispatch;         /* mixed evaluation kernels: BT_DISPATCH_AUTO (default),
+                             BT_DISPATCH_QUEUE (persistent blocks taking cost-sorted
+                             work items from a device counter) or BT_DISPATCH_GRID
+                             (one block per work item); results are identical     */
 } bt_options;
 
 enum { BT_TREE_GPU = 0, BT_TREE_HOST = 1 };
+enum { BT_DISPATCH_AUTO = 0, BT_DISPATCH_QUEUE = 1, BT_DISPATCH_GRID = 2 };
 
 /* Per-call report (all optional: pass NULL). */
 typedef struct bt_report {
@@ -121,6 +126,48 @@ int bt_eval(int numTargets, int numSources,
             int kernel, double kernelParam, int approximation, int compute_type,
             double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
             double sizeCheck, const bt_options *opts, bt_report *report);
+
+/* Batched evaluation of independent systems (no counterpart in the
+ * reference, which evaluates one system per call).  System k's targets are
+ * entries [targetOffsets[k], targetOffsets[k+1]) of the target arrays and of
+ * outputArray, its sources entries [sourceOffsets[k], sourceOffsets[k+1]) of
+ * the source arrays (offsets: numSystems+1 host entries, starting at 0).
+ * Every system gets its own trees and interaction lists, exactly as a
+ * separate bt_eval call would build them, and the same potentials bit for
+ * bit; all systems share one upward pass, one evaluation kernel and one
+ * downward pass, so many small systems fill the GPU together. */
+int bt_eval_batch(int numSystems, const long long *targetOffsets, const long long *sourceOffsets,
+                  const double *targetX, const double *targetY, const double *targetZ,
+                  const double *sourceX, const double *sourceY, const double *sourceZ,
+                  const double *sourceValue, double *outputArray,
+                  int kernel, double kernelParam, int approximation, int compute_type,
+                  double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+                  double sizeCheck, const bt_options *opts, bt_report *report);
+
+/* Sessions (no counterpart in the reference): fixed geometry, new charges.
+ * For a solver that evaluates the same particles many times with changing
+ * charges (an iterative method whose matrix-vector product is the
+ * treecode), bt_session_create builds the trees and interaction lists,
+ * makes the degree selection (BT_DEGREE_LEARNED: with the charges given
+ * here), uploads everything and captures the whole device sequence (charges
+ * into tree order, upward pass, evaluation kernels, downward pass, reorder)
+ * as one CUDA graph; bt_session_eval copies in the new charges, replays the
+ * graph and copies out the potentials.  Arguments as bt_eval_batch (one
+ * system: offsets {0, numTargets} and {0, numSources}); with
+ * opts->inputs_on_device the charges and outputs of bt_session_eval are
+ * device pointers too.  A session owns its device memory until
+ * bt_session_destroy. */
+typedef struct bt_session bt_session;
+int bt_session_create(int numSystems, const long long *targetOffsets, const long long *sourceOffsets,
+                      const double *targetX, const double *targetY, const double *targetZ,
+                      const double *sourceX, const double *sourceY, const double *sourceZ,
+                      const double *sourceValue, int kernel, double kernelParam,
+                      int approximation, int compute_type, double theta, int interpOrder,
+                      int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck,
+                      const bt_options *opts, bt_session **session);
+int bt_session_eval(bt_session *session, const double *sourceValue, double *outputArray,
+                    bt_report *report);
+int bt_session_destroy(bt_session *session);
 
 /* Allocation-free evaluation (no counterpart in the reference).
  *
