@@ -100,6 +100,8 @@ int get_ctx(int device, DeviceCtx **out)
     std::lock_guard<std::mutex> lk(g_ctx_mu);
     DeviceCtx &c = g_ctx[device];
     if (cudaSetDevice(device) != cudaSuccess) { set_err("cudaSetDevice failed"); return BT_ERR_CUDA; }
+    // an error left by the caller's earlier work is not this call's
+    cudaGetLastError();
     if (c.device < 0) {
         if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
             set_err("stream creation failed");
@@ -396,14 +398,17 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
     bt::GtArrays sa{d_sx, d_sy, d_sz, d_sq, d_sord};
     int e = bt::gpu_build_forest(sys.n, sys.soff.data(), sx, sy, sz, sq, o.maxs, sa, d_work, wbytes, &pl.st, st,
                                  &launches);
+    const char *which = "source";
     if (!e && !same) {
         bt::GtArrays ta{d_tx, d_ty, d_tz, nullptr, d_tord};
+        which = "target";
         e = bt::gpu_build_forest(sys.n, sys.toff.data(), tx, ty, tz, nullptr, o.maxt, ta, d_work, wbytes, &pl.tt, st,
                                  &launches);
     }
     g_launches += launches;
     if (e) {
-        set_err("CUDA error %s in the tree build", cudaGetErrorString((cudaError_t)e));
+        set_err("CUDA error %s in the %s tree build (bt_gputree.cu:%d)", cudaGetErrorString((cudaError_t)e), which,
+                bt::gpu_tree_fail_line());
         return BT_ERR_CUDA;
     }
     pl.src.n = ns;
@@ -439,6 +444,10 @@ struct DevPlan {
     double *d_xgrid[BT_MAX_DEGREE + 1] = {}, *d_xQ[BT_MAX_DEGREE + 1] = {};
     float *d_xQ32[BT_MAX_DEGREE + 1] = {};
     double *d_out = nullptr;    // potentials in caller order (run_plan's own buffer)
+    bt::HermChunk *d_hchunks = nullptr;     // Hermite P2M: particle chunks of every node
+    int3 *d_hred = nullptr;                 // nodes with several chunks
+    double *d_hpartial = nullptr;           // their partial moments
+    int n_hchunks = 0, n_hred = 0;
 };
 
 // The device sequence of one evaluation (stream-ordered, no host
@@ -446,8 +455,14 @@ struct DevPlan {
 // positions, upward pass, grid-output and particle-output kernels, downward
 // pass, and the scatter of the potentials into caller order at scatter_out.
 // ev: 5 events bracketing the phases, or nullptr.
-int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatter_out, long long &launches)
+int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatter_out, long long &launches,
+               bool capturing = false)
 {
+    // inside a stream capture an event becomes a record node of the graph
+    // only when recorded as external
+    auto record = [&](int k) {
+        return capturing ? cudaEventRecordWithFlags(ev[k], st, cudaEventRecordExternal) : cudaEventRecord(ev[k], st);
+    };
     int rc = BT_OK;
     const bool mixed = v.mixed, herm = v.herm, need_src_clusters = v.need_src_clusters, need_tgt_grids = v.need_tgt_grids;
     const int n = v.n, P = v.P, ns = v.ns, nt = v.nt, max_np1 = v.max_np1;
@@ -514,12 +529,18 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         bt::launch_rel_positions(v.T_nleaves, d_tleaves, d_tibeg, d_tnum, d_tctr, d_tx, d_ty, d_tz, nullptr, d_tpos, st);
         launches += 2;
     }
-    if (ev) CK(cudaEventRecord(ev[0], st));
+    if (ev) CK(record(0));
     // upward pass
     if (need_src_clusters && ns > 0) {
-        bt::launch_p2m(n, herm, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
-                       d_sz, d_sq, d_Q, st);
-        launches++;
+        if (herm) {
+            bt::launch_p2m_hermite(n, v.n_hchunks, v.d_hchunks, v.n_hred, v.d_hred, d_sgrid, d_slen, d_ww, d_sx, d_sy,
+                                   d_sz, d_sq, d_Q, v.d_hpartial, st);
+            launches += v.n_hred > 0 ? 2 : 1;
+        } else {
+            bt::launch_p2m(n, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
+                           d_sz, d_sq, d_Q, st);
+            launches++;
+        }
         if (!herm) {
             for (int l = v.S_max_depth - 1; l >= 0; l--) {
                 int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
@@ -551,7 +572,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         }
     }
     CK(cudaGetLastError());
-    if (ev) CK(cudaEventRecord(ev[1], st));
+    if (ev) CK(record(1));
     // grid-output evaluation (CP, M2L) and L2L
     if (mixed && v.queue) CK(cudaMemsetAsync(d_queue, 0, 2 * sizeof(int), st));
     if (need_tgt_grids && nt > 0 && mixed) {
@@ -573,7 +594,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         launches++;
     }
     CK(cudaGetLastError());
-    if (ev) CK(cudaEventRecord(ev[2], st));
+    if (ev) CK(record(2));
     // particle-output evaluation (PC, PP)
     if (nt > 0 && mixed) {
         bt::MixedTargetsArgs a;
@@ -602,7 +623,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         launches++;
     }
     CK(cudaGetLastError());
-    if (ev) CK(cudaEventRecord(ev[3], st));
+    if (ev) CK(record(3));
     // downward pass
     if (need_tgt_grids && nt > 0) {
         if (!herm) {
@@ -619,7 +640,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         launches++;
     }
     CK(cudaGetLastError());
-    if (ev) CK(cudaEventRecord(ev[4], st));
+    if (ev) CK(record(4));
     bt::launch_scatter(nt, d_order, d_pot, scatter_out, st);
     launches++;
     CK(cudaGetLastError());
@@ -731,6 +752,15 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         }
     }
 
+    // Hermite upward pass: particle chunks of every source node
+    std::vector<bt::HermChunk> hchunks;
+    std::vector<int3> hred;
+    int hslots = 0;
+    if (herm && need_src_clusters) hslots = bt::hermite_chunks(S.n, S.ibeg, S.numpar, hchunks, hred);
+    bt::HermChunk *d_hchunks = nullptr;
+    int3 *d_hred = nullptr;
+    double *d_hpartial = nullptr;
+
     // device layout
     double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx, *d_ty, *d_tz, *d_pot, *d_sgrid, *d_tgrid, *d_slen, *d_tlen, *d_ww;
     double *d_Q = nullptr, *d_Phi = nullptr;
@@ -766,6 +796,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     L.add(&d_out, nt);
     int *d_queue;           // work-queue counters of the two evaluation kernels
     L.add(&d_queue, 2);
+    if (herm && need_src_clusters) {
+        L.add(&d_hchunks, hchunks.size());
+        L.add(&d_hred, hred.size());
+        L.add(&d_hpartial, (size_t)hslots * 8 * P);
+    }
     float4 *d_spos = nullptr, *d_tpos = nullptr;
     float *d_Q32 = nullptr;
     double *d_sctr = nullptr, *d_tctr = nullptr;
@@ -824,6 +859,10 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         UP(d_ccoff, pl.g_cc.off, pl.g_cc.rows + 1); UP(d_ccidx, pl.g_cc.idx, pl.g_cc.off[pl.g_cc.rows]);
         UP(d_cpoff, pl.g_cp.off, pl.g_cp.rows + 1); UP(d_cpidx, pl.g_cp.idx, pl.g_cp.off[pl.g_cp.rows]);
         UP(d_evitems, ev_items.data(), ev_items.size());
+        if (herm && need_src_clusters) {
+            UP(d_hchunks, hchunks.data(), hchunks.size());
+            UP(d_hred, hred.data(), hred.size());
+        }
         UP(d_griditems, grid_items.data(), grid_items.size());
         UP(d_l2pitems, l2p_items.data(), l2p_items.size());
         if (mixed) {
@@ -849,6 +888,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         else v.T_lvl_off.assign(T.max_depth + 1, 0);
         v.xdeg = xdeg;
         v.n_grid_items = (int)grid_items.size(); v.n_ev_items = (int)ev_items.size(); v.n_l2p_items = (int)l2p_items.size();
+        v.d_hchunks = d_hchunks; v.d_hred = d_hred; v.d_hpartial = d_hpartial;
+        v.n_hchunks = (int)hchunks.size(); v.n_hred = (int)hred.size();
         v.d_sx = d_sx;
         v.d_sy = d_sy;
         v.d_sz = d_sz;
@@ -924,6 +965,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             cudaEventElapsedTime(&b, ev[1], ev[2]);
             cudaEventElapsedTime(&c, ev[2], ev[3]);
             cudaEventElapsedTime(&d, ev[3], ev[4]);
+            cudaGetLastError();
             rep->ms_upward = a;
             rep->ms_compute = b + c;
             rep->ms_downward = d;
@@ -1890,7 +1932,7 @@ int bt_session_create(int numSystems, const long long *targetOffsets, const long
         if (e == cudaSuccess) {
             bt::launch_gather(ns, sorder, S->d_qin, (double *)S->v.d_sq, st);
             long long launches = 1;
-            int rc2 = issue_plan(S->v, st, S->ev, S->v.d_out, launches);
+            int rc2 = issue_plan(S->v, st, S->ev, S->v.d_out, launches, true);
             e = cudaStreamEndCapture(st, &S->graph);
             if (rc2 != BT_OK) rc = rc2;
             S->graph_kernels = launches;
@@ -1941,6 +1983,7 @@ int bt_session_eval(bt_session *session, const double *sourceValue, double *outp
         cudaEventElapsedTime(&b, S->ev[1], S->ev[2]);
         cudaEventElapsedTime(&c, S->ev[2], S->ev[3]);
         cudaEventElapsedTime(&d, S->ev[3], S->ev[4]);
+        cudaGetLastError();
         report->ms_upward = a;
         report->ms_compute = b + c;
         report->ms_downward = d;

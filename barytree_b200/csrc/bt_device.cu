@@ -9,6 +9,9 @@
 //   potentials on target grids: same layout as charges.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <vector>
+
 #include <cfloat>
 #include <cstdint>
 
@@ -322,6 +325,201 @@ k_p2m_hermite(int n, const int *__restrict__ ibeg, const int *__restrict__ numpa
         if (j < P)
 #pragma unroll
             for (int m = 0; m < 8; m++) Q[((size_t)node * 8 + m) * P + j] = acc[jj][m];
+    }
+}
+
+// Hermite P2M over particle chunks: every node's particles are split into
+// chunks of HC_PARTICLES, one block per chunk, so the root's N particles
+// spread over N / HC_PARTICLES blocks instead of one.  A chunk of a node with
+// a single chunk writes Q directly; the chunks of a larger node write partial
+// moments that k_hermite_reduce sums in chunk order (deterministic).
+// Separable form for degree <= 7: each thread owns one (k2,k3) column with
+// all 8 moments x (n+1) k1 entries in registers; per particle it forms the
+// four y-z products (value/derivative on each axis) times q, then 8 FMAs per
+// k1 against x values every thread reads from the same shared address.
+constexpr int HC_PARTICLES = 2048;
+constexpr int HC_SUB = 32;
+
+template <int NP1>
+__global__ void __launch_bounds__(64)
+k_p2m_hermite_sep(const HermChunk *__restrict__ chunks, const double *__restrict__ grid,
+                  const double *__restrict__ box_len, const double *__restrict__ ww, const double *__restrict__ sx,
+                  const double *__restrict__ sy, const double *__restrict__ sz, const double *__restrict__ sq,
+                  double *__restrict__ Q, double *__restrict__ partial)
+{
+    constexpr int n = NP1 - 1, COLS = NP1 * NP1, P = COLS * NP1;
+    const HermChunk ch = chunks[blockIdx.x];
+    const int node = ch.node;
+    __shared__ double nodes[3 * NP1], wws[NP1], len[3];
+    __shared__ double A[3][HC_SUB][NP1], Bd[3][HC_SUB][NP1], qs[HC_SUB];
+    for (int i = threadIdx.x; i < 3 * NP1; i += blockDim.x) nodes[i] = grid[(size_t)node * 3 * NP1 + i];
+    for (int i = threadIdx.x; i < NP1; i += blockDim.x) wws[i] = ww[i];
+    if (threadIdx.x < 3) len[threadIdx.x] = box_len[node * 3 + threadIdx.x];
+    const int col = threadIdx.x;
+    const bool on = col < COLS;
+    const int k2 = on ? col % NP1 : 0, k3 = on ? col / NP1 : 0;
+    double acc[8][NP1];
+#pragma unroll
+    for (int m = 0; m < 8; m++)
+#pragma unroll
+        for (int k = 0; k < NP1; k++) acc[m][k] = 0.0;
+    __syncthreads();
+    for (int c0 = 0; c0 < ch.count; c0 += HC_SUB) {
+        const int cm = min(HC_SUB, ch.count - c0);
+        for (int w = threadIdx.x; w < cm * 3; w += blockDim.x) {
+            const int i = w / 3, ax = w % 3;
+            const double *src = ax == 0 ? sx : ax == 1 ? sy : sz;
+            double a[MAXNP], bb[MAXNP];
+            hermite_basis(n, nodes + ax * NP1, src[ch.begin + c0 + i], wws, len[ax], a, bb);
+#pragma unroll
+            for (int k = 0; k < NP1; k++) { A[ax][i][k] = a[k]; Bd[ax][i][k] = bb[k]; }
+            if (ax == 0) qs[i] = sq[ch.begin + c0 + i];
+        }
+        __syncthreads();
+        for (int i = 0; i < cm; i++) {
+            const double q = qs[i];
+            const double az = A[2][i][k3] * q, bz = Bd[2][i][k3] * q;
+            const double ay = A[1][i][k2], by = Bd[1][i][k2];
+            const double yAA = ay * az, yBA = by * az, yAB = ay * bz, yBB = by * bz;
+#pragma unroll
+            for (int k = 0; k < NP1; k++) {
+                const double ax = A[0][i][k], bx = Bd[0][i][k];
+                acc[0][k] = fma(ax, yAA, acc[0][k]);
+                acc[1][k] = fma(bx, yAA, acc[1][k]);
+                acc[2][k] = fma(ax, yBA, acc[2][k]);
+                acc[3][k] = fma(ax, yAB, acc[3][k]);
+                acc[4][k] = fma(bx, yBA, acc[4][k]);
+                acc[5][k] = fma(ax, yBB, acc[5][k]);
+                acc[6][k] = fma(bx, yAB, acc[6][k]);
+                acc[7][k] = fma(bx, yBB, acc[7][k]);
+            }
+        }
+        __syncthreads();
+    }
+    if (!on) return;
+    double *dst = ch.slot < 0 ? Q + (size_t)node * 8 * P : partial + (size_t)ch.slot * 8 * P;
+#pragma unroll
+    for (int m = 0; m < 8; m++)
+#pragma unroll
+        for (int k = 0; k < NP1; k++) dst[(size_t)m * P + k + NP1 * col] = acc[m][k];
+}
+
+// Degrees above 7: one thread per grid point with 8 accumulators, over the
+// same chunks.
+__global__ void __launch_bounds__(HP2M_THREADS)
+k_p2m_hermite_chunks(int n, const HermChunk *__restrict__ chunks, const double *__restrict__ grid,
+                     const double *__restrict__ box_len, const double *__restrict__ ww,
+                     const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
+                     const double *__restrict__ sq, double *__restrict__ Q, double *__restrict__ partial)
+{
+    const HermChunk ch = chunks[blockIdx.x];
+    const int node = ch.node;
+    const int np1 = n + 1, P = np1 * np1 * np1;
+    __shared__ double nodes[3 * MAXNP], wws[MAXNP], len[3];
+    __shared__ double Ab[HP2M_CHUNK][3][MAXNP], Bb[HP2M_CHUNK][3][MAXNP];
+    __shared__ double qs[HP2M_CHUNK];
+    for (int i = threadIdx.x; i < 3 * np1; i += blockDim.x) nodes[i] = grid[(size_t)node * 3 * np1 + i];
+    for (int i = threadIdx.x; i < np1; i += blockDim.x) wws[i] = ww[i];
+    if (threadIdx.x < 3) len[threadIdx.x] = box_len[node * 3 + threadIdx.x];
+    double acc[HP2M_MAXJ][8];
+#pragma unroll
+    for (int jj = 0; jj < HP2M_MAXJ; jj++)
+#pragma unroll
+        for (int m = 0; m < 8; m++) acc[jj][m] = 0.0;
+    __syncthreads();
+    for (int c0 = 0; c0 < ch.count; c0 += HP2M_CHUNK) {
+        int cm = min(HP2M_CHUNK, ch.count - c0);
+        for (int w = threadIdx.x; w < cm * 3; w += blockDim.x) {
+            int i = w / 3, a = w % 3;
+            const double *src = a == 0 ? sx : a == 1 ? sy : sz;
+            double A[MAXNP], B[MAXNP];
+            hermite_basis(n, nodes + a * np1, src[ch.begin + c0 + i], wws, len[a], A, B);
+            for (int k = 0; k <= n; k++) { Ab[i][a][k] = A[k]; Bb[i][a][k] = B[k]; }
+            if (a == 0) qs[i] = sq[ch.begin + c0 + i];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int jj = 0; jj < HP2M_MAXJ; jj++) {
+            int j = threadIdx.x + jj * HP2M_THREADS;
+            if (j < P) {
+                int k1 = j % np1, k2 = (j / np1) % np1, k3 = j / (np1 * np1);
+                for (int i = 0; i < cm; i++) {
+                    double ax = Ab[i][0][k1], bx = Bb[i][0][k1];
+                    double ay = Ab[i][1][k2], by = Bb[i][1][k2];
+                    double az = Ab[i][2][k3] * qs[i], bz = Bb[i][2][k3] * qs[i];
+                    double axay = ax * ay, bxay = bx * ay, axby = ax * by, bxby = bx * by;
+                    acc[jj][0] += axay * az;
+                    acc[jj][1] += bxay * az;
+                    acc[jj][2] += axby * az;
+                    acc[jj][3] += axay * bz;
+                    acc[jj][4] += bxby * az;
+                    acc[jj][5] += axby * bz;
+                    acc[jj][6] += bxay * bz;
+                    acc[jj][7] += bxby * bz;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    double *dst = ch.slot < 0 ? Q + (size_t)node * 8 * P : partial + (size_t)ch.slot * 8 * P;
+#pragma unroll
+    for (int jj = 0; jj < HP2M_MAXJ; jj++) {
+        int j = threadIdx.x + jj * HP2M_THREADS;
+        if (j < P)
+#pragma unroll
+            for (int m = 0; m < 8; m++) dst[(size_t)m * P + j] = acc[jj][m];
+    }
+}
+
+// Q of a node with several chunks = the sum of its chunks' partial moments,
+// in chunk order.  red[r] = (node, first slot, number of slots).
+__global__ void k_hermite_reduce(int width, const int3 *__restrict__ red, const double *__restrict__ partial,
+                                 double *__restrict__ Q)
+{
+    const int3 r = red[blockIdx.y];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < width; j += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < r.z; c++) s += partial[(size_t)(r.y + c) * width + j];
+        Q[(size_t)r.x * width + j] = s;
+    }
+}
+
+int hermite_chunks(int nnodes, const int *ibeg, const int *numpar, std::vector<HermChunk> &chunks,
+                   std::vector<int3> &red)
+{
+    chunks.clear();
+    red.clear();
+    int slots = 0;
+    for (int v = 0; v < nnodes; v++) {
+        const int np = numpar[v], nc = (np + HC_PARTICLES - 1) / HC_PARTICLES;
+        if (nc <= 1) {
+            chunks.push_back(HermChunk{v, ibeg[v], np, -1});
+            continue;
+        }
+        red.push_back(make_int3(v, slots, nc));
+        for (int c = 0; c < nc; c++)
+            chunks.push_back(HermChunk{v, ibeg[v] + c * HC_PARTICLES, std::min(HC_PARTICLES, np - c * HC_PARTICLES),
+                                       slots++});
+    }
+    return slots;
+}
+
+void launch_p2m_hermite(int n, int nchunks, const HermChunk *chunks, int nred, const int3 *red, const double *grid,
+                        const double *box_len, const double *ww, const double *sx, const double *sy, const double *sz,
+                        const double *sq, double *Q, double *partial, cudaStream_t st)
+{
+    if (nchunks <= 0) return;
+    switch (n + 1) {
+#define BT_HC(N) case N: k_p2m_hermite_sep<N><<<nchunks, 64, 0, st>>>(chunks, grid, box_len, ww, sx, sy, sz, sq, Q, partial); break;
+        BT_HC(2) BT_HC(3) BT_HC(4) BT_HC(5) BT_HC(6) BT_HC(7) BT_HC(8)
+#undef BT_HC
+    default:
+        k_p2m_hermite_chunks<<<nchunks, HP2M_THREADS, 0, st>>>(n, chunks, grid, box_len, ww, sx, sy, sz, sq, Q, partial);
+    }
+    if (nred > 0) {
+        const int width = 8 * (n + 1) * (n + 1) * (n + 1);
+        dim3 g((width + 255) / 256, nred);
+        k_hermite_reduce<<<g, 256, 0, st>>>(width, red, partial, Q);
     }
 }
 

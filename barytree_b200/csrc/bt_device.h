@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <vector>
 #include <cstdint>
 
 namespace bt {
@@ -37,6 +39,18 @@ struct EvalGridsArgs {
 void launch_p2m(int n, bool hermite, int nleaves, const int *leaves, int nnodes, const int *ibeg, const int *numpar,
                 const double *grid, const double *box_len, const double *ww, const double *sx, const double *sy,
                 const double *sz, const double *sq, double *Q, cudaStream_t st);
+// Hermite P2M over particle chunks (see bt_device.cu).  slot < 0: the chunk
+// is its node's only one and writes Q directly.
+struct HermChunk {
+    int node, begin, count, slot;
+};
+// Chunks of every node and, for nodes with several chunks, (node, first slot,
+// slot count); returns the number of partial slots (8 (n+1)^3 doubles each).
+int hermite_chunks(int nnodes, const int *ibeg, const int *numpar, std::vector<HermChunk> &chunks,
+                   std::vector<int3> &red);
+void launch_p2m_hermite(int n, int nchunks, const HermChunk *chunks, int nred, const int3 *red, const double *grid,
+                        const double *box_len, const double *ww, const double *sx, const double *sy, const double *sz,
+                        const double *sq, double *Q, double *partial, cudaStream_t st);
 void launch_m2m(int n, int nparents, const int *parents, const int *nchild, const int *child, const double *grid,
                 double *Q, cudaStream_t st);
 void launch_l2l(int n, int nparents, const int *parents, const int *nchild, const int *child, const double *grid,

@@ -227,10 +227,15 @@ int preorder(const std::vector<HNode> &nodes, int i, int next, std::vector<int> 
     return next;
 }
 
+int g_fail_line = 0;
+
 #define GT_CK(call)                                    \
     do {                                               \
         cudaError_t e_ = (call);                       \
-        if (e_ != cudaSuccess) return (int)e_;         \
+        if (e_ != cudaSuccess) {                       \
+            g_fail_line = __LINE__;                    \
+            return (int)e_;                            \
+        }                                              \
     } while (0)
 
 // Nodes of one level: at most 8 per split node of the level above, and a
@@ -242,6 +247,8 @@ size_t level_nodes_max(int n, int maxpar, int nsys)
 }
 
 }  // namespace
+
+int gpu_tree_fail_line() { return g_fail_line; }
 
 size_t gpu_tree_work_bytes(int n, int maxpar, bool with_q, int nsys)
 {

@@ -38,4 +38,7 @@ int gpu_build_forest(int nsys, const int64_t *sys_off, const double *x, const do
 int gpu_arrays_equal(const double *a, const double *b, size_t n, unsigned long long *flag, bool *equal,
                      cudaStream_t st);
 
+// Source line (bt_gputree.cu) of the last failing CUDA call of a build.
+int gpu_tree_fail_line();
+
 }  // namespace bt

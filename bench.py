@@ -191,9 +191,14 @@ def cpu_baseline(cfg, cores=1):
                       f" with this configuration's distribution and parameters; {secs:.1f} s wall"}
 
 
+PROFILE_FOR_CONFIG = {5: "eval_targets_mixed_blobs2M.md"}
+
+
 def traffic_from_profiles(config_id):
     """DRAM bytes per launch of the evaluation kernel, from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", f"eval_targets_config{config_id}.md")
+    if config_id not in PROFILE_FOR_CONFIG:
+        return None
+    path = os.path.join(ROOT, "profiles", PROFILE_FOR_CONFIG[config_id])
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -440,7 +445,9 @@ def main():
         rep = reps[-1]
         ev_ms = statistics.mean(r["ms_eval_kernel"] for r in reps)
         achieved = rep["eval_flops"] / (ev_ms * 1e-3) / 1e12 if ev_ms > 0 else None
-        peak = fp64_peak if prec == B.PRECISION_FP64 else fp32_peak
+        # Hermite evaluates in FP64 in either precision mode
+        fp64_kernels = prec == B.PRECISION_FP64 or cfg["approx"] == 2
+        peak = fp64_peak if fp64_kernels else fp32_peak
         # the binding pipe of the mixed Lagrange kernels is the special-function
         # unit: one rsqrt per evaluation (Yukawa: rsqrt + ex2)
         w = {1: 10.0, 2: 13.0, 3: 11.0}[cfg["kernel"]]
@@ -464,8 +471,8 @@ def main():
             # detects and copies once: x, y, z, q go host->device, potentials back
             "e2e": {"value": e2e, "unit": "targets/s", "h2d_bytes_per_step": 4 * 8 * n,
                     "d2h_bytes_per_step": 8 * n, "ms_per_step": ms_e2e / args.steps},
-            "roofline": roofline(sfu, achieved, peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_rate,
-                                 traffic_from_profiles(args.config)),
+            "roofline": roofline(sfu, achieved, peak, B.PRECISION_FP64 if fp64_kernels else prec, rep, ev_ms, w,
+                                 mufu_per_eval, rsqrt_rate, traffic_from_profiles(args.config)),
             "phases_ms": {k: rep[k] for k in ("ms_setup", "ms_upward", "ms_compute", "ms_downward", "ms_transfer")},
             "interactions": {k: rep[k] for k in ("pp_ptwise", "pc_ptwise", "cp_ptwise", "cc_ptwise")},
             "clocks": clock_info,
