@@ -27,6 +27,7 @@
 #include "bt_mixed.h"
 #include "bt_learned.h"
 #include "bt_gputree.h"
+#include "bt_ss.h"
 #include "bt_host.h"
 
 namespace {
@@ -155,8 +156,20 @@ int validate(int nt, int ns, const void *tx, const void *ty, const void *tz, con
         set_err("kernel %d not provided (COULOMB, YUKAWA, REGULARIZED_COULOMB are)", p.kernel);
         return BT_ERR_UNSUPPORTED;
     }
-    if (p.sing == SUBTRACTION) { set_err("singularity subtraction is not provided"); return BT_ERR_UNSUPPORTED; }
-    if (p.sing != SKIPPING) { set_err("invalid singularity %d", p.sing); return BT_ERR_PARAM; }
+    if (p.sing == SUBTRACTION) {
+        // the reference has subtraction kernels for PC (all three kernels,
+        // Lagrange and Hermite) and for CP / CC with Coulomb and Yukawa,
+        // Lagrange only (src/interaction_compute/interaction_compute_cp.c:96-290,
+        // interaction_compute_cc.c:129-290, interaction_compute_downpass.c:126-128)
+        if (p.ctype != PARTICLE_CLUSTER && (p.approx == HERMITE || p.kernel == REGULARIZED_COULOMB)) {
+            set_err("singularity subtraction with cluster-particle or cluster-cluster is provided for Coulomb and "
+                    "Yukawa with Lagrange interpolation");
+            return BT_ERR_UNSUPPORTED;
+        }
+    } else if (p.sing != SKIPPING) {
+        set_err("invalid singularity %d", p.sing);
+        return BT_ERR_PARAM;
+    }
     if (p.approx != LAGRANGE && p.approx != HERMITE) { set_err("invalid approximation %d", p.approx); return BT_ERR_PARAM; }
     if (p.ctype != PARTICLE_CLUSTER && p.ctype != CLUSTER_PARTICLE && p.ctype != CLUSTER_CLUSTER) {
         set_err("invalid compute type %d", p.ctype);
@@ -305,6 +318,13 @@ struct Systems {
     Systems(int nsys, const long long *t, const long long *s) : n(nsys), toff(t, t + nsys + 1), soff(s, s + nsys + 1) {}
 };
 
+// Singularity subtraction inputs in caller order: target charges and
+// source weights (host or device memory).
+struct SsIn {
+    const double *tq, *sw;
+    bool on_device;
+};
+
 // Whether two host arrays hold the same bits (parallel compare).
 bool same_host(const double *a, const double *b, size_t n)
 {
@@ -444,6 +464,9 @@ struct DevPlan {
     double *d_xgrid[BT_MAX_DEGREE + 1] = {}, *d_xQ[BT_MAX_DEGREE + 1] = {};
     float *d_xQ32[BT_MAX_DEGREE + 1] = {};
     double *d_out = nullptr;    // potentials in caller order (run_plan's own buffer)
+    bool ss = false;                        // singularity subtraction
+    double kp2 = 0.0, ss_c = 0.0;           // kernel_params[1]; correction constant
+    double *d_tq = nullptr, *d_sw = nullptr, *d_qw = nullptr, *d_W = nullptr, *d_Phiw = nullptr;
     bt::HermChunk *d_hchunks = nullptr;     // Hermite P2M: particle chunks of every node
     int3 *d_hred = nullptr;                 // nodes with several chunks
     double *d_hpartial = nullptr;           // their partial moments
@@ -531,7 +554,29 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     }
     if (ev) CK(record(0));
     // upward pass
-    if (need_src_clusters && ns > 0) {
+    if (need_src_clusters && ns > 0 && v.ss) {
+        // subtraction: proxies of q*w (Q) and of w (W) by the same passes
+        const double *charges[2] = {v.d_qw, v.d_sw};
+        double *proxies[2] = {d_Q, v.d_W};
+        for (int k = 0; k < 2; k++) {
+            if (herm) {
+                bt::launch_p2m_hermite(n, v.n_hchunks, v.d_hchunks, v.n_hred, v.d_hred, d_sgrid, d_slen, d_ww, d_sx,
+                                       d_sy, d_sz, charges[k], proxies[k], v.d_hpartial, st);
+                launches += v.n_hred > 0 ? 2 : 1;
+                continue;
+            }
+            bt::launch_p2m(n, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
+                           d_sz, charges[k], proxies[k], st);
+            launches++;
+            for (int l = v.S_max_depth - 1; l >= 0; l--) {
+                int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
+                if (cnt > 0) {
+                    bt::launch_m2m(n, cnt, d_slvl + v.S_lvl_off[l], d_snch, d_sch, d_sgrid, proxies[k], st);
+                    launches++;
+                }
+            }
+        }
+    } else if (need_src_clusters && ns > 0) {
         if (herm) {
             bt::launch_p2m_hermite(n, v.n_hchunks, v.d_hchunks, v.n_hred, v.d_hred, d_sgrid, d_slen, d_ww, d_sx, d_sy,
                                    d_sz, d_sq, d_Q, v.d_hpartial, st);
@@ -551,7 +596,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
             }
         }
         if (mixed) {
-            bt::launch_to_f32((size_t)v.S_n * P, d_Q, d_Q32, st);
+            bt::launch_to_f32((size_t)v.S_n * P * (herm ? 8 : 1), d_Q, d_Q32, st);
             launches++;
         }
         // proxy charges at the other degrees chosen per interaction
@@ -575,7 +620,16 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     if (ev) CK(record(1));
     // grid-output evaluation (CP, M2L) and L2L
     if (mixed && v.queue) CK(cudaMemsetAsync(d_queue, 0, 2 * sizeof(int), st));
-    if (need_tgt_grids && nt > 0 && mixed) {
+    if (need_tgt_grids && nt > 0 && v.ss) {
+        bt::SsGridsArgs g;
+        g.n = n; g.nitems = v.n_grid_items; g.items = d_griditems; g.t_grid = d_tgrid;
+        g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_cpoff; g.p_idx = d_cpidx;
+        g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.Q = d_Q; g.W = v.d_W;
+        g.sx = d_sx; g.sy = d_sy; g.sz = d_sz; g.sq = d_sq; g.sw = v.d_sw; g.kp = v.kp;
+        g.Phi_q = d_Phi; g.Phi_w = v.d_Phiw;
+        bt::launch_ss_grids(v.kernel, g, st);
+        launches++;
+    } else if (need_tgt_grids && nt > 0 && mixed) {
         bt::MixedGridsArgs g;
         g.n = n; g.nitems = v.n_grid_items; g.items = d_griditems; g.t_grid = d_tgrid; g.t_ctr = d_tctr;
         g.queue = v.queue ? d_queue : nullptr;
@@ -596,10 +650,19 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     CK(cudaGetLastError());
     if (ev) CK(record(2));
     // particle-output evaluation (PC, PP)
-    if (nt > 0 && mixed) {
+    if (nt > 0 && v.ss) {
+        bt::SsTargetsArgs a;
+        a.n = n; a.nitems = v.n_ev_items; a.items = d_evitems; a.leaf_node = d_tleaves;
+        a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.a_off = d_aoff; a.a_idx = d_aidx; a.d_off = d_doff; a.d_idx = d_didx;
+        a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_grid = d_sgrid; a.Q = d_Q; a.W = v.d_W;
+        a.sx = d_sx; a.sy = d_sy; a.sz = d_sz; a.sq = d_sq; a.sw = v.d_sw;
+        a.tx = d_tx; a.ty = d_ty; a.tz = d_tz; a.tq = v.d_tq; a.kp = v.kp; a.kp2 = v.kp2; a.pot = d_pot;
+        bt::launch_ss_targets(v.kernel, herm, a, st);
+        launches++;
+    } else if (nt > 0 && mixed) {
         bt::MixedTargetsArgs a;
         memset(&a, 0, sizeof a);
-        a.n = n; a.max_np1 = max_np1; a.nitems = v.n_ev_items; a.items = d_evitems;
+        a.n = n; a.max_np1 = max_np1; a.nitems = v.n_ev_items; a.items = d_evitems; a.herm = herm;
         a.queue = v.queue ? d_queue + 1 : nullptr;
         a.leaf_node = d_tleaves; a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.t_ctr = d_tctr; a.tpos = d_tpos;
         a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = d_adeg;
@@ -638,6 +701,25 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         bt::launch_l2p(n, herm, v.n_l2p_items, d_l2pitems, d_tleaves, d_tpar, d_tibeg, d_tnum, d_tgrid,
                        d_tlen, d_ww, d_Phi, d_tx, d_ty, d_tz, d_pot, st);
         launches++;
+        if (v.ss) {
+            // the weight field, interpolated and multiplied by -tq per target
+            for (int l = 0; l < v.T_max_depth; l++) {
+                int cnt = v.T_lvl_off[l + 1] - v.T_lvl_off[l];
+                if (cnt > 0) {
+                    bt::launch_l2l(n, cnt, d_tlvl + v.T_lvl_off[l], d_tnch, d_tch, d_tgrid, v.d_Phiw, st);
+                    launches++;
+                }
+            }
+            bt::launch_l2p(n, false, v.n_l2p_items, d_l2pitems, d_tleaves, d_tpar, d_tibeg, d_tnum, d_tgrid,
+                           d_tlen, d_ww, v.d_Phiw, d_tx, d_ty, d_tz, d_pot, st, v.d_tq);
+            launches++;
+        }
+    }
+    if (v.ss && nt > 0) {
+        // subtraction correction (InteractionCompute_SubtractionPotentialCorrection,
+        // src/interaction_compute/interaction_compute_correction.c:22-45)
+        bt::launch_ss_correction(nt, v.ss_c, v.d_tq, d_pot, st);
+        launches++;
     }
     CK(cudaGetLastError());
     if (ev) CK(record(4));
@@ -652,7 +734,8 @@ done:
 // execute = false: prepare only (uploads done, the device sequence not
 // issued), for capture into a graph by the caller.
 int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on_device, bt_report *rep,
-             const DevParts *dp = nullptr, bool queue = false, DevPlan *dv_out = nullptr, bool execute = true)
+             const DevParts *dp = nullptr, bool queue = false, DevPlan *dv_out = nullptr, bool execute = true,
+             const SsIn *ss = nullptr)
 {
     const bt_params &o = pl.prm;
     const int n = o.degree, P = o.P;
@@ -705,7 +788,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) c += S.numpar[pl.t_direct.idx[k]];
         leaf_cost[u] = c;
     }
-    const bool mixed = o.precision == BT_PRECISION_MIXED && !herm;
+    const bool ssm = ss != nullptr;
+    // mixed precision: Lagrange, and Hermite particle-cluster (its far field
+    // in FP32 over the 8 moments); Hermite grid outputs and subtraction
+    // evaluate in FP64
+    const bool mixed = o.precision == BT_PRECISION_MIXED && !ssm && (!herm || o.ctype == PARTICLE_CLUSTER);
     std::vector<int2> ev_items =
         make_items(T.nleaves, leaf_count.data(), mixed ? bt::mixed_targets_chunk() : 128, leaf_cost);
     std::vector<int2> grid_items, l2p_items;
@@ -796,6 +883,17 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     L.add(&d_out, nt);
     int *d_queue;           // work-queue counters of the two evaluation kernels
     L.add(&d_queue, 2);
+    // subtraction: target charges and source weights in tree order, q*w,
+    // the weight proxies and the weight field, a staging buffer for the
+    // caller-order inputs, and the source order when the host built the tree
+    double *d_tq = nullptr, *d_sw = nullptr, *d_qw = nullptr, *d_W = nullptr, *d_Phiw = nullptr, *d_ssin = nullptr;
+    int *d_sordh = nullptr;
+    if (ssm) {
+        L.add(&d_tq, nt); L.add(&d_sw, ns); L.add(&d_qw, ns); L.add(&d_ssin, std::max(nt, ns));
+        if (need_src_clusters) L.add(&d_W, (size_t)S.n * P * nq);
+        if (need_tgt_grids) L.add(&d_Phiw, (size_t)T.n * P);
+        if (!dp) L.add(&d_sordh, ns);
+    }
     if (herm && need_src_clusters) {
         L.add(&d_hchunks, hchunks.size());
         L.add(&d_hred, hred.size());
@@ -812,7 +910,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     float *d_xQ32[BT_MAX_DEGREE + 1] = {};
     if (mixed) {
         L.add(&d_spos, ns); L.add(&d_tpos, nt);
-        if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P);
+        if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P * nq);
         L.add(&d_sctr, sctr.size()); L.add(&d_tctr, tctr.size());
         L.add(&d_mxdoff, mx_doff.size()); L.add(&d_mxdidx, mx_didx.size()); L.add(&d_mxdflag, mx_dflag.size());
         L.add(&d_mxcpoff, mx_cpoff.size()); L.add(&d_mxcpidx, mx_cpidx.size());
@@ -865,6 +963,17 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         }
         UP(d_griditems, grid_items.data(), grid_items.size());
         UP(d_l2pitems, l2p_items.data(), l2p_items.size());
+        if (ssm) {
+            const cudaMemcpyKind kin = ss->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+            const int *sorder = dp ? dp->sorder : d_sordh;
+            if (!dp) UP(d_sordh, pl.src.order, ns);
+            if (nt > 0) CK(cudaMemcpyAsync(d_ssin, ss->tq, sizeof(double) * (size_t)nt, kin, st));
+            bt::launch_gather(nt, d_order, d_ssin, d_tq, st);
+            if (ns > 0) CK(cudaMemcpyAsync(d_ssin, ss->sw, sizeof(double) * (size_t)ns, kin, st));
+            bt::launch_gather(ns, sorder, d_ssin, d_sw, st);
+            bt::launch_mul(ns, d_sq, d_sw, d_qw, st);
+            launches += 3;
+        }
         if (mixed) {
             UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
@@ -889,6 +998,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.xdeg = xdeg;
         v.n_grid_items = (int)grid_items.size(); v.n_ev_items = (int)ev_items.size(); v.n_l2p_items = (int)l2p_items.size();
         v.d_hchunks = d_hchunks; v.d_hred = d_hred; v.d_hpartial = d_hpartial;
+        v.ss = ssm; v.kp2 = o.kp2; v.ss_c = ssm ? bt::ss_correction_constant(o.kernel, o.kp) : 0.0;
+        v.d_tq = d_tq; v.d_sw = d_sw; v.d_qw = d_qw; v.d_W = d_W; v.d_Phiw = d_Phiw;
         v.n_hchunks = (int)hchunks.size(); v.n_hred = (int)hred.size();
         v.d_sx = d_sx;
         v.d_sy = d_sy;
@@ -1202,7 +1313,8 @@ int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double 
 
 int eval_common(const Systems &sys, const double *tx, const double *ty, const double *tz, const double *sx,
                 const double *sy, const double *sz, const double *sq, double *out, bt_params &prm,
-                const bt_options *opts, bt_report *rep, bool use_static_scratch = false)
+                const bt_options *opts, bt_report *rep, bool use_static_scratch = false,
+                const double *tq = nullptr, const double *sw = nullptr)
 {
     g_err[0] = 0;
     const int64_t nt64 = sys.toff[sys.n], ns64 = sys.soff[sys.n];
@@ -1223,6 +1335,18 @@ int eval_common(const Systems &sys, const double *tx, const double *ty, const do
     double tol = 1e-6;
     rc = parse_options(opts, prm, learned, tol, queue);
     if (rc != BT_OK) return rc;
+    if (prm.sing == SUBTRACTION) {
+        // Particles_Validate (src/particles/particles.c:170-193): subtraction
+        // needs the target charges and source weights
+        if (!tq || !sw) {
+            set_err("singularity subtraction needs target charges and source weights");
+            return BT_ERR_PARAM;
+        }
+        if (learned) {
+            set_err("learned degree selection is not provided with singularity subtraction");
+            return BT_ERR_UNSUPPORTED;
+        }
+    }
     DeviceCtx *ctx = nullptr;
     rc = get_ctx(device, &ctx);
     if (rc != BT_OK) return rc;
@@ -1286,7 +1410,8 @@ int eval_common(const Systems &sys, const double *tx, const double *ty, const do
             rep->ms_setup = now_ms() - t0;
         }
     }
-    rc = run_plan(ctx, *arena, pl, out, on_dev, rep, dpp, queue);
+    SsIn ssin{tq, sw, on_dev};
+    rc = run_plan(ctx, *arena, pl, out, on_dev, rep, dpp, queue, nullptr, true, prm.sing == SUBTRACTION ? &ssin : nullptr);
     bt_plan_free(&pl);
     if (rc != BT_OK && !on_dev) memset(out, 0, sizeof(double) * (size_t)nt);
     return rc;
@@ -1340,13 +1465,12 @@ int BaryTreeInterface_ex(int numTargets, int numSources, const double *targetX, 
                          double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
                          double sizeCheck, double beta, int verbosity)
 {
-    (void)targetValue; (void)sourceWeight;
     bt_params prm;
     bt_params_setup(&prm, kernel, numKernelParams, kernelParams, singularity, approximation, compute_type, theta,
                     interpOrder, maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, beta, verbosity);
     bt_report rep;
     int rc = eval_common(Systems(numTargets, numSources), targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
-                         outputArray, prm, nullptr, verbosity > 0 ? &rep : nullptr);
+                         outputArray, prm, nullptr, verbosity > 0 ? &rep : nullptr, false, targetValue, sourceWeight);
     if (verbosity > 0 && rc == BT_OK) {
         printf("[BaryTree] barytree_b200: %d targets, %d sources, setup %.3f ms, upward %.3f ms, "
                "compute %.3f ms, downward %.3f ms, total %.3f ms\n",

@@ -705,7 +705,7 @@ __global__ void __launch_bounds__(L2P_THREADS)
 k_l2p(int n, const int2 *__restrict__ items, const int *__restrict__ leaf_node, const int *__restrict__ t_ibeg,
       const int *__restrict__ t_numpar, const double *__restrict__ t_grid, const double *__restrict__ Phi,
       const double *__restrict__ tx, const double *__restrict__ ty, const double *__restrict__ tz,
-      double *__restrict__ pot)
+      const double *__restrict__ mult, double *__restrict__ pot)
 {
     extern __shared__ double sm[];
     const int2 it = items[blockIdx.x];
@@ -736,7 +736,7 @@ k_l2p(int n, const int2 *__restrict__ items, const int *__restrict__ leaf_node, 
         }
         acc += Lb[(2 * np1 + k3) * L2P_THREADS + threadIdx.x] * s3;
     }
-    pot[t] += acc;
+    pot[t] += mult ? -mult[t] * acc : acc;
 }
 
 // Hermite downward pass (cp_comp_pot_hermite, src/interaction_compute/interaction_compute_downpass.c:860-1109):
@@ -1009,14 +1009,15 @@ void launch_eval_grids(int kernel, bool hermite, const EvalGridsArgs &a, cudaStr
 void launch_l2p(int n, bool hermite, int nitems, const int2 *items, const int *leaf_node, const int *parent,
                 const int *t_ibeg, const int *t_numpar, const double *t_grid, const double *box_len,
                 const double *ww, const double *Phi, const double *tx, const double *ty, const double *tz,
-                double *pot, cudaStream_t st)
+                double *pot, cudaStream_t st, const double *mult)
 {
     if (nitems <= 0) return;
     int np1 = n + 1, P = np1 * np1 * np1;
     if (!hermite) {
         size_t sm = sizeof(double) * (size_t)(3 * np1 + P + 3 * np1 * L2P_THREADS);
         cudaFuncSetAttribute(k_l2p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_l2p<<<nitems, L2P_THREADS, sm, st>>>(n, items, leaf_node, t_ibeg, t_numpar, t_grid, Phi, tx, ty, tz, pot);
+        k_l2p<<<nitems, L2P_THREADS, sm, st>>>(n, items, leaf_node, t_ibeg, t_numpar, t_grid, Phi, tx, ty, tz, mult,
+                                               pot);
     } else {
         size_t sm = sizeof(double) * (size_t)(3 * np1 + 8 * P + 6 * np1 * L2P_THREADS);
         cudaFuncSetAttribute(k_l2p_hermite, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

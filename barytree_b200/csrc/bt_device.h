@@ -60,7 +60,7 @@ void launch_eval_grids(int kernel, bool hermite, const EvalGridsArgs &a, cudaStr
 void launch_l2p(int n, bool hermite, int nitems, const int2 *items, const int *leaf_node, const int *parent,
                 const int *t_ibeg, const int *t_numpar, const double *t_grid, const double *box_len,
                 const double *ww, const double *Phi, const double *tx, const double *ty, const double *tz,
-                double *pot, cudaStream_t st);
+                double *pot, cudaStream_t st, const double *mult = nullptr);
 void launch_scatter(int n, const int *order, const double *src, double *dst, cudaStream_t st);
 // dst[i] = src[order[i]] (inputs in caller order -> tree order)
 void launch_gather(int n, const int *order, const double *src, double *dst, cudaStream_t st);

@@ -49,6 +49,7 @@ typedef struct {
 typedef struct {
     int kernel, approx, sing, ctype, degree, P, maxs, maxt;
     double theta, size_check, kp, beta;
+    double kp2;             /* kernel_params[1] (regularized Coulomb with subtraction: epsilon) */
     int verbosity;
     int precision;          /* 0 = FP64, 1 = mixed (FP32 evaluations, FP64 reductions) */
 } bt_params;

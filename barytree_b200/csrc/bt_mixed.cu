@@ -137,6 +137,96 @@ __device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, con
     for (int t = 0; t < NT; t++) out[t] = 0.f;
 }
 
+// Hermite far field of one source cluster for NT targets (FP32; moments
+// q[m * P + j], m = 0..7 in the reference's order q, qx, qy, qz, qxy, qyz,
+// qxz, qxyz, with qxy..qxz pre-multiplied by 3 and qxyz by 15 when staged).
+// The terms of K_*_PC_Hermite (src/kernels/coulomb/coulomb_pc.c:66-138,
+// yukawa/yukawa_pc.c, regularized-coulomb/regularized-coulomb_pc.c):
+//   r^-1 q + r^-3 (qx dx + qy dy + qz dz) + 3 r^-5 (qxy dx dy + qyz dy dz
+//   + qxz dx dz) + 15 r^-7 qxyz dx dy dz, Yukawa with exp(-kappa r) and the
+//   polynomials in kappa r.  Kahan-compensated per grid row.
+template <int KT, int NP1, int NT>
+__device__ __forceinline__ void pc_cluster_herm(const float *x, const float *y, const float *z, const float *g,
+                                                const float *q, float kc, float kp, float *out)
+{
+    constexpr int P = NP1 * NP1 * NP1;
+    float gx[NT][NP1];
+#pragma unroll
+    for (int t = 0; t < NT; t++)
+#pragma unroll
+        for (int k = 0; k < NP1; k++) gx[t][k] = x[t] - g[k];
+    float s[NT], c[NT];
+#pragma unroll
+    for (int t = 0; t < NT; t++) { s[t] = 0.f; c[t] = 0.f; }
+    int j = 0;
+    for (int k3 = 0; k3 < NP1; k3++) {
+        const float gz = g[2 * NP1 + k3];
+        for (int k2 = 0; k2 < NP1; k2++) {
+            const float gy = g[NP1 + k2];
+            float dy[NT], dz[NT], dyz[NT], dydz[NT], row[NT];
+#pragma unroll
+            for (int t = 0; t < NT; t++) {
+                dy[t] = y[t] - gy;
+                dz[t] = z[t] - gz;
+                dyz[t] = fmaf(dy[t], dy[t], dz[t] * dz[t]);
+                if (KT == 3) dyz[t] += kc;
+                dydz[t] = dy[t] * dz[t];
+                row[t] = 0.f;
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < NP1; k1++) {
+                const int jj = j + k1;
+                const float q0 = q[jj], q1 = q[P + jj], q2 = q[2 * P + jj], q3 = q[3 * P + jj];
+                const float q4 = q[4 * P + jj], q5 = q[5 * P + jj], q6 = q[6 * P + jj], q7 = q[7 * P + jj];
+#pragma unroll
+                for (int t = 0; t < NT; t++) {
+                    const float dx = gx[t][k1];
+                    const float r2 = fmaf(dx, dx, dyz[t]);
+                    const float rinv = rsqrt_apx(r2);
+                    const float rinv2 = rinv * rinv;
+                    const float dxdy = dx * dy[t], dxdz = dx * dz[t];
+                    const float a1 = fmaf(q1, dx, fmaf(q2, dy[t], q3 * dz[t]));
+                    const float a2 = fmaf(q4, dxdy, fmaf(q5, dydz[t], q6 * dxdz));
+                    const float a3 = q7 * dxdy * dz[t];
+                    if (KT == 2) {
+                        // Yukawa: exp(-kappa r) (r^-1 q + r^-3 (1 + kr) a1 + r^-5 (3 + 3kr + k^2r^2) a2
+                        // + r^-7 (15 + 15kr + 6k^2r^2 + k^3r^3) a3), with a2, a3 staged x3, x15
+                        const float r = r2 * rinv, kr = kp * r, kr2 = kr * kr;
+                        const float e = ex2_apx(kc * r);
+                        const float p1 = 1.0f + kr;
+                        const float p2 = fmaf(kr2, 1.0f / 3.0f, p1);                    // (3 + 3kr + k^2r^2) / 3
+                        const float p3 = fmaf(kr2 * kr, 1.0f / 15.0f, fmaf(kr2, 0.4f, p1));  // (15 + 15kr + 6k^2r^2 + k^3r^3) / 15
+                        const float r3 = rinv * rinv2, r5 = r3 * rinv2, r7 = r5 * rinv2;
+                        row[t] = fmaf(e, fmaf(rinv, q0, fmaf(r3 * p1, a1, fmaf(r5 * p2, a2, r7 * p3 * a3))), row[t]);
+                    } else {
+                        const float r3 = rinv * rinv2, r5 = r3 * rinv2, r7 = r5 * rinv2;
+                        row[t] = fmaf(rinv, q0, fmaf(r3, a1, fmaf(r5, a2, fmaf(r7, a3, row[t]))));
+                    }
+                }
+            }
+            j += NP1;
+#pragma unroll
+            for (int t = 0; t < NT; t++) kahan_add(s[t], c[t], row[t]);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = s[t] - c[t];
+}
+
+template <int KT, int NT>
+__device__ void pc_cluster_herm_dispatch(int np1, const float *x, const float *y, const float *z, const float *g,
+                                         const float *q, float kc, float kp, float *out)
+{
+    switch (np1) {
+#define BT_CASE(N) case N: pc_cluster_herm<KT, N, NT>(x, y, z, g, q, kc, kp, out); return;
+        BT_CASE(2) BT_CASE(3) BT_CASE(4) BT_CASE(5) BT_CASE(6) BT_CASE(7) BT_CASE(8)
+        BT_CASE(9) BT_CASE(10) BT_CASE(11) BT_CASE(12) BT_CASE(13)
+#undef BT_CASE
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = 0.f;
+}
+
 // Near-field tiles.  FP32 leaf-relative coordinates carry an absolute error
 // of about 6e-8 of the leaf size, a large relative error for a pair much
 // closer than the leaf size, and such a pair dominates its target's
@@ -297,7 +387,7 @@ __device__ __forceinline__ int next_item(int *queue, int *slot)
     return w;
 }
 
-template <int KT>
+template <int KT, bool HERM>
 __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const int2 it, float *smf)
 {
     const int u = it.x;
@@ -329,16 +419,26 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
         float *g = smf;
         float *q = smf + 3 * 16;
         const double *gs = a.s_grid[deg] + (size_t)s * 3 * np1;
-        const float *Qs = a.Q32[deg] + (size_t)s * P;
         for (int i = threadIdx.x; i < 3 * np1; i += blockDim.x) {
             int ax = i / np1;
             double c = ax == 0 ? cx : ax == 1 ? cy : cz;
             g[ax * np1 + (i % np1)] = (float)(gs[i] - c);
         }
-        for (int i = threadIdx.x; i < P; i += blockDim.x) q[i] = Qs[i];
-        __syncthreads();
         float v[MX_TPT];
-        pc_cluster_dispatch<KT, MX_TPT>(np1, x, y, z, g, q, kc, v);
+        if (HERM) {
+            const float *Qs = a.Q32[deg] + (size_t)s * 8 * P;
+            for (int i = threadIdx.x; i < 8 * P; i += blockDim.x) {
+                const int m = i / P;
+                q[i] = Qs[i] * (m == 7 ? 15.0f : m >= 4 ? 3.0f : 1.0f);
+            }
+            __syncthreads();
+            pc_cluster_herm_dispatch<KT, MX_TPT>(np1, x, y, z, g, q, kc, (float)a.kp, v);
+        } else {
+            const float *Qs = a.Q32[deg] + (size_t)s * P;
+            for (int i = threadIdx.x; i < P; i += blockDim.x) q[i] = Qs[i];
+            __syncthreads();
+            pc_cluster_dispatch<KT, MX_TPT>(np1, x, y, z, g, q, kc, v);
+        }
 #pragma unroll
         for (int t = 0; t < MX_TPT; t++) acc[t] += (double)v[t];
         __syncthreads();
@@ -392,7 +492,7 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
         if (act[t]) a.pot[tid[t]] = acc[t];
 }
 
-template <int KT>
+template <int KT, bool HERM>
 __global__ void BT_MX_BOUNDS
 k_eval_targets_mixed(MixedTargetsArgs a)
 {
@@ -400,7 +500,7 @@ k_eval_targets_mixed(MixedTargetsArgs a)
     __shared__ int slot;
     int w = a.queue ? next_item(a.queue, &slot) : blockIdx.x;
     while (w < a.nitems) {
-        targets_item<KT>(a, a.items[w], smf);
+        targets_item<KT, HERM>(a, a.items[w], smf);
         if (!a.queue) break;
         w = next_item(a.queue, &slot);
     }
@@ -511,9 +611,9 @@ void launch_to_f32(size_t n, const double *src, float *dst, cudaStream_t st)
 
 int mixed_targets_chunk() { return MX_CHUNK; }
 
-static size_t mixed_smem(int max_np1)
+static size_t mixed_smem(int max_np1, bool herm = false)
 {
-    size_t far = sizeof(float) * (size_t)(3 * 16 + max_np1 * max_np1 * max_np1);
+    size_t far = sizeof(float) * (size_t)(3 * 16 + (herm ? 8 : 1) * max_np1 * max_np1 * max_np1);
     size_t near = sizeof(float4) * MX_TILE;
     return far > near ? far : near;
 }
@@ -530,21 +630,21 @@ static int queue_grid(K kernel, size_t smem, int nitems)
     return g < nitems ? g : nitems;
 }
 
-template <int KT>
+template <int KT, bool HERM>
 static void eval_targets_mixed_t(const MixedTargetsArgs &a, cudaStream_t st)
 {
-    size_t sm = mixed_smem(a.max_np1);
-    cudaFuncSetAttribute(k_eval_targets_mixed<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int grid = a.queue ? queue_grid(k_eval_targets_mixed<KT>, sm, a.nitems) : a.nitems;
-    k_eval_targets_mixed<KT><<<grid, MX_THREADS, sm, st>>>(a);
+    size_t sm = mixed_smem(a.max_np1, HERM);
+    cudaFuncSetAttribute(k_eval_targets_mixed<KT, HERM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int grid = a.queue ? queue_grid(k_eval_targets_mixed<KT, HERM>, sm, a.nitems) : a.nitems;
+    k_eval_targets_mixed<KT, HERM><<<grid, MX_THREADS, sm, st>>>(a);
 }
 
 void launch_eval_targets_mixed(int kernel, const MixedTargetsArgs &a, cudaStream_t st)
 {
     if (a.nitems <= 0) return;
-    if (kernel == 1) eval_targets_mixed_t<1>(a, st);
-    else if (kernel == 2) eval_targets_mixed_t<2>(a, st);
-    else eval_targets_mixed_t<3>(a, st);
+    if (kernel == 1) a.herm ? eval_targets_mixed_t<1, true>(a, st) : eval_targets_mixed_t<1, false>(a, st);
+    else if (kernel == 2) a.herm ? eval_targets_mixed_t<2, true>(a, st) : eval_targets_mixed_t<2, false>(a, st);
+    else a.herm ? eval_targets_mixed_t<3, true>(a, st) : eval_targets_mixed_t<3, false>(a, st);
 }
 
 template <int KT>

@@ -19,6 +19,7 @@ struct MixedTargetsArgs {
     int n, max_np1, nitems;
     const int2 *items;
     int *queue;                                 // work-queue counter (zeroed), or nullptr: one block per item
+    bool herm;                                  // Hermite far field (Q32: 8 moments of P per node)
     const int *leaf_node, *t_ibeg, *t_numpar;
     const double *t_ctr;                        // target node centres (FP64, 3 per node)
     const float4 *tpos;                         // targets relative to their leaf centre

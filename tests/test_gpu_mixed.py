@@ -46,12 +46,31 @@ def test_mixed_vs_direct_degree8(ctype):
     assert np.linalg.norm(pot[idx] - d) / np.linalg.norm(d) <= TOL_VS_DIRECT
 
 
-def test_mixed_hermite_runs_in_fp64():
-    """Hermite has no FP32 kernels: the mixed option evaluates it with the FP64 kernels."""
+@pytest.mark.parametrize("kernel,kp", [(1, 0.0), (2, 0.5), (3, 1e-3)])
+def test_mixed_hermite_particle_cluster(kernel, kp):
+    """Hermite PC in mixed precision (FP32 over the 8 moments, FP64 upward
+    pass) against the FP64 Hermite treecode, and against the direct sum."""
+    rng = np.random.default_rng(40 + kernel)
+    n = 40000
+    x, y, z = (np.clip(rng.normal(0, 0.25, n), -1, 1) for _ in range(3))
+    q = rng.choice([-1.0, 1.0], n)
+    kw = dict(kernel=kernel, kernel_param=kp, approximation=2, degree=6, max_source_leaf=1000, max_target_leaf=1000,
+              size_check=4.0)
+    a = B.treecode(x, y, z, x, y, z, q, precision=B.PRECISION_MIXED, **kw)
+    b = B.treecode(x, y, z, x, y, z, q, precision=B.PRECISION_FP64, **kw)
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) <= (TOL_VS_FP64_TREE_YUKAWA if kernel == 2 else TOL_VS_FP64_TREE)
+    idx = np.arange(0, n, 13)
+    d = B.direct(x[idx], y[idx], z[idx], x, y, z, q, kernel, kp)
+    assert np.linalg.norm(a[idx] - d) / np.linalg.norm(d) <= TOL_VS_DIRECT
+
+
+def test_mixed_hermite_grid_outputs_run_in_fp64():
+    """Hermite cluster-particle has no FP32 kernels: the mixed option
+    evaluates it with the FP64 kernels, bit for bit."""
     tx, ty, tz, sx, sy, sz, sq = uniform_inputs(4, 8000)
-    a = B.treecode(tx, ty, tz, sx, sy, sz, sq, approximation=2, degree=4, max_source_leaf=200,
+    a = B.treecode(tx, ty, tz, sx, sy, sz, sq, approximation=2, compute_type=2, degree=4, max_source_leaf=200,
                    max_target_leaf=200, size_check=4.0, precision=B.PRECISION_MIXED)
-    b = B.treecode(tx, ty, tz, sx, sy, sz, sq, approximation=2, degree=4, max_source_leaf=200,
+    b = B.treecode(tx, ty, tz, sx, sy, sz, sq, approximation=2, compute_type=2, degree=4, max_source_leaf=200,
                    max_target_leaf=200, size_check=4.0, precision=B.PRECISION_FP64)
     assert np.array_equal(a, b)
 

@@ -131,7 +131,13 @@ def test_error_codes_without_exiting():
     assert _bti(sx=None)[0] == B.BT_ERR_PARAM                  # NULL source array
     assert _bti(tx=None)[0] == B.BT_ERR_PARAM
     assert _bti(nt=-1)[0] == B.BT_ERR_PARAM
-    assert _bti(sing=2)[0] == B.BT_ERR_UNSUPPORTED              # singularity subtraction
+    assert _bti(sing=2)[0] == B.BT_ERR_PARAM                    # subtraction without target charges / weights
+    w = np.ones(100)
+    # subtraction exists for CP / CC only with Coulomb and Yukawa, Lagrange
+    # (src/interaction_compute/interaction_compute_cp.c:121-248)
+    assert _bti(sing=2, tq=w, sw=w, ctype=2, approx=2)[0] == B.BT_ERR_UNSUPPORTED
+    assert _bti(sing=2, tq=w, sw=w, ctype=3, kernel=3)[0] == B.BT_ERR_UNSUPPORTED
+    assert _bti(sing=3)[0] == B.BT_ERR_PARAM
     assert _bti(kernel=5)[0] == B.BT_ERR_UNSUPPORTED            # ATAN
     assert _bti(ctype=3, approx=2)[0] == B.BT_ERR_UNSUPPORTED   # CC Hermite (interaction_compute_cc.c:146)
     assert _bti(approx=0)[0] == B.BT_ERR_PARAM
