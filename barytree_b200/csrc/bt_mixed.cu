@@ -454,8 +454,11 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
         float xs[MX_TPT], ys[MX_TPT], zs[MX_TPT];   // targets in the source leaf's frame
 #pragma unroll
         for (int t = 0; t < MX_TPT; t++) { xs[t] = x[t] - ox; ys[t] = y[t] - oy; zs[t] = z[t] - oz; }
+        // at least the smallest normal float, so that a coincident pair (r2
+        // == 0 after flushing) always takes the FP64 path with the skipping
+        // rule, also between single-particle leaves of radius 0
         const double rr = MX_CLOSE_FRAC * (trad + a.s_rad[s]);
-        const float thr2 = (float)(rr * rr);
+        const float thr2 = fmaxf((float)(rr * rr), FLT_MIN);
         for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
             const int cm = min(MX_TILE, sn - c0), cm4 = (cm + 3) & ~3;
             for (int i = threadIdx.x; i < cm4; i += blockDim.x) {

@@ -112,3 +112,16 @@ def test_mixed_coincident_points():
                    precision=B.PRECISION_FP64)
     assert np.all(np.isfinite(a))
     assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-6
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_mixed_single_particle_leaves(kernel):
+    """Leaves of one particle (radius 0) evaluated against themselves: the
+    coincident self pair must be skipped, as in FP64."""
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(17, 3000)
+    kw = dict(kernel=kernel, kernel_param=0.5 if kernel == 2 else 0.0, degree=3, max_source_leaf=1,
+              max_target_leaf=1)
+    a = B.treecode(tx, ty, tz, sx, sy, sz, sq, precision=B.PRECISION_MIXED, **kw)
+    b = B.treecode(tx, ty, tz, sx, sy, sz, sq, precision=B.PRECISION_FP64, **kw)
+    assert np.all(np.isfinite(a))
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) <= TOL_VS_FP64_TREE_YUKAWA
