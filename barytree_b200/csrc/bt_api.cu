@@ -249,15 +249,20 @@ void count_interactions(const bt_plan &pl, bt_report *r)
     if (o.ctype == PARTICLE_CLUSTER || o.ctype == CLUSTER_PARTICLE) {
         const bt_tree &trav = o.ctype == PARTICLE_CLUSTER ? pl.st : pl.tt;
         const bt_tree &bat = o.ctype == PARTICLE_CLUSTER ? pl.tt : pl.st;
+        long long pp = 0, pa = 0, npp = 0, na_all = 0;
+#pragma omp parallel for schedule(static) reduction(+ : pp, pa, npp, na_all)
         for (int i = 0; i < bat.nleaves; i++) {
             long long m = bat.numpar[bat.leaves[i]];
-            for (int64_t k = pl.pp.off[i]; k < pl.pp.off[i + 1]; k++) r->pp_ptwise += m * trav.numpar[pl.pp.idx[k]];
+            for (int64_t k = pl.pp.off[i]; k < pl.pp.off[i + 1]; k++) pp += m * trav.numpar[pl.pp.idx[k]];
             long long na = pl.ap.off[i + 1] - pl.ap.off[i];
-            if (o.ctype == PARTICLE_CLUSTER) r->pc_ptwise += na * m * P;
-            else r->cp_ptwise += na * m * P;
-            r->num_pp += pl.pp.off[i + 1] - pl.pp.off[i];
-            if (o.ctype == PARTICLE_CLUSTER) r->num_pc += na; else r->num_cp += na;
+            pa += na * m * P;
+            npp += pl.pp.off[i + 1] - pl.pp.off[i];
+            na_all += na;
         }
+        r->pp_ptwise = pp;
+        r->num_pp = npp;
+        if (o.ctype == PARTICLE_CLUSTER) { r->pc_ptwise = pa; r->num_pc = na_all; }
+        else { r->cp_ptwise = pa; r->num_cp = na_all; }
     } else {
         for (int i = 0; i < pl.tt.n; i++) {
             long long m = pl.tt.numpar[i];
@@ -298,13 +303,21 @@ void expand_to_leaves(const bt_csr &in, const bt_tree &t, const std::vector<int>
                       const std::vector<int> &count, std::vector<int64_t> &off, std::vector<int> &idx)
 {
     off.assign(in.rows + 1, 0);
-    idx.clear();
+#pragma omp parallel for schedule(static)
     for (int r = 0; r < in.rows; r++) {
+        int64_t c = 0;
+        for (int64_t k = in.off[r]; k < in.off[r + 1]; k++) c += count[in.idx[k]];
+        off[r + 1] = c;
+    }
+    for (int r = 0; r < in.rows; r++) off[r + 1] += off[r];
+    idx.resize((size_t)off[in.rows]);
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < in.rows; r++) {
+        int64_t o = off[r];
         for (int64_t k = in.off[r]; k < in.off[r + 1]; k++) {
-            int s = in.idx[k];
-            for (int l = 0; l < count[s]; l++) idx.push_back(t.leaves[first[s] + l]);
+            const int s = in.idx[k];
+            for (int l = 0; l < count[s]; l++) idx[o++] = t.leaves[first[s] + l];
         }
-        off[r + 1] = (int64_t)idx.size();
     }
 }
 
@@ -774,6 +787,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     const bool need_tgt_grids = (o.ctype != PARTICLE_CLUSTER);
     std::vector<int> leaf_count(T.nleaves);
     std::vector<double> leaf_cost(T.nleaves, 0.0);
+#pragma omp parallel for schedule(static)
     for (int u = 0; u < T.nleaves; u++) {
         leaf_count[u] = T.numpar[T.leaves[u]];
         double c = 0;
@@ -826,6 +840,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         expand_to_leaves(pl.t_direct, S, lf, lc, mx_doff, mx_didx);
         expand_to_leaves(pl.g_cp, S, lf, lc, mx_cpoff, mx_cpidx);
         mx_dflag.resize(mx_didx.size());
+#pragma omp parallel for schedule(static)
         for (int u = 0; u < T.nleaves; u++) {
             int t = T.leaves[u];
             for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) {
@@ -1086,6 +1101,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             rep->target_nodes = T.n;
             double tend = now_ms();
             rep->ms_transfer = (tend - t_setup) - (a + b + c + d);
+            rep->ms_setup += t_setup - t0;      // host preparation of the device arrays
             rep->ms_total += tend - t0;
         }
     }
@@ -1193,19 +1209,42 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         const int rows = pl.t_approx.rows;
         int64_t *aoff = (int64_t *)malloc(sizeof(int64_t) * (rows + 1));
         int64_t *doff = (int64_t *)malloc(sizeof(int64_t) * (rows + 1));
-        std::vector<int> aidx, didx;
-        std::vector<unsigned char> adeg;
         aoff[0] = doff[0] = 0;
+        // per row: entries kept as clusters and entries moved to the direct list
+#pragma omp parallel for schedule(static)
         for (int u = 0; u < rows; u++) {
+            int64_t na = 0, nd = pl.t_direct.off[u + 1] - pl.t_direct.off[u];
             for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++) {
-                pl.sel_hist[choice[k] == bt::MLP_PP ? 13 : choice[k]]++;
-                if (choice[k] == bt::MLP_PP) didx.push_back(pl.t_approx.idx[k]);
-                else { aidx.push_back(pl.t_approx.idx[k]); adeg.push_back(choice[k]); }
+                if (choice[k] == bt::MLP_PP) nd++;
+                else na++;
             }
-            for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) didx.push_back(pl.t_direct.idx[k]);
-            aoff[u + 1] = (int64_t)aidx.size();
-            doff[u + 1] = (int64_t)didx.size();
+            aoff[u + 1] = na;
+            doff[u + 1] = nd;
         }
+        for (int u = 0; u < rows; u++) {
+            aoff[u + 1] += aoff[u];
+            doff[u + 1] += doff[u];
+        }
+        std::vector<int> aidx((size_t)aoff[rows]), didx((size_t)doff[rows]);
+        std::vector<unsigned char> adeg((size_t)aoff[rows]);
+        long long hist[14] = {};
+#pragma omp parallel
+        {
+            long long h[14] = {};
+#pragma omp for schedule(static)
+            for (int u = 0; u < rows; u++) {
+                int64_t a = aoff[u], d = doff[u];
+                for (int64_t k = pl.t_approx.off[u]; k < pl.t_approx.off[u + 1]; k++) {
+                    h[choice[k] == bt::MLP_PP ? 13 : choice[k]]++;
+                    if (choice[k] == bt::MLP_PP) didx[d++] = pl.t_approx.idx[k];
+                    else { aidx[a] = pl.t_approx.idx[k]; adeg[a++] = choice[k]; }
+                }
+                for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) didx[d++] = pl.t_direct.idx[k];
+            }
+#pragma omp critical
+            for (int i = 0; i < 14; i++) hist[i] += h[i];
+        }
+        for (int i = 0; i < 14; i++) pl.sel_hist[i] += hist[i];
         bt_csr_free(&pl.t_approx);
         bt_csr_free(&pl.t_direct);
         pl.t_approx.rows = pl.t_direct.rows = rows;
@@ -1228,6 +1267,7 @@ void count_learned(const bt_plan &pl, bt_report *r)
 {
     const bt_tree &S = pl.st, &T = pl.tt;
     long long pp = 0, pc = 0;
+#pragma omp parallel for schedule(static) reduction(+ : pp, pc)
     for (int u = 0; u < T.nleaves; u++) {
         long long m = T.numpar[T.leaves[u]];
         for (int64_t k = pl.t_direct.off[u]; k < pl.t_direct.off[u + 1]; k++) pp += m * S.numpar[pl.t_direct.idx[k]];
