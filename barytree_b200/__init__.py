@@ -36,6 +36,9 @@ class Kernel(CEnum):
     DCF = 7
     SIN_OVER_R = 8
     MQ = 9
+    RBS_U = 10
+    RBS_V = 11
+    USER = 12
 
 
 class Singularity(CEnum):
@@ -109,7 +112,7 @@ _BTI_ARGS = (
 
 # every exported symbol of include/barytree_b200.h
 EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
-                    "bt_tree_dump", "bt_tree_dump_ex", "bt_eval_batch", "bt_session_create", "bt_session_eval", "bt_session_destroy", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
+                    "bt_tree_dump", "bt_tree_dump_ex", "bt_eval_batch", "bt_direct_ex", "bt_session_create", "bt_session_eval", "bt_session_destroy", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
                     "bt_selector_nweights", "bt_selector_set", "bt_selector_training_data", "bt_selector_train",
                     "bt_mlp_loss_grad", "bt_mlp_predict")
 
@@ -147,6 +150,9 @@ def lib():
                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                 ctypes.POINTER(Options), ctypes.POINTER(Report))
     L.bt_eval_batch.restype = ctypes.c_int
+    L.bt_direct_ex.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
+                               ctypes.c_int, _dp, ctypes.c_int)
+    L.bt_direct_ex.restype = ctypes.c_int
     L.bt_session_create.argtypes = (ctypes.c_int, _llp, _llp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(Options),
@@ -370,11 +376,13 @@ def measure_peaks(device=0):
 
 
 def direct(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0, device=0):
-    """FP64 direct sum on the GPU (error reference)."""
+    """FP64 direct sum on the GPU (error reference); kernel_param may be a
+    sequence of kernel parameters (two for regularized Yukawa, atan, MQ)."""
     tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
     out = np.zeros(len(tx))
-    rc = lib().bt_direct(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
-                         int(kernel), float(kernel_param), int(device))
+    kp = _c(np.atleast_1d(np.asarray(kernel_param, dtype=np.float64)))
+    rc = lib().bt_direct_ex(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
+                            int(kernel), len(kp), _p(kp), int(device))
     _check(rc)
     return out
 

@@ -152,25 +152,49 @@ int validate(int nt, int ns, const void *tx, const void *ty, const void *tz, con
         set_err("one or more required particle arrays is unset");
         return BT_ERR_PARAM;
     }
-    if (p.kernel != COULOMB && p.kernel != YUKAWA && p.kernel != REGULARIZED_COULOMB) {
-        set_err("kernel %d not provided (COULOMB, YUKAWA, REGULARIZED_COULOMB are)", p.kernel);
-        return BT_ERR_UNSUPPORTED;
-    }
-    if (p.sing == SUBTRACTION) {
-        // the reference has subtraction kernels for PC (all three kernels,
-        // Lagrange and Hermite) and for CP / CC with Coulomb and Yukawa,
-        // Lagrange only (src/interaction_compute/interaction_compute_cp.c:96-290,
-        // interaction_compute_cc.c:129-290, interaction_compute_downpass.c:126-128)
-        if (p.ctype != PARTICLE_CLUSTER && (p.approx == HERMITE || p.kernel == REGULARIZED_COULOMB)) {
-            set_err("singularity subtraction with cluster-particle or cluster-cluster is provided for Coulomb and "
-                    "Yukawa with Lagrange interpolation");
-            return BT_ERR_UNSUPPORTED;
-        }
-    } else if (p.sing != SKIPPING) {
+    if (p.approx != LAGRANGE && p.approx != HERMITE) { set_err("invalid approximation %d", p.approx); return BT_ERR_PARAM; }
+    if (p.sing != SKIPPING && p.sing != SUBTRACTION) {
         set_err("invalid singularity %d", p.sing);
         return BT_ERR_PARAM;
     }
-    if (p.approx != LAGRANGE && p.approx != HERMITE) { set_err("invalid approximation %d", p.approx); return BT_ERR_PARAM; }
+    // kernels and the combinations the reference provides them in
+    // (src/interaction_compute/interaction_compute_pc.c, _cp.c, _cc.c; the
+    // others exit): Hermite for Coulomb, Yukawa, regularized Coulomb and
+    // sin-over-r; grid outputs (CP, CC) for all but atan and MQ; subtraction
+    // for Coulomb, Yukawa and the two regularized kernels in PC, and for
+    // Coulomb and Yukawa with Lagrange in CP / CC
+    // (interaction_compute_downpass.c:126-128)
+    const int k = p.kernel;
+    const bool known = k == COULOMB || k == YUKAWA || k == REGULARIZED_COULOMB || k == REGULARIZED_YUKAWA ||
+                       k == ATAN || k == SIN_OVER_R || k == MQ || k == RBS_U || k == RBS_V || k == USER;
+    if (!known) {
+        set_err("kernel %d not provided", k);
+        return BT_ERR_UNSUPPORTED;
+    }
+    const bool hermite_ok = k == COULOMB || k == YUKAWA || k == REGULARIZED_COULOMB || k == SIN_OVER_R;
+    if (p.approx == HERMITE && !hermite_ok) {
+        set_err("kernel %d has no Hermite form in the reference", k);
+        return BT_ERR_UNSUPPORTED;
+    }
+    if ((k == ATAN || k == MQ) && p.ctype != PARTICLE_CLUSTER) {
+        set_err("the atan and MQ kernels are provided for particle-cluster only, as in the reference");
+        return BT_ERR_UNSUPPORTED;
+    }
+    if (p.sing == SUBTRACTION) {
+        const bool ss_pc = k == COULOMB || k == YUKAWA || k == REGULARIZED_COULOMB ||
+                           (k == REGULARIZED_YUKAWA && p.approx == LAGRANGE);
+        const bool ss_grid = (k == COULOMB || k == YUKAWA) && p.approx == LAGRANGE;
+        if (!(p.ctype == PARTICLE_CLUSTER ? ss_pc : ss_grid)) {
+            set_err("singularity subtraction is not provided for kernel %d with this approximation and compute "
+                    "type (the reference exits there)", k);
+            return BT_ERR_UNSUPPORTED;
+        }
+    }
+    if ((k == REGULARIZED_YUKAWA || k == ATAN || k == MQ || (k == REGULARIZED_COULOMB && p.sing == SUBTRACTION)) &&
+        p.nkp < 2) {
+        set_err("kernel %d needs two kernel parameters", k);
+        return BT_ERR_PARAM;
+    }
     if (p.ctype != PARTICLE_CLUSTER && p.ctype != CLUSTER_PARTICLE && p.ctype != CLUSTER_CLUSTER) {
         set_err("invalid compute type %d", p.ctype);
         return BT_ERR_PARAM;
@@ -656,7 +680,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         g.n = n; g.nitems = v.n_grid_items; g.items = d_griditems; g.t_grid = d_tgrid;
         g.c_off = d_ccoff; g.c_idx = d_ccidx; g.p_off = d_cpoff; g.p_idx = d_cpidx;
         g.s_ibeg = d_sibeg; g.s_numpar = d_snum; g.s_grid = d_sgrid; g.Q = d_Q;
-        g.sx = d_sx; g.sy = d_sy; g.sz = d_sz; g.sq = d_sq; g.kp = v.kp; g.Phi = d_Phi;
+        g.sx = d_sx; g.sy = d_sy; g.sz = d_sz; g.sq = d_sq; g.kp = v.kp; g.kp2 = v.kp2; g.Phi = d_Phi;
         bt::launch_eval_grids(v.kernel, herm, g, st);
         launches++;
     }
@@ -694,7 +718,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.a_off = d_aoff; a.a_idx = d_aidx; a.d_off = d_doff; a.d_idx = d_didx;
         a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_grid = d_sgrid; a.Q = d_Q;
         a.sx = d_sx; a.sy = d_sy; a.sz = d_sz; a.sq = d_sq; a.tx = d_tx; a.ty = d_ty; a.tz = d_tz;
-        a.kp = v.kp; a.pot = d_pot;
+        a.kp = v.kp; a.kp2 = v.kp2; a.pot = d_pot;
         bt::launch_eval_targets(v.kernel, herm, a, st);
         launches++;
     }
@@ -806,7 +830,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     // mixed precision: Lagrange, and Hermite particle-cluster (its far field
     // in FP32 over the 8 moments); Hermite grid outputs and subtraction
     // evaluate in FP64
-    const bool mixed = o.precision == BT_PRECISION_MIXED && !ssm && (!herm || o.ctype == PARTICLE_CLUSTER);
+    const bool mixed = o.precision == BT_PRECISION_MIXED && !ssm && (!herm || o.ctype == PARTICLE_CLUSTER) &&
+                       o.kernel <= REGULARIZED_COULOMB;
     std::vector<int2> ev_items =
         make_items(T.nleaves, leaf_count.data(), mixed ? bt::mixed_targets_chunk() : 128, leaf_cost);
     std::vector<int2> grid_items, l2p_items;
@@ -1596,6 +1621,14 @@ int bt_direct(int numTargets, int numSources, const double *targetX, const doubl
               const double *sourceX, const double *sourceY, const double *sourceZ, const double *sourceValue,
               double *outputArray, int kernel, double kernelParam, int device)
 {
+    return bt_direct_ex(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+                        outputArray, kernel, 1, &kernelParam, device);
+}
+
+int bt_direct_ex(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,
+                 const double *sourceX, const double *sourceY, const double *sourceZ, const double *sourceValue,
+                 double *outputArray, int kernel, int numKernelParams, const double *kernelParams, int device)
+{
     g_err[0] = 0;
     if (numTargets < 0 || numSources < 0) { set_err("negative count"); return BT_ERR_PARAM; }
     if (numTargets == 0) return BT_OK;
@@ -1603,7 +1636,13 @@ int bt_direct(int numTargets, int numSources, const double *targetX, const doubl
         set_err("NULL array");
         return BT_ERR_PARAM;
     }
-    if (kernel != COULOMB && kernel != YUKAWA && kernel != REGULARIZED_COULOMB) { set_err("kernel not provided"); return BT_ERR_UNSUPPORTED; }
+    if (kernel != COULOMB && kernel != YUKAWA && kernel != REGULARIZED_COULOMB && kernel != REGULARIZED_YUKAWA &&
+        kernel != ATAN && kernel != SIN_OVER_R && kernel != MQ && kernel != RBS_U && kernel != RBS_V && kernel != USER) {
+        set_err("kernel not provided");
+        return BT_ERR_UNSUPPORTED;
+    }
+    const double kernelParam = numKernelParams > 0 && kernelParams ? kernelParams[0] : 0.0;
+    const double kernelParam2 = numKernelParams > 1 && kernelParams ? kernelParams[1] : 0.0;
     DeviceCtx *ctx = nullptr;
     int rc = get_ctx(device, &ctx);
     if (rc != BT_OK) return rc;
@@ -1623,7 +1662,7 @@ int bt_direct(int numTargets, int numSources, const double *targetX, const doubl
         if (numSources > 0)
             for (int i = 0; i < 4; i++) CK(cudaMemcpyAsync(d_s[i], hs[i], sizeof(double) * numSources, cudaMemcpyHostToDevice, st));
         bt::launch_direct(kernel, numTargets, numSources, d_t[0], d_t[1], d_t[2], d_s[0], d_s[1], d_s[2], d_s[3],
-                          kernelParam, d_o, st);
+                          kernelParam, d_o, st, kernelParam2);
         g_launches += 1;
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(outputArray, d_o, sizeof(double) * numTargets, cudaMemcpyDeviceToHost, st));

@@ -541,7 +541,7 @@ k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ le
                const double *__restrict__ Q, const double *__restrict__ sx, const double *__restrict__ sy,
                const double *__restrict__ sz, const double *__restrict__ sq,
                const double *__restrict__ tx, const double *__restrict__ ty, const double *__restrict__ tz,
-               double kp, double *__restrict__ pot)
+               double kp, double kp2, double *__restrict__ pot)
 {
     extern __shared__ double sm[];
     const int2 it = items[blockIdx.x];
@@ -571,12 +571,14 @@ k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ le
                 double dz = z - g[2 * np1 + k3];
                 for (int k2 = 0; k2 < np1; k2++) {
                     double dy = y - g[np1 + k2];
-                    if (!HERM) {
+                    if (!HERM && KT <= K_REGCOULOMB) {
                         double dyz = dy * dy + dz * dz;
                         for (int k1 = 0; k1 < np1; k1++, j++) {
                             double dx = x - g[k1];
                             acc += k_far<KT>(fma(dx, dx, dyz), q[j], kp);
                         }
+                    } else if (!HERM) {
+                        for (int k1 = 0; k1 < np1; k1++, j++) acc += k_any<KT, false>(x - g[k1], dy, dz, q[j], kp, kp2);
                     } else {
                         for (int k1 = 0; k1 < np1; k1++, j++) {
                             double dx = x - g[k1];
@@ -602,7 +604,7 @@ k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ le
                 for (int i = 0; i < cm; i++) {
                     double4 p = tile[i];
                     double dx = x - p.x, dy = y - p.y, dz = z - p.z;
-                    acc += k_pp<KT>(dx * dx + dy * dy + dz * dz, p.w, kp);
+                    acc += k_any<KT, true>(dx, dy, dz, p.w, kp, kp2);
                 }
             }
             __syncthreads();
@@ -622,7 +624,8 @@ k_eval_grids(int n, const int2 *__restrict__ items, const double *__restrict__ t
              const int64_t *__restrict__ p_off, const int *__restrict__ p_idx,
              const int *__restrict__ s_ibeg, const int *__restrict__ s_numpar, const double *__restrict__ s_grid,
              const double *__restrict__ Q, const double *__restrict__ sx, const double *__restrict__ sy,
-             const double *__restrict__ sz, const double *__restrict__ sq, double kp, double *__restrict__ Phi)
+             const double *__restrict__ sz, const double *__restrict__ sq, double kp, double kp2,
+             double *__restrict__ Phi)
 {
     extern __shared__ double sm[];
     const int2 it = items[blockIdx.x];
@@ -651,10 +654,15 @@ k_eval_grids(int n, const int2 *__restrict__ items, const double *__restrict__ t
                     double dz = z - g[2 * np1 + k3];
                     for (int k2 = 0; k2 < np1; k2++) {
                         double dy = y - g[np1 + k2];
-                        double dyz = dy * dy + dz * dz;
-                        for (int k1 = 0; k1 < np1; k1++, j++) {
-                            double dx = x - g[k1];
-                            acc[0] += k_far<KT>(fma(dx, dx, dyz), q[j], kp);
+                        if (KT <= K_REGCOULOMB) {
+                            double dyz = dy * dy + dz * dz;
+                            for (int k1 = 0; k1 < np1; k1++, j++) {
+                                double dx = x - g[k1];
+                                acc[0] += k_far<KT>(fma(dx, dx, dyz), q[j], kp);
+                            }
+                        } else {
+                            for (int k1 = 0; k1 < np1; k1++, j++)
+                                acc[0] += k_any<KT, false>(x - g[k1], dy, dz, q[j], kp, kp2);
                         }
                     }
                 }
@@ -675,8 +683,7 @@ k_eval_grids(int n, const int2 *__restrict__ items, const double *__restrict__ t
                 for (int i = 0; i < cm; i++) {
                     double4 p = tile[i];
                     if (!HERM) {
-                        double dx = x - p.x, dy = y - p.y, dz = z - p.z;
-                        acc[0] += k_far<KT>(dx * dx + dy * dy + dz * dz, p.w, kp);
+                        acc[0] += k_any<KT, false>(x - p.x, y - p.y, z - p.z, p.w, kp, kp2);
                     } else {
                         k_cp_herm<KT>(p.x - x, p.y - y, p.z - z, p.w, kp, acc);
                     }
@@ -815,7 +822,7 @@ template <int KT>
 __global__ void __launch_bounds__(EV_THREADS)
 k_direct(int nt, int ns, const double *__restrict__ tx, const double *__restrict__ ty, const double *__restrict__ tz,
          const double *__restrict__ sx, const double *__restrict__ sy, const double *__restrict__ sz,
-         const double *__restrict__ sq, double kp, double *__restrict__ out)
+         const double *__restrict__ sq, double kp, double kp2, double *__restrict__ out)
 {
     __shared__ double4 tile[PP_TILE];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -829,8 +836,7 @@ k_direct(int nt, int ns, const double *__restrict__ tx, const double *__restrict
         __syncthreads();
         for (int i = 0; i < cm; i++) {
             double4 p = tile[i];
-            double dx = x - p.x, dy = y - p.y, dz = z - p.z;
-            acc += k_pp<KT>(dx * dx + dy * dy + dz * dz, p.w, kp);
+            acc += k_any<KT, true>(x - p.x, y - p.y, z - p.z, p.w, kp, kp2);
         }
         __syncthreads();
     }
@@ -974,15 +980,29 @@ static void eval_targets_t(const EvalTargetsArgs &a, cudaStream_t st)
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     fn<<<a.nitems, EV_THREADS, sm, st>>>(a.n, a.items, a.leaf_node, a.t_ibeg, a.t_numpar, a.a_off, a.a_idx,
                                          a.d_off, a.d_idx, a.s_ibeg, a.s_numpar, a.s_grid, a.Q, a.sx, a.sy,
-                                         a.sz, a.sq, a.tx, a.ty, a.tz, a.kp, a.pot);
+                                         a.sz, a.sq, a.tx, a.ty, a.tz, a.kp, a.kp2, a.pot);
 }
 
+// Kernels with Hermite forms: Coulomb, Yukawa, regularized Coulomb, sin-over-r.
 void launch_eval_targets(int kernel, bool hermite, const EvalTargetsArgs &a, cudaStream_t st)
 {
     if (a.nitems <= 0) return;
-    if (kernel == K_COULOMB) hermite ? eval_targets_t<K_COULOMB, true>(a, st) : eval_targets_t<K_COULOMB, false>(a, st);
-    else if (kernel == K_YUKAWA) hermite ? eval_targets_t<K_YUKAWA, true>(a, st) : eval_targets_t<K_YUKAWA, false>(a, st);
-    else hermite ? eval_targets_t<K_REGCOULOMB, true>(a, st) : eval_targets_t<K_REGCOULOMB, false>(a, st);
+    switch (kernel) {
+    case K_COULOMB: hermite ? eval_targets_t<K_COULOMB, true>(a, st) : eval_targets_t<K_COULOMB, false>(a, st); break;
+    case K_YUKAWA: hermite ? eval_targets_t<K_YUKAWA, true>(a, st) : eval_targets_t<K_YUKAWA, false>(a, st); break;
+    case K_REGCOULOMB:
+        hermite ? eval_targets_t<K_REGCOULOMB, true>(a, st) : eval_targets_t<K_REGCOULOMB, false>(a, st);
+        break;
+    case K_SINOVERR:
+        hermite ? eval_targets_t<K_SINOVERR, true>(a, st) : eval_targets_t<K_SINOVERR, false>(a, st);
+        break;
+    case K_REGYUKAWA: eval_targets_t<K_REGYUKAWA, false>(a, st); break;
+    case K_ATAN: eval_targets_t<K_ATAN, false>(a, st); break;
+    case K_MQ: eval_targets_t<K_MQ, false>(a, st); break;
+    case K_RBSU: eval_targets_t<K_RBSU, false>(a, st); break;
+    case K_RBSV: eval_targets_t<K_RBSV, false>(a, st); break;
+    default: eval_targets_t<K_USER, false>(a, st);
+    }
 }
 
 template <int KT, bool HERM>
@@ -995,15 +1015,25 @@ static void eval_grids_t(const EvalGridsArgs &a, cudaStream_t st)
     auto fn = k_eval_grids<KT, HERM>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     fn<<<a.nitems, EV_THREADS, sm, st>>>(a.n, a.items, a.t_grid, a.c_off, a.c_idx, a.p_off, a.p_idx, a.s_ibeg,
-                                         a.s_numpar, a.s_grid, a.Q, a.sx, a.sy, a.sz, a.sq, a.kp, a.Phi);
+                                         a.s_numpar, a.s_grid, a.Q, a.sx, a.sy, a.sz, a.sq, a.kp, a.kp2, a.Phi);
 }
 
+// Grid outputs (CP, CC) exist for all but the periodic kernels (atan, MQ).
 void launch_eval_grids(int kernel, bool hermite, const EvalGridsArgs &a, cudaStream_t st)
 {
     if (a.nitems <= 0) return;
-    if (kernel == K_COULOMB) hermite ? eval_grids_t<K_COULOMB, true>(a, st) : eval_grids_t<K_COULOMB, false>(a, st);
-    else if (kernel == K_YUKAWA) hermite ? eval_grids_t<K_YUKAWA, true>(a, st) : eval_grids_t<K_YUKAWA, false>(a, st);
-    else hermite ? eval_grids_t<K_REGCOULOMB, true>(a, st) : eval_grids_t<K_REGCOULOMB, false>(a, st);
+    switch (kernel) {
+    case K_COULOMB: hermite ? eval_grids_t<K_COULOMB, true>(a, st) : eval_grids_t<K_COULOMB, false>(a, st); break;
+    case K_YUKAWA: hermite ? eval_grids_t<K_YUKAWA, true>(a, st) : eval_grids_t<K_YUKAWA, false>(a, st); break;
+    case K_REGCOULOMB:
+        hermite ? eval_grids_t<K_REGCOULOMB, true>(a, st) : eval_grids_t<K_REGCOULOMB, false>(a, st);
+        break;
+    case K_SINOVERR: hermite ? eval_grids_t<K_SINOVERR, true>(a, st) : eval_grids_t<K_SINOVERR, false>(a, st); break;
+    case K_REGYUKAWA: eval_grids_t<K_REGYUKAWA, false>(a, st); break;
+    case K_RBSU: eval_grids_t<K_RBSU, false>(a, st); break;
+    case K_RBSV: eval_grids_t<K_RBSV, false>(a, st); break;
+    default: eval_grids_t<K_USER, false>(a, st);
+    }
 }
 
 void launch_l2p(int n, bool hermite, int nitems, const int2 *items, const int *leaf_node, const int *parent,
@@ -1028,13 +1058,24 @@ void launch_l2p(int n, bool hermite, int nitems, const int2 *items, const int *l
 
 void launch_direct(int kernel, int nt, int ns, const double *tx, const double *ty, const double *tz,
                    const double *sx, const double *sy, const double *sz, const double *sq, double kp, double *out,
-                   cudaStream_t st)
+                   cudaStream_t st, double kp2)
 {
     if (nt <= 0) return;
     int grid = (nt + EV_THREADS - 1) / EV_THREADS;
-    if (kernel == K_COULOMB) k_direct<K_COULOMB><<<grid, EV_THREADS, 0, st>>>(nt, ns, tx, ty, tz, sx, sy, sz, sq, kp, out);
-    else if (kernel == K_YUKAWA) k_direct<K_YUKAWA><<<grid, EV_THREADS, 0, st>>>(nt, ns, tx, ty, tz, sx, sy, sz, sq, kp, out);
-    else k_direct<K_REGCOULOMB><<<grid, EV_THREADS, 0, st>>>(nt, ns, tx, ty, tz, sx, sy, sz, sq, kp, out);
+#define BT_DIRECT(K) k_direct<K><<<grid, EV_THREADS, 0, st>>>(nt, ns, tx, ty, tz, sx, sy, sz, sq, kp, kp2, out)
+    switch (kernel) {
+    case K_COULOMB: BT_DIRECT(K_COULOMB); break;
+    case K_YUKAWA: BT_DIRECT(K_YUKAWA); break;
+    case K_REGCOULOMB: BT_DIRECT(K_REGCOULOMB); break;
+    case K_REGYUKAWA: BT_DIRECT(K_REGYUKAWA); break;
+    case K_ATAN: BT_DIRECT(K_ATAN); break;
+    case K_SINOVERR: BT_DIRECT(K_SINOVERR); break;
+    case K_MQ: BT_DIRECT(K_MQ); break;
+    case K_RBSU: BT_DIRECT(K_RBSU); break;
+    case K_RBSV: BT_DIRECT(K_RBSV); break;
+    default: BT_DIRECT(K_USER);
+    }
+#undef BT_DIRECT
 }
 
 }  // namespace bt

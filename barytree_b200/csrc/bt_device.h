@@ -19,7 +19,7 @@ struct EvalTargetsArgs {
     const double *s_grid, *Q;
     const double *sx, *sy, *sz, *sq;
     const double *tx, *ty, *tz;
-    double kp;
+    double kp, kp2;                             // kernel_params[0], [1]
     double *pot;
 };
 
@@ -32,7 +32,7 @@ struct EvalGridsArgs {
     const int *s_ibeg, *s_numpar;
     const double *s_grid, *Q;
     const double *sx, *sy, *sz, *sq;
-    double kp;
+    double kp, kp2;                             // kernel_params[0], [1]
     double *Phi;
 };
 
@@ -67,6 +67,6 @@ void launch_gather(int n, const int *order, const double *src, double *dst, cuda
 float run_probe(int which, int sms, double *ops, void *scratch, cudaStream_t st);
 void launch_direct(int kernel, int nt, int ns, const double *tx, const double *ty, const double *tz,
                    const double *sx, const double *sy, const double *sz, const double *sq, double kp, double *out,
-                   cudaStream_t st);
+                   cudaStream_t st, double kp2 = 0.0);
 
 }  // namespace bt

@@ -49,7 +49,8 @@ typedef struct {
 typedef struct {
     int kernel, approx, sing, ctype, degree, P, maxs, maxt;
     double theta, size_check, kp, beta;
-    double kp2;             /* kernel_params[1] (regularized Coulomb with subtraction: epsilon) */
+    double kp2;             /* kernel_params[1] (epsilon of regularized kernels, delta of atan / MQ) */
+    int nkp;                /* number of kernel parameters given */
     int verbosity;
     int precision;          /* 0 = FP64, 1 = mixed (FP32 evaluations, FP64 reductions) */
 } bt_params;

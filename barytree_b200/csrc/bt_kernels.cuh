@@ -18,7 +18,11 @@
 
 namespace bt {
 
-enum KernelType { K_COULOMB = 1, K_YUKAWA = 2, K_REGCOULOMB = 3 };
+// The reference's KERNEL values (src/interface/BaryTreeInterface.h:7-22).
+enum KernelType {
+    K_COULOMB = 1, K_YUKAWA = 2, K_REGCOULOMB = 3, K_REGYUKAWA = 4, K_ATAN = 5,
+    K_SINOVERR = 8, K_MQ = 9, K_RBSU = 10, K_RBSV = 11, K_USER = 12
+};
 
 constexpr int MAXNP = 17;   // n+1 <= 17 (degree <= 16)
 
@@ -56,6 +60,50 @@ __device__ __forceinline__ double k_far(double r2, double q, double kp)
     }
 }
 
+// Any kernel at displacement d = target (or target grid point) - source (or
+// source grid point); PP applies the reference's skipping rule.  kp, kp2 =
+// kernel_params[0], [1]:
+//   regularized Yukawa  q exp(-kappa r) / sqrt(r^2 + eps^2)      (kappa, eps)
+//       src/kernels/regularized-yukawa/regularized-yukawa_{pp,pc,cp}.c
+//   sin-over-r          q sin(k r) / r, PP skips r <= DBL_MIN     (k)
+//       src/kernels/sin-over-r/sin-over-r_{pp,pc,cp}.c
+//   user kernel         q exp(-k r) / r, PP skips r <= DBL_MIN    (k)
+//       src/kernels/user_kernel/user_kernel_{pp,pc,cp}.c
+//   RBS u / v (2-D)     +-1/(2 pi) q dy|dx / (dx^2 + dy^2 + delta^2)   (delta)
+//       src/kernels/rbs-u/rbs-u_*.c, src/kernels/rbs-v/rbs-v_*.c
+//   atan, MQ (1-D periodic in z, period L, width delta)           (L, delta)
+//       src/kernels/atan/atan_{pp,pc}.c, src/kernels/mq/mq_{pp,pc}.c
+template <int KT, bool PP>
+__device__ __forceinline__ double k_any(double dx, double dy, double dz, double q, double kp, double kp2)
+{
+    constexpr double pi = 3.14159265358979323846;
+    if (KT == K_COULOMB || KT == K_YUKAWA || KT == K_REGCOULOMB) {
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        return PP ? k_pp<KT>(r2, q, kp) : k_far<KT>(r2, q, kp);
+    } else if (KT == K_REGYUKAWA) {
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        return q * exp(-kp * r) / sqrt(r * r + kp2 * kp2);
+    } else if (KT == K_SINOVERR || KT == K_USER) {
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        if (PP && !(r > DBL_MIN)) return 0.0;
+        return KT == K_SINOVERR ? q * sin(kp * r) / r : q * exp(-kp * r) / r;
+    } else if (KT == K_RBSU || KT == K_RBSV) {
+        const double r = dx * dx + dy * dy + kp * kp;
+        return KT == K_RBSU ? 1. / (2. * pi) * q * dy / r : -1. / (2. * pi) * q * dx / r;
+    } else {
+        double d = dz / kp;
+        if (d < -0.5) d += 1.0;
+        if (d > 0.5) d -= 1.0;
+        if (KT == K_ATAN) {
+            const double factor = sqrt(1. + 1.0 / (kp2 * kp2));
+            const double wadj = 1. / (1. - kp2 / sqrt(1. + kp2 * kp2));
+            return wadj * (q * (1.0 / pi * atan(factor * tan(pi * d)) - d));
+        }
+        const double dl2 = kp2 * kp2 / kp / kp;
+        return q * (.5 * d * sqrt(1 + 4 * dl2) / sqrt(d * d + dl2) - d);
+    }
+}
+
 // Hermite PC value at displacement d = target - grid point for the 8 moments
 // q0..q7 = (q, qx, qy, qz, qxy, qyz, qxz, qxyz).
 template <int KT>
@@ -70,6 +118,20 @@ __device__ __forceinline__ double k_pc_herm(double dx, double dy, double dz, con
             + r3inv * (1 + kp * r) * (q[P] * dx + q[2 * P] * dy + q[3 * P] * dz)
             + r5inv * (3 + 3 * kp * r + k2 * rr2) * (q[4 * P] * dx * dy + q[5 * P] * dy * dz + q[6 * P] * dx * dz)
             + r7inv * (15 + 15 * kp * r + 6 * k2 * rr2 + k3 * r3) * q[7 * P] * dx * dy * dz);
+    }
+    if (KT == K_SINOVERR) {
+        // src/kernels/sin-over-r/sin-over-r_pc.c:68-150
+        const double r = sqrt(r2);
+        if (!(r > DBL_MIN)) return 0.0;
+        const double rinv = 1 / r, r2inv = rinv * rinv, r3inv = rinv * r2inv, r4inv = r2inv * r2inv,
+                     r5inv = r3inv * r2inv, r6inv = r3inv * r3inv, r7inv = r4inv * r3inv;
+        const double k2 = kp * kp, k3 = k2 * kp, sinr = sin(kp * r), cosr = cos(kp * r);
+        return sinr * rinv * q[0]
+            + (sinr * r3inv - kp * cosr * r2inv) * (q[P] * dx + q[2 * P] * dy + q[3 * P] * dz)
+            + (sinr * (3 * r5inv - k2 * r3inv) - 3 * kp * cosr * r4inv)
+                * (q[4 * P] * dx * dy + q[5 * P] * dy * dz + q[6 * P] * dx * dz)
+            + (sinr * (15 * r7inv - 6 * k2 * r5inv) + cosr * (k3 * r4inv - 15 * kp * r6inv))
+                * q[7 * P] * dx * dy * dz;
     }
     if (KT == K_REGCOULOMB) r2 += kp * kp;
     double rinv = rsqrt(r2);
@@ -86,6 +148,19 @@ template <int KT>
 __device__ __forceinline__ void k_cp_herm(double dx, double dy, double dz, double q, double kp, double *o)
 {
     double r2 = dx * dx + dy * dy + dz * dz;
+    if (KT == K_SINOVERR) {
+        // src/kernels/sin-over-r/sin-over-r_cp.c:68-175
+        const double r = sqrt(r2);
+        const double rinv = 1 / r, r2inv = rinv * rinv, r3inv = rinv * r2inv, r4inv = r2inv * r2inv,
+                     r5inv = r3inv * r2inv, r6inv = r3inv * r3inv, r7inv = r4inv * r3inv;
+        const double k2 = kp * kp, k3 = k2 * kp, sinr = sin(kp * r) * q, cosr = cos(kp * r) * q;
+        const double d1 = sinr * r3inv - kp * cosr * r2inv;
+        const double d2 = sinr * (3 * r5inv - k2 * r3inv) - 3 * kp * cosr * r4inv;
+        const double d3 = sinr * (15 * r7inv - 6 * k2 * r5inv) + cosr * (k3 * r4inv - 15 * kp * r6inv);
+        o[0] += sinr * rinv; o[1] += d1 * dx; o[2] += d1 * dy; o[3] += d1 * dz;
+        o[4] += d2 * dx * dy; o[5] += d2 * dy * dz; o[6] += d2 * dx * dz; o[7] += d3 * dx * dy * dz;
+        return;
+    }
     if (KT == K_REGCOULOMB) r2 += kp * kp;
     if (KT == K_YUKAWA) {
         double r = sqrt(r2), r3 = r2 * r, r2inv = 1.0 / r2;

@@ -11,6 +11,9 @@
 //   regularized Coulomb (alpha, eps = kernel_params[0..1]):
 //       K = 1/sqrt(r^2+eps^2), g = exp(-r^2/alpha^2), c = 2 pi alpha^2
 //       (src/kernels/regularized-coulomb/regularized-coulomb_ss_*.c)
+//   regularized Yukawa (kappa, eps): K = exp(-kappa r)/sqrt(r^2+eps^2),
+//       g = 1, c = 4 pi / kappa^2, particle-cluster Lagrange only
+//       (src/kernels/regularized-yukawa/regularized-yukawa_ss_*.c)
 // Source clusters carry two proxy arrays: Q from q*w and W from w (the same
 // upward pass applied to both, src/clusters/clusters.c:162-200).  PC uses
 // (Q_k - tq W_k g) K; target grids carry two fields, Phi_q from q*w (or Q)
@@ -46,6 +49,10 @@ __device__ __forceinline__ double ss_pp(double dx, double dy, double dz, double 
     } else if (KT == K_YUKAWA) {
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         return r > DBL_MIN ? (q - tq) * w * exp(-kp * r) / r : 0.0;
+    } else if (KT == K_REGYUKAWA) {
+        // regularized-yukawa_ss_pp.c: never skips
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        return (q - tq) * w * exp(-kp * r) / sqrt(r * r + kp2 * kp2);
     } else {
         const double r2 = dx * dx + dy * dy + dz * dz;
         return (q - tq * exp(-r2 / (kp * kp))) * w / sqrt(r2 + kp2 * kp2);
@@ -63,6 +70,9 @@ __device__ __forceinline__ double ss_pc(double dx, double dy, double dz, double 
     } else if (KT == K_YUKAWA) {
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         return (Qk - tq * Wk) * exp(-kp * r) / r;
+    } else if (KT == K_REGYUKAWA) {
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        return (Qk - tq * Wk) * exp(-kp * r) / sqrt(r * r + kp2 * kp2);
     } else {
         const double r2 = dx * dx + dy * dy + dz * dz;
         return (Qk - tq * Wk * exp(-r2 / (kp * kp))) / sqrt(r2 + kp2 * kp2);
@@ -253,6 +263,7 @@ void launch_ss_targets(int kernel, bool hermite, const SsTargetsArgs &a, cudaStr
     if (a.nitems <= 0) return;
     if (kernel == K_COULOMB) hermite ? ss_targets_t<K_COULOMB, true>(a, st) : ss_targets_t<K_COULOMB, false>(a, st);
     else if (kernel == K_YUKAWA) hermite ? ss_targets_t<K_YUKAWA, true>(a, st) : ss_targets_t<K_YUKAWA, false>(a, st);
+    else if (kernel == K_REGYUKAWA) ss_targets_t<K_REGYUKAWA, false>(a, st);
     else hermite ? ss_targets_t<K_REGCOULOMB, true>(a, st) : ss_targets_t<K_REGCOULOMB, false>(a, st);
 }
 
@@ -276,7 +287,7 @@ void launch_ss_correction(int n, double c, const double *tq, double *pot, cudaSt
 double ss_correction_constant(int kernel, double kp)
 {
     const double pi = 3.14159265358979323846;
-    if (kernel == K_YUKAWA) return 4.0 * pi / kp / kp;
+    if (kernel == K_YUKAWA || kernel == K_REGYUKAWA) return 4.0 * pi / kp / kp;
     return 2.0 * pi * kp * kp;
 }
 

@@ -31,6 +31,7 @@ void bt_params_setup(bt_params *o, int kernel, int nkp, const double *kp, int si
     o->kernel = kernel; o->sing = sing; o->approx = approx; o->ctype = ctype;
     o->kp = (nkp > 0 && kp) ? kp[0] : 0.0;
     o->kp2 = (nkp > 1 && kp) ? kp[1] : 0.0;
+    o->nkp = kp ? nkp : 0;
     o->verbosity = verbosity;
     if (beta < 0 || beta > 1) {
         o->beta = -1;

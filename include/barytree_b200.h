@@ -213,6 +213,15 @@ int bt_direct(int numTargets, int numSources,
               const double *sourceValue, double *outputArray,
               int kernel, double kernelParam, int device);
 
+/* bt_direct with the kernel parameters as an array (two for regularized
+ * Yukawa, atan and MQ), like BaryTreeInterface's numKernelParams /
+ * kernelParams; covers every kernel this library provides. */
+int bt_direct_ex(int numTargets, int numSources,
+                 const double *targetX, const double *targetY, const double *targetZ,
+                 const double *sourceX, const double *sourceY, const double *sourceZ,
+                 const double *sourceValue, double *outputArray, int kernel,
+                 int numKernelParams, const double *kernelParams, int device);
+
 /* Interaction lists as the product builds them, in the canonical triple form
  * (unit, kind, node): kind 0 = PP, 1 = approx (PC / CP / CC), 2 = PC (CC
  * mode), 3 = CP (CC mode).  Mirrors InteractionLists_Make

@@ -121,7 +121,7 @@ def _bti(**over):
     p = lambda a: None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
     rc = B.lib().BaryTreeInterface_ex(args["nt"], args["ns"], p(args["tx"]), p(args["ty"]), p(args["tz"]),
                                       p(args["tq"]), p(args["sx"]), p(args["sy"]), p(args["sz"]), p(args["sq"]),
-                                      p(args["sw"]), p(out), args["kernel"], 1, p(args["kp"]), args["sing"],
+                                      p(args["sw"]), p(out), args["kernel"], len(args["kp"]), p(args["kp"]), args["sing"],
                                       args["approx"], args["ctype"], args["theta"], args["deg"], args["ls"],
                                       args["lt"], args["sc"], args["beta"], 0)
     return rc, out
@@ -138,7 +138,10 @@ def test_error_codes_without_exiting():
     assert _bti(sing=2, tq=w, sw=w, ctype=2, approx=2)[0] == B.BT_ERR_UNSUPPORTED
     assert _bti(sing=2, tq=w, sw=w, ctype=3, kernel=3)[0] == B.BT_ERR_UNSUPPORTED
     assert _bti(sing=3)[0] == B.BT_ERR_PARAM
-    assert _bti(kernel=5)[0] == B.BT_ERR_UNSUPPORTED            # ATAN
+    assert _bti(kernel=6)[0] == B.BT_ERR_UNSUPPORTED            # TCF: no kernel in the reference
+    assert _bti(kernel=5, ctype=2, kp=np.array([1.0, 0.1]))[0] == B.BT_ERR_UNSUPPORTED   # atan is PC only
+    assert _bti(kernel=4, approx=2, kp=np.array([0.5, 0.1]))[0] == B.BT_ERR_UNSUPPORTED  # no Hermite reg. Yukawa
+    assert _bti(kernel=4)[0] == B.BT_ERR_PARAM                  # regularized Yukawa needs (kappa, eps)
     assert _bti(ctype=3, approx=2)[0] == B.BT_ERR_UNSUPPORTED   # CC Hermite (interaction_compute_cc.c:146)
     assert _bti(approx=0)[0] == B.BT_ERR_PARAM
     assert _bti(ctype=0)[0] == B.BT_ERR_PARAM
