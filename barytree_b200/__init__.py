@@ -114,7 +114,9 @@ _BTI_ARGS = (
 EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
                     "bt_tree_dump", "bt_tree_dump_ex", "bt_eval_batch", "bt_direct_ex", "bt_session_create", "bt_session_eval", "bt_session_destroy", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
                     "bt_selector_nweights", "bt_selector_set", "bt_selector_training_data", "bt_selector_train",
-                    "bt_mlp_loss_grad", "bt_mlp_predict")
+                    "bt_mlp_loss_grad", "bt_mlp_predict", "bt_eval_ex", "bt_direct_full", "bt_eval_noalloc",
+                    "treedriver", "directdriver", "RunParams_Setup", "RunParams_Validate", "RunParams_Free",
+                    "RunParams_Print")
 
 _lib = None
 
@@ -153,6 +155,14 @@ def lib():
     L.bt_direct_ex.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
                                ctypes.c_int, _dp, ctypes.c_int)
     L.bt_direct_ex.restype = ctypes.c_int
+    L.bt_direct_full.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                 ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int)
+    L.bt_direct_full.restype = ctypes.c_int
+    L.bt_eval_ex.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                             ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                             ctypes.c_double, ctypes.POINTER(Options), ctypes.POINTER(Report))
+    L.bt_eval_ex.restype = ctypes.c_int
     L.bt_session_create.argtypes = (ctypes.c_int, _llp, _llp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(Options),
@@ -250,16 +260,23 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
              approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER,
              theta=0.7, degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
              precision=PRECISION_FP64, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0,
-             tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, return_report=False):
-    """Extended entry point (bt_eval): options for precision / degree policy / tree build and a report."""
+             tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, return_report=False,
+             singularity=Singularity.SKIPPING, target_q=None, source_w=None, beta=-1.0):
+    """Extended entry point (bt_eval_ex): options for precision / degree policy /
+    tree build and a report.  kernel_param may be a sequence (two parameters
+    for regularized Coulomb/Yukawa, atan, MQ); singularity subtraction takes
+    the target charges and source weights."""
     tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
+    tq = _c(target_q) if target_q is not None else None
+    sw = _c(source_w) if source_w is not None else None
+    kp = _c(np.atleast_1d(np.asarray(kernel_param, dtype=np.float64)))
     out = np.zeros(len(tx))
     opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, int(tree_build), int(dispatch))
     rep = Report()
-    rc = lib().bt_eval(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
-                       int(kernel), float(kernel_param), int(approximation), int(compute_type), float(theta),
-                       int(degree), int(max_source_leaf), int(max_target_leaf), float(size_check),
-                       ctypes.byref(opts), ctypes.byref(rep))
+    rc = lib().bt_eval_ex(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(tq), _p(sx), _p(sy), _p(sz), _p(sq), _p(sw),
+                          _p(out), int(kernel), len(kp), _p(kp), int(singularity), int(approximation),
+                          int(compute_type), float(theta), int(degree), int(max_source_leaf), int(max_target_leaf),
+                          float(size_check), float(beta), ctypes.byref(opts), ctypes.byref(rep))
     _check(rc)
     return (out, rep.as_dict()) if return_report else out
 
@@ -375,14 +392,18 @@ def measure_peaks(device=0):
     return a.value, b.value, c.value
 
 
-def direct(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0, device=0):
+def direct(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0, device=0,
+           singularity=Singularity.SKIPPING, target_q=None, source_w=None):
     """FP64 direct sum on the GPU (error reference); kernel_param may be a
-    sequence of kernel parameters (two for regularized Yukawa, atan, MQ)."""
+    sequence of kernel parameters (two for regularized Yukawa, atan, MQ).
+    With singularity subtraction, target_q and source_w are required."""
     tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
+    tq = _c(target_q) if target_q is not None else None
+    sw = _c(source_w) if source_w is not None else None
     out = np.zeros(len(tx))
     kp = _c(np.atleast_1d(np.asarray(kernel_param, dtype=np.float64)))
-    rc = lib().bt_direct_ex(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq), _p(out),
-                            int(kernel), len(kp), _p(kp), int(device))
+    rc = lib().bt_direct_full(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(tq), _p(sx), _p(sy), _p(sz), _p(sq),
+                              _p(sw), _p(out), int(kernel), len(kp), _p(kp), int(singularity), int(device))
     _check(rc)
     return out
 

@@ -1571,6 +1571,20 @@ int bt_eval(int numTargets, int numSources, const double *targetX, const double 
                        outputArray, prm, opts, report);
 }
 
+int bt_eval_ex(int numTargets, int numSources, const double *targetX, const double *targetY, const double *targetZ,
+               const double *targetValue, const double *sourceX, const double *sourceY, const double *sourceZ,
+               const double *sourceValue, const double *sourceWeight, double *outputArray, int kernel,
+               int numKernelParams, const double *kernelParams, int singularity, int approximation,
+               int compute_type, double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+               double sizeCheck, double beta, const bt_options *opts, bt_report *report)
+{
+    bt_params prm;
+    bt_params_setup(&prm, kernel, numKernelParams, kernelParams, singularity, approximation, compute_type, theta,
+                    interpOrder, maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, beta, 0);
+    return eval_common(Systems(numTargets, numSources), targetX, targetY, targetZ, sourceX, sourceY, sourceZ, sourceValue,
+                       outputArray, prm, opts, report, false, targetValue, sourceWeight);
+}
+
 int bt_eval_noalloc(int numTargets, int numSources, const double *targetX, const double *targetY,
                     const double *targetZ, const double *sourceX, const double *sourceY, const double *sourceZ,
                     const double *sourceValue, double *outputArray, int kernel, double kernelParam,
@@ -1629,8 +1643,18 @@ int bt_direct_ex(int numTargets, int numSources, const double *targetX, const do
                  const double *sourceX, const double *sourceY, const double *sourceZ, const double *sourceValue,
                  double *outputArray, int kernel, int numKernelParams, const double *kernelParams, int device)
 {
+    return bt_direct_full(numTargets, numSources, targetX, targetY, targetZ, nullptr, sourceX, sourceY, sourceZ,
+                          sourceValue, nullptr, outputArray, kernel, numKernelParams, kernelParams, SKIPPING, device);
+}
+
+int bt_direct_full(int numTargets, int numSources, const double *targetX, const double *targetY,
+                   const double *targetZ, const double *targetValue, const double *sourceX, const double *sourceY,
+                   const double *sourceZ, const double *sourceValue, const double *sourceWeight, double *outputArray,
+                   int kernel, int numKernelParams, const double *kernelParams, int singularity, int device)
+{
     g_err[0] = 0;
     if (numTargets < 0 || numSources < 0) { set_err("negative count"); return BT_ERR_PARAM; }
+    if (singularity != SKIPPING && singularity != SUBTRACTION) { set_err("invalid singularity"); return BT_ERR_PARAM; }
     if (numTargets == 0) return BT_OK;
     if (!targetX || !targetY || !targetZ || !outputArray || (numSources > 0 && (!sourceX || !sourceY || !sourceZ || !sourceValue))) {
         set_err("NULL array");
@@ -1641,6 +1665,18 @@ int bt_direct_ex(int numTargets, int numSources, const double *targetX, const do
         set_err("kernel not provided");
         return BT_ERR_UNSUPPORTED;
     }
+    // The direct sum subtracts only for the kernels that have a subtraction
+    // pair term; the others ignore the setting, as the reference's direct
+    // driver does (interaction_compute_direct.c:26-231, interaction_compute_correction.c:22-45).
+    const bool ss = singularity == SUBTRACTION && bt::ss_direct_kernel(kernel);
+    if (ss && (!targetValue || (numSources > 0 && !sourceWeight))) {
+        set_err("singularity subtraction needs target charges and source weights");
+        return BT_ERR_PARAM;
+    }
+    if (ss && numKernelParams < (kernel == REGULARIZED_COULOMB || kernel == REGULARIZED_YUKAWA ? 2 : 1)) {
+        set_err("kernel needs more parameters");
+        return BT_ERR_PARAM;
+    }
     const double kernelParam = numKernelParams > 0 && kernelParams ? kernelParams[0] : 0.0;
     const double kernelParam2 = numKernelParams > 1 && kernelParams ? kernelParams[1] : 0.0;
     DeviceCtx *ctx = nullptr;
@@ -1648,22 +1684,30 @@ int bt_direct_ex(int numTargets, int numSources, const double *targetX, const do
     if (rc != BT_OK) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t st = ctx->stream;
-    double *d_t[3], *d_s[4], *d_o;
+    double *d_t[4], *d_s[5], *d_o;
     {
         Layout L;
-        for (int i = 0; i < 3; i++) L.add(&d_t[i], numTargets);
-        for (int i = 0; i < 4; i++) L.add(&d_s[i], numSources);
+        for (int i = 0; i < 4; i++) L.add(&d_t[i], numTargets);
+        for (int i = 0; i < 5; i++) L.add(&d_s[i], numSources);
         L.add(&d_o, numTargets);
         if (!ctx->arena.reserve(L.total())) { set_err("device allocation failed"); return BT_ERR_CUDA; }
         L.bind(ctx->arena);
-        const double *ht[3] = {targetX, targetY, targetZ};
-        const double *hs[4] = {sourceX, sourceY, sourceZ, sourceValue};
-        for (int i = 0; i < 3; i++) CK(cudaMemcpyAsync(d_t[i], ht[i], sizeof(double) * numTargets, cudaMemcpyHostToDevice, st));
+        const int ntc = ss ? 4 : 3, nsc = ss ? 5 : 4;
+        const double *ht[4] = {targetX, targetY, targetZ, targetValue};
+        const double *hs[5] = {sourceX, sourceY, sourceZ, sourceValue, sourceWeight};
+        for (int i = 0; i < ntc; i++) CK(cudaMemcpyAsync(d_t[i], ht[i], sizeof(double) * numTargets, cudaMemcpyHostToDevice, st));
         if (numSources > 0)
-            for (int i = 0; i < 4; i++) CK(cudaMemcpyAsync(d_s[i], hs[i], sizeof(double) * numSources, cudaMemcpyHostToDevice, st));
-        bt::launch_direct(kernel, numTargets, numSources, d_t[0], d_t[1], d_t[2], d_s[0], d_s[1], d_s[2], d_s[3],
-                          kernelParam, d_o, st, kernelParam2);
-        g_launches += 1;
+            for (int i = 0; i < nsc; i++) CK(cudaMemcpyAsync(d_s[i], hs[i], sizeof(double) * numSources, cudaMemcpyHostToDevice, st));
+        if (ss) {
+            bt::launch_ss_direct(kernel, numTargets, numSources, d_t[0], d_t[1], d_t[2], d_t[3], d_s[0], d_s[1], d_s[2],
+                                 d_s[3], d_s[4], kernelParam, kernelParam2, d_o, st);
+            bt::launch_ss_correction(numTargets, bt::ss_correction_constant(kernel, kernelParam), d_t[3], d_o, st);
+            g_launches += 2;
+        } else {
+            bt::launch_direct(kernel, numTargets, numSources, d_t[0], d_t[1], d_t[2], d_s[0], d_s[1], d_s[2], d_s[3],
+                              kernelParam, d_o, st, kernelParam2);
+            g_launches += 1;
+        }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(outputArray, d_o, sizeof(double) * numTargets, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

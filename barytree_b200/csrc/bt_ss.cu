@@ -248,6 +248,36 @@ __global__ void k_axpy(int n, double c, const double *__restrict__ x, double *__
     if (i < n) y[i] += c * x[i];
 }
 
+// SS direct sum over all sources (InteractionCompute_Direct with
+// singularity subtraction, src/interaction_compute/interaction_compute_direct.c:26-231):
+// one target per thread, sources staged through shared memory.
+template <int KT>
+__global__ void __launch_bounds__(SS_THREADS)
+k_ss_direct(int nt, int ns, const double *__restrict__ tx, const double *__restrict__ ty,
+            const double *__restrict__ tz, const double *__restrict__ tq, const double *__restrict__ sx,
+            const double *__restrict__ sy, const double *__restrict__ sz, const double *__restrict__ sq,
+            const double *__restrict__ sw, double kp, double kp2, double *__restrict__ out)
+{
+    __shared__ double s_x[SS_TILE], s_y[SS_TILE], s_z[SS_TILE], s_q[SS_TILE], s_w[SS_TILE];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = t < nt;
+    const double x = active ? tx[t] : 0.0, y = active ? ty[t] : 0.0, z = active ? tz[t] : 0.0;
+    const double q = active ? tq[t] : 0.0;
+    double acc = 0.0;
+    for (int c0 = 0; c0 < ns; c0 += SS_TILE) {
+        const int cm = min(SS_TILE, ns - c0);
+        for (int i = threadIdx.x; i < cm; i += blockDim.x) {
+            s_x[i] = sx[c0 + i]; s_y[i] = sy[c0 + i]; s_z[i] = sz[c0 + i];
+            s_q[i] = sq[c0 + i]; s_w[i] = sw[c0 + i];
+        }
+        __syncthreads();
+        for (int i = 0; i < cm; i++)
+            acc += ss_pp<KT>(x - s_x[i], y - s_y[i], z - s_z[i], s_q[i], s_w[i], q, kp, kp2);
+        __syncthreads();
+    }
+    if (active) out[t] = acc;
+}
+
 template <int KT, bool HERM>
 void ss_targets_t(const SsTargetsArgs &a, cudaStream_t st)
 {
@@ -272,6 +302,25 @@ void launch_ss_grids(int kernel, const SsGridsArgs &a, cudaStream_t st)
     if (a.nitems <= 0) return;
     if (kernel == K_COULOMB) k_ss_grids<K_COULOMB><<<a.nitems, SS_THREADS, 0, st>>>(a);
     else k_ss_grids<K_YUKAWA><<<a.nitems, SS_THREADS, 0, st>>>(a);
+}
+
+bool ss_direct_kernel(int kernel)
+{
+    return kernel == K_COULOMB || kernel == K_YUKAWA || kernel == K_REGCOULOMB || kernel == K_REGYUKAWA;
+}
+
+void launch_ss_direct(int kernel, int nt, int ns, const double *tx, const double *ty, const double *tz,
+                      const double *tq, const double *sx, const double *sy, const double *sz, const double *sq,
+                      const double *sw, double kp, double kp2, double *out, cudaStream_t st)
+{
+    if (nt <= 0) return;
+    const int grid = (nt + SS_THREADS - 1) / SS_THREADS;
+#define BT_SSD(K) k_ss_direct<K><<<grid, SS_THREADS, 0, st>>>(nt, ns, tx, ty, tz, tq, sx, sy, sz, sq, sw, kp, kp2, out)
+    if (kernel == K_COULOMB) BT_SSD(K_COULOMB);
+    else if (kernel == K_YUKAWA) BT_SSD(K_YUKAWA);
+    else if (kernel == K_REGYUKAWA) BT_SSD(K_REGYUKAWA);
+    else BT_SSD(K_REGCOULOMB);
+#undef BT_SSD
 }
 
 void launch_mul(int n, const double *a, const double *b, double *c, cudaStream_t st)

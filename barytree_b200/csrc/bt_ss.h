@@ -36,6 +36,13 @@ struct SsGridsArgs {
 int ss_chunk();                                 // targets per work item of launch_ss_targets
 void launch_ss_targets(int kernel, bool hermite, const SsTargetsArgs &a, cudaStream_t st);
 void launch_ss_grids(int kernel, const SsGridsArgs &a, cudaStream_t st);
+// Kernels with a singularity-subtraction direct sum (Coulomb, Yukawa and
+// their regularized forms); the others ignore the singularity setting.
+bool ss_direct_kernel(int kernel);
+// out[t] = sum_j of the SS pair term over all sources (no correction term)
+void launch_ss_direct(int kernel, int nt, int ns, const double *tx, const double *ty, const double *tz,
+                      const double *tq, const double *sx, const double *sy, const double *sz, const double *sq,
+                      const double *sw, double kp, double kp2, double *out, cudaStream_t st);
 void launch_mul(int n, const double *a, const double *b, double *c, cudaStream_t st);
 // pot[i] += c tq[i]
 void launch_ss_correction(int n, double c, const double *tq, double *pot, cudaStream_t st);

@@ -127,6 +127,20 @@ int bt_eval(int numTargets, int numSources,
             double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
             double sizeCheck, const bt_options *opts, bt_report *report);
 
+/* BaryTreeInterface_ex with options and a report: every argument of the
+ * reference entry point (target charges and source weights for singularity
+ * subtraction, all kernel parameters, beta) plus the extended options.
+ * opts and report may be NULL (FP64, defaults). */
+int bt_eval_ex(int numTargets, int numSources,
+               const double *targetX, const double *targetY, const double *targetZ,
+               const double *targetValue,
+               const double *sourceX, const double *sourceY, const double *sourceZ,
+               const double *sourceValue, const double *sourceWeight, double *outputArray,
+               int kernel, int numKernelParams, const double *kernelParams,
+               int singularity, int approximation, int compute_type,
+               double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
+               double sizeCheck, double beta, const bt_options *opts, bt_report *report);
+
 /* Batched evaluation of independent systems (no counterpart in the
  * reference, which evaluates one system per call).  System k's targets are
  * entries [targetOffsets[k], targetOffsets[k+1]) of the target arrays and of
@@ -221,6 +235,21 @@ int bt_direct_ex(int numTargets, int numSources,
                  const double *sourceX, const double *sourceY, const double *sourceZ,
                  const double *sourceValue, double *outputArray, int kernel,
                  int numKernelParams, const double *kernelParams, int device);
+
+/* FP64 direct sum with every argument of the reference's direct driver
+ * (src/drivers/directdriver.c:23-122, interaction_compute_direct.c:26-231):
+ * with singularity == SUBTRACTION, Coulomb, Yukawa and their regularized
+ * forms use the subtraction pair term and add the correction constant times
+ * the target charge (interaction_compute_correction.c:22-45); targetValue
+ * and sourceWeight are then required.  Other kernels ignore the setting, as
+ * in the reference.  outputArray is overwritten. */
+int bt_direct_full(int numTargets, int numSources,
+                   const double *targetX, const double *targetY, const double *targetZ,
+                   const double *targetValue,
+                   const double *sourceX, const double *sourceY, const double *sourceZ,
+                   const double *sourceValue, const double *sourceWeight, double *outputArray,
+                   int kernel, int numKernelParams, const double *kernelParams,
+                   int singularity, int device);
 
 /* Interaction lists as the product builds them, in the canonical triple form
  * (unit, kind, node): kind 0 = PP, 1 = approx (PC / CP / CC), 2 = PC (CC

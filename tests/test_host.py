@@ -19,7 +19,8 @@ from oracle import oracle as O
 
 
 def _header_functions():
-    src = open(os.path.join(ROOT, "include", "barytree_b200.h")).read()
+    inc = os.path.join(ROOT, "include")
+    src = "\n".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ \*]*?\b([A-Za-z_][A-Za-z0-9_]*)\s*\(",
                                  src, flags=re.M)))
@@ -27,7 +28,7 @@ def _header_functions():
 
 def test_library_exports_every_declared_symbol():
     names = _header_functions()
-    assert "BaryTreeInterface" in names and "bt_eval" in names
+    assert "BaryTreeInterface" in names and "bt_eval" in names and "treedriver" in names
     lib = ctypes.CDLL(B.LIB_PATH)
     for n in names:
         assert hasattr(lib, n), n
