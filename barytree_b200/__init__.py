@@ -94,6 +94,15 @@ class Report(ctypes.Structure):
         return d
 
 
+class Tuning(ctypes.Structure):
+    """bt_tuning: tile shape of the mixed particle-output kernel."""
+    _fields_ = [("targets_per_thread", ctypes.c_int), ("source_tile", ctypes.c_int), ("dispatch", ctypes.c_int),
+                ("ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class BaryTreeError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"barytree_b200 error {code}: {msg}")
@@ -116,7 +125,7 @@ EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_
                     "bt_selector_nweights", "bt_selector_set", "bt_selector_training_data", "bt_selector_train",
                     "bt_mlp_loss_grad", "bt_mlp_predict", "bt_eval_ex", "bt_direct_full", "bt_eval_noalloc",
                     "treedriver", "directdriver", "RunParams_Setup", "RunParams_Validate", "RunParams_Free",
-                    "RunParams_Print")
+                    "RunParams_Print", "bt_autotune", "bt_tuning_set", "bt_tuning_get")
 
 _lib = None
 
@@ -163,6 +172,17 @@ def lib():
                              ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                              ctypes.c_double, ctypes.POINTER(Options), ctypes.POINTER(Report))
     L.bt_eval_ex.restype = ctypes.c_int
+    L.bt_autotune.argtypes = (ctypes.c_int, _llp, _llp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
+                              ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                              ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(Options),
+                              ctypes.POINTER(Tuning), ctypes.POINTER(Tuning), ctypes.c_int,
+                              ctypes.POINTER(ctypes.c_int))
+    L.bt_autotune.restype = ctypes.c_int
+    L.bt_tuning_set.argtypes = (ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tuning))
+    L.bt_tuning_set.restype = ctypes.c_int
+    L.bt_tuning_get.argtypes = (ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tuning),
+                                ctypes.POINTER(ctypes.c_int))
+    L.bt_tuning_get.restype = ctypes.c_int
     L.bt_session_create.argtypes = (ctypes.c_int, _llp, _llp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(Options),
@@ -365,6 +385,71 @@ class Session:
 
     def __del__(self):
         self.close()
+
+
+def autotune(systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
+             compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
+             max_target_leaf=2000, size_check=1.0, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0):
+    """bt_autotune: times the mixed particle-output kernel's 18 tile shapes on
+    this workload (a list of systems (tx, ty, tz, sx, sy, sz, sq), as for
+    Session) and installs the fastest for (device, kernel, approximation).
+    Returns (best, trials) as dicts."""
+    systems = [tuple(map(_c, s)) for s in systems]
+    toff = np.concatenate([[0], np.cumsum([len(s[0]) for s in systems])]).astype(np.int64)
+    soff = np.concatenate([[0], np.cumsum([len(s[3]) for s in systems])]).astype(np.int64)
+    cat = [_c(np.concatenate([s[i] for s in systems])) for i in range(7)]
+    opts = Options(PRECISION_MIXED, int(degree_policy), float(tolerance), int(device), 0, TREE_GPU, DISPATCH_AUTO)
+    best = Tuning()
+    trials = (Tuning * 32)()
+    nt = ctypes.c_int(0)
+    rc = lib().bt_autotune(len(systems), toff.ctypes.data_as(_llp), soff.ctypes.data_as(_llp),
+                           *(_p(a) for a in cat), int(kernel), float(kernel_param), int(approximation),
+                           int(compute_type), float(theta), int(degree), int(max_source_leaf), int(max_target_leaf),
+                           float(size_check), ctypes.byref(opts), ctypes.byref(best), trials, 32, ctypes.byref(nt))
+    _check(rc)
+    return best.as_dict(), [trials[i].as_dict() for i in range(nt.value)]
+
+
+def tuning_get(kernel=Kernel.COULOMB, approximation=Approximation.LAGRANGE, device=0):
+    """(shape dict, installed) for (device, kernel, approximation)."""
+    t = Tuning()
+    inst = ctypes.c_int(0)
+    _check(lib().bt_tuning_get(int(device), int(kernel), int(approximation), ctypes.byref(t), ctypes.byref(inst)))
+    return t.as_dict(), bool(inst.value)
+
+
+def tuning_set(shape, kernel=Kernel.COULOMB, approximation=Approximation.LAGRANGE, device=0):
+    """Install a shape dict (as returned by autotune), or None to remove it."""
+    if shape is None:
+        _check(lib().bt_tuning_set(int(device), int(kernel), int(approximation), None))
+        return
+    t = Tuning(int(shape["targets_per_thread"]), int(shape["source_tile"]), int(shape["dispatch"]),
+               float(shape.get("ms", 0.0)))
+    _check(lib().bt_tuning_set(int(device), int(kernel), int(approximation), ctypes.byref(t)))
+
+
+def save_tuning(path, device=0):
+    """Write every installed shape of a device to a JSON file."""
+    import json
+    out = []
+    for k in Kernel:
+        for a in (Approximation.LAGRANGE, Approximation.HERMITE):
+            shape, inst = tuning_get(k, a, device)
+            if inst:
+                out.append({"kernel": int(k), "approximation": int(a), **shape})
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    return len(out)
+
+
+def load_tuning(path, device=0):
+    """Install the shapes of a file written by save_tuning."""
+    import json
+    with open(path) as f:
+        entries = json.load(f)
+    for e in entries:
+        tuning_set(e, e["kernel"], e["approximation"], device)
+    return len(entries)
 
 
 def treecode_ptr(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, kernel=Kernel.COULOMB, kernel_param=0.0,

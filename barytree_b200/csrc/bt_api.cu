@@ -86,6 +86,37 @@ struct DeviceCtx {
 DeviceCtx g_ctx[16];
 std::mutex g_ctx_mu;
 
+// Tile shape and dispatch of the mixed particle-output kernel.
+struct EvalShape {
+    bool queue = false;
+    int tpt = 2, tile = 1024;
+};
+
+// Autotuned shapes per device, kernel and approximation (bt_autotune,
+// bt_tuning_set); process-wide.
+std::mutex g_tune_mu;
+bt_tuning g_tuned[16][16][3];
+bool g_has_tuned[16][16][3];
+
+bool tune_key_ok(int device, int kernel, int approx)
+{
+    return device >= 0 && device < 16 && kernel >= 0 && kernel < 16 && approx >= 0 && approx < 3;
+}
+
+EvalShape tuned_shape(int device, int kernel, int approx)
+{
+    EvalShape sh;
+    if (!tune_key_ok(device, kernel, approx)) return sh;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_has_tuned[device][kernel][approx]) {
+        const bt_tuning &t = g_tuned[device][kernel][approx];
+        sh.queue = t.dispatch == BT_DISPATCH_QUEUE;
+        sh.tpt = t.targets_per_thread;
+        sh.tile = t.source_tile;
+    }
+    return sh;
+}
+
 int get_ctx(int device, DeviceCtx **out)
 {
     int ndev = 0;
@@ -486,6 +517,7 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
 struct DevPlan {
     bool mixed = false, herm = false, need_src_clusters = false, need_tgt_grids = false;
     bool queue = false;     // mixed kernels on a device work queue
+    int tpt = 2, tile = 1024;   // tile shape of the mixed particle-output kernel
     int n = 0, P = 0, ns = 0, nt = 0, max_np1 = 0, kernel = 0;
     double kp = 0.0;
     int S_n = 0, S_nleaves = 0, S_max_depth = 0, T_n = 0, T_nleaves = 0, T_max_depth = 0;
@@ -510,6 +542,28 @@ struct DevPlan {
     int n_hchunks = 0, n_hred = 0;
 };
 
+// Arguments of the mixed particle-output kernel of a prepared plan.
+bt::MixedTargetsArgs mixed_targets_args(const DevPlan &v)
+{
+    bt::MixedTargetsArgs a;
+    memset(&a, 0, sizeof a);
+    const int n = v.n;
+    a.n = n; a.max_np1 = v.max_np1; a.nitems = v.n_ev_items; a.items = v.d_evitems; a.herm = v.herm;
+    a.queue = v.queue ? v.d_queue + 1 : nullptr;
+    a.tpt = v.tpt; a.tile = v.tile;
+    a.leaf_node = v.d_tleaves; a.t_ibeg = v.d_tibeg; a.t_numpar = v.d_tnum; a.t_ctr = v.d_tctr; a.tpos = v.d_tpos;
+    a.a_off = v.d_aoff; a.a_idx = v.d_aidx; a.a_deg = v.d_adeg;
+    a.s_grid[n] = v.d_sgrid; a.Q32[n] = v.d_Q32;
+    for (size_t i = 0; i < v.xdeg.size(); i++) { a.s_grid[v.xdeg[i]] = v.d_xgrid[i]; a.Q32[v.xdeg[i]] = v.d_xQ32[i]; }
+    a.d_off = v.d_mxdoff; a.d_idx = v.d_mxdidx; a.d_flag = v.d_mxdflag; a.s_ibeg = v.d_sibeg; a.s_numpar = v.d_snum;
+    a.s_ctr = v.d_sctr;
+    a.spos = v.d_spos; a.kc = bt::mixed_kernel_constant(v.kernel, v.kp); a.pot = v.d_pot;
+    a.t_rad = v.d_trad; a.s_rad = v.d_srad;
+    a.tx64 = v.d_tx; a.ty64 = v.d_ty; a.tz64 = v.d_tz; a.sx64 = v.d_sx; a.sy64 = v.d_sy; a.sz64 = v.d_sz; a.sq64 = v.d_sq;
+    a.kp = v.kp;
+    return a;
+}
+
 // The device sequence of one evaluation (stream-ordered, no host
 // synchronisation, so it can be captured into a CUDA graph): relative
 // positions, upward pass, grid-output and particle-output kernels, downward
@@ -525,7 +579,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     };
     int rc = BT_OK;
     const bool mixed = v.mixed, herm = v.herm, need_src_clusters = v.need_src_clusters, need_tgt_grids = v.need_tgt_grids;
-    const int n = v.n, P = v.P, ns = v.ns, nt = v.nt, max_np1 = v.max_np1;
+    const int n = v.n, P = v.P, ns = v.ns, nt = v.nt;
     const std::vector<int> &xdeg = v.xdeg;
     auto d_sx = v.d_sx;
     auto d_sy = v.d_sy;
@@ -542,8 +596,6 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     auto d_ww = v.d_ww;
     auto d_Q = v.d_Q;
     auto d_Phi = v.d_Phi;
-    auto d_srad = v.d_srad;
-    auto d_trad = v.d_trad;
     auto d_sctr = v.d_sctr;
     auto d_tctr = v.d_tctr;
     auto d_sibeg = v.d_sibeg;
@@ -565,13 +617,11 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     auto d_cpidx = v.d_cpidx;
     auto d_order = v.d_order;
     auto d_queue = v.d_queue;
-    auto d_mxdidx = v.d_mxdidx;
     auto d_mxcpidx = v.d_mxcpidx;
     auto d_aoff = v.d_aoff;
     auto d_doff = v.d_doff;
     auto d_ccoff = v.d_ccoff;
     auto d_cpoff = v.d_cpoff;
-    auto d_mxdoff = v.d_mxdoff;
     auto d_mxcpoff = v.d_mxcpoff;
     auto d_evitems = v.d_evitems;
     auto d_griditems = v.d_griditems;
@@ -579,8 +629,6 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     auto d_spos = v.d_spos;
     auto d_tpos = v.d_tpos;
     auto d_Q32 = v.d_Q32;
-    auto d_mxdflag = v.d_mxdflag;
-    auto d_adeg = v.d_adeg;
     auto &d_xgrid = v.d_xgrid;
     auto &d_xQ = v.d_xQ;
     auto &d_xQ32 = v.d_xQ32;
@@ -697,19 +745,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         bt::launch_ss_targets(v.kernel, herm, a, st);
         launches++;
     } else if (nt > 0 && mixed) {
-        bt::MixedTargetsArgs a;
-        memset(&a, 0, sizeof a);
-        a.n = n; a.max_np1 = max_np1; a.nitems = v.n_ev_items; a.items = d_evitems; a.herm = herm;
-        a.queue = v.queue ? d_queue + 1 : nullptr;
-        a.leaf_node = d_tleaves; a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.t_ctr = d_tctr; a.tpos = d_tpos;
-        a.a_off = d_aoff; a.a_idx = d_aidx; a.a_deg = d_adeg;
-        a.s_grid[n] = d_sgrid; a.Q32[n] = d_Q32;
-        for (size_t i = 0; i < xdeg.size(); i++) { a.s_grid[xdeg[i]] = d_xgrid[i]; a.Q32[xdeg[i]] = d_xQ32[i]; }
-        a.d_off = d_mxdoff; a.d_idx = d_mxdidx; a.d_flag = d_mxdflag; a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_ctr = d_sctr;
-        a.spos = d_spos; a.kc = bt::mixed_kernel_constant(v.kernel, v.kp); a.pot = d_pot;
-        a.t_rad = d_trad; a.s_rad = d_srad;
-        a.tx64 = d_tx; a.ty64 = d_ty; a.tz64 = d_tz; a.sx64 = d_sx; a.sy64 = d_sy; a.sz64 = d_sz; a.sq64 = d_sq;
-        a.kp = v.kp;
+        const bt::MixedTargetsArgs a = mixed_targets_args(v);
         bt::launch_eval_targets_mixed(v.kernel, a, st);
         launches++;
     } else if (nt > 0) {
@@ -771,7 +807,7 @@ done:
 // execute = false: prepare only (uploads done, the device sequence not
 // issued), for capture into a graph by the caller.
 int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on_device, bt_report *rep,
-             const DevParts *dp = nullptr, bool queue = false, DevPlan *dv_out = nullptr, bool execute = true,
+             const DevParts *dp = nullptr, const EvalShape &shape = EvalShape(), DevPlan *dv_out = nullptr, bool execute = true,
              const SsIn *ss = nullptr)
 {
     const bt_params &o = pl.prm;
@@ -1027,7 +1063,9 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         cudaEvent_t *ev = ctx->ev;
         DevPlan v;
         v.mixed = mixed; v.herm = herm; v.need_src_clusters = need_src_clusters; v.need_tgt_grids = need_tgt_grids;
-        v.queue = queue;
+        v.queue = shape.queue;
+        v.tpt = shape.tpt;
+        v.tile = shape.tile;
         v.n = n; v.P = P; v.ns = ns; v.nt = nt; v.max_np1 = max_np1; v.kernel = o.kernel; v.kp = o.kp;
         v.S_n = S.n; v.S_nleaves = S.nleaves; v.S_max_depth = S.max_depth;
         v.T_n = T.n; v.T_nleaves = T.nleaves; v.T_max_depth = T.max_depth;
@@ -1343,7 +1381,7 @@ int static_scratch_arena(int device, Arena **out)
 
 // Checks the options and applies them to prm: precision, learned degree
 // policy and its tolerance, dispatch of the mixed evaluation kernels.
-int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double &tol, bool &queue)
+int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double &tol, EvalShape &shape)
 {
     if (opts && opts->precision != BT_PRECISION_FP64 && opts->precision != BT_PRECISION_MIXED) {
         set_err("invalid precision %d", opts->precision);
@@ -1363,10 +1401,15 @@ int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double 
         set_err("invalid dispatch %d", opts->dispatch);
         return BT_ERR_PARAM;
     }
-    // AUTO: one block per work item.  Persistent blocks on a device counter
-    // measured 2.5 % slower for the 16M clustered system (cost-sorted items
-    // are already dispatched longest first by the block scheduler).
-    queue = opts && opts->dispatch == BT_DISPATCH_QUEUE;
+    // Tile shape and dispatch: the device's autotuned shape for this kernel
+    // and approximation (bt_autotune / bt_tuning_set), else the defaults.
+    // Default dispatch: one block per work item.  Persistent blocks on a
+    // device counter measured 2.5 % slower for the 16M clustered system
+    // (cost-sorted items are already dispatched longest first by the block
+    // scheduler).  An explicit dispatch option overrides the tuned one.
+    shape = tuned_shape(opts ? opts->device : 0, prm.kernel, prm.approx);
+    if (opts && opts->dispatch == BT_DISPATCH_QUEUE) shape.queue = true;
+    if (opts && opts->dispatch == BT_DISPATCH_GRID) shape.queue = false;
     if (learned && (prm.precision != BT_PRECISION_MIXED || prm.ctype != PARTICLE_CLUSTER || prm.approx != LAGRANGE ||
                     prm.kernel != COULOMB)) {
         set_err("learned degree selection is provided for mixed precision, particle-cluster, Lagrange, Coulomb");
@@ -1396,9 +1439,10 @@ int eval_common(const Systems &sys, const double *tx, const double *ty, const do
         return BT_OK;
     }
     int device = opts ? opts->device : 0;
-    bool learned = false, queue = false;
+    bool learned = false;
+    EvalShape shape;
     double tol = 1e-6;
-    rc = parse_options(opts, prm, learned, tol, queue);
+    rc = parse_options(opts, prm, learned, tol, shape);
     if (rc != BT_OK) return rc;
     if (prm.sing == SUBTRACTION) {
         // Particles_Validate (src/particles/particles.c:170-193): subtraction
@@ -1476,7 +1520,7 @@ int eval_common(const Systems &sys, const double *tx, const double *ty, const do
         }
     }
     SsIn ssin{tq, sw, on_dev};
-    rc = run_plan(ctx, *arena, pl, out, on_dev, rep, dpp, queue, nullptr, true, prm.sing == SUBTRACTION ? &ssin : nullptr);
+    rc = run_plan(ctx, *arena, pl, out, on_dev, rep, dpp, shape, nullptr, true, prm.sing == SUBTRACTION ? &ssin : nullptr);
     bt_plan_free(&pl);
     if (rc != BT_OK && !on_dev) memset(out, 0, sizeof(double) * (size_t)nt);
     return rc;
@@ -2132,9 +2176,10 @@ int bt_session_create(int numSystems, const long long *targetOffsets, const long
         set_err("sessions build their trees on the GPU");
         return BT_ERR_UNSUPPORTED;
     }
-    bool learned = false, queue = false;
+    bool learned = false;
+    EvalShape shape;
     double tol = 1e-6;
-    rc = parse_options(opts, prm, learned, tol, queue);
+    rc = parse_options(opts, prm, learned, tol, shape);
     if (rc != BT_OK) return rc;
     const int device = opts ? opts->device : 0;
     DeviceCtx *ctx = nullptr;
@@ -2163,7 +2208,7 @@ int bt_session_create(int numSystems, const long long *targetOffsets, const long
         }
     }
     if (rc == BT_OK)
-        rc = run_plan(ctx, S->arena, pl, nullptr, true, nullptr, &dp, queue, &S->v, false);
+        rc = run_plan(ctx, S->arena, pl, nullptr, true, nullptr, &dp, shape, &S->v, false);
     const int *sorder = dp.sorder;
     bt_plan_free(&pl);
     if (rc == BT_OK && cudaMalloc(&S->d_qin, sizeof(double) * (size_t)ns) != cudaSuccess) {
@@ -2251,6 +2296,154 @@ int bt_session_destroy(bt_session *session)
         session_free(S);
     }
     return BT_OK;
+}
+
+int bt_tuning_set(int device, int kernel, int approximation, const bt_tuning *t)
+{
+    g_err[0] = 0;
+    if (!tune_key_ok(device, kernel, approximation)) { set_err("invalid device, kernel or approximation"); return BT_ERR_PARAM; }
+    if (t && (!bt::mixed_shape_valid(t->targets_per_thread, t->source_tile) ||
+              (t->dispatch != BT_DISPATCH_GRID && t->dispatch != BT_DISPATCH_QUEUE))) {
+        set_err("invalid tile shape (%d targets per thread, %d-source tiles, dispatch %d)", t->targets_per_thread,
+                t->source_tile, t->dispatch);
+        return BT_ERR_PARAM;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_has_tuned[device][kernel][approximation] = t != nullptr;
+    if (t) g_tuned[device][kernel][approximation] = *t;
+    return BT_OK;
+}
+
+int bt_tuning_get(int device, int kernel, int approximation, bt_tuning *t, int *installed)
+{
+    g_err[0] = 0;
+    if (!t || !tune_key_ok(device, kernel, approximation)) { set_err("invalid arguments"); return BT_ERR_PARAM; }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const bool has = g_has_tuned[device][kernel][approximation];
+    if (has) {
+        *t = g_tuned[device][kernel][approximation];
+    } else {
+        const EvalShape d;
+        t->targets_per_thread = d.tpt; t->source_tile = d.tile;
+        t->dispatch = d.queue ? BT_DISPATCH_QUEUE : BT_DISPATCH_GRID; t->ms = 0.0f;
+    }
+    if (installed) *installed = has ? 1 : 0;
+    return BT_OK;
+}
+
+int bt_autotune(int numSystems, const long long *targetOffsets, const long long *sourceOffsets,
+                const double *targetX, const double *targetY, const double *targetZ, const double *sourceX,
+                const double *sourceY, const double *sourceZ, const double *sourceValue, int kernel,
+                double kernelParam, int approximation, int compute_type, double theta, int interpOrder,
+                int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck, const bt_options *opts,
+                bt_tuning *best, bt_tuning *trials, int maxTrials, int *numTrials)
+{
+    g_err[0] = 0;
+    if (numTrials) *numTrials = 0;
+    if (!best) { set_err("best is NULL"); return BT_ERR_PARAM; }
+    if (!opts || opts->precision != BT_PRECISION_MIXED) {
+        set_err("autotuning covers the mixed-precision particle-output kernel: set BT_PRECISION_MIXED");
+        return BT_ERR_UNSUPPORTED;
+    }
+    if (!tune_key_ok(opts->device, kernel, approximation)) { set_err("invalid device, kernel or approximation"); return BT_ERR_PARAM; }
+    // the problem as a session with the given dispatch (the shapes are set per trial below)
+    bt_options o = *opts;
+    o.dispatch = BT_DISPATCH_GRID;
+    bt_session *sess = nullptr;
+    int rc = bt_session_create(numSystems, targetOffsets, sourceOffsets, targetX, targetY, targetZ, sourceX, sourceY,
+                               sourceZ, sourceValue, kernel, kernelParam, approximation, compute_type, theta,
+                               interpOrder, maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, &o, &sess);
+    if (rc != BT_OK) return rc;
+    Session *S = reinterpret_cast<Session *>(sess);
+    // one full evaluation, so every array the kernel reads holds its values
+    double *scratch = nullptr;
+    std::vector<double> hscratch;
+    if (S->on_dev) {
+        if (cudaMalloc(&scratch, sizeof(double) * (size_t)S->nt) != cudaSuccess) {
+            cudaGetLastError();
+            bt_session_destroy(sess);
+            set_err("device allocation failed");
+            return BT_ERR_CUDA;
+        }
+    } else {
+        hscratch.resize((size_t)S->nt);
+        scratch = hscratch.data();
+    }
+    rc = bt_session_eval(sess, sourceValue, scratch, nullptr);
+    if (S->on_dev) cudaFree(scratch);
+    if (rc != BT_OK) { bt_session_destroy(sess); return rc; }
+    if (!S->v.mixed || S->v.n_ev_items <= 0 || S->v.ss) {
+        bt_session_destroy(sess);
+        set_err("this problem has no mixed particle-output work to tune");
+        return BT_ERR_UNSUPPORTED;
+    }
+    std::vector<bt_tuning> res;
+    {
+        std::lock_guard<std::mutex> lk(S->ctx->mu);
+        cudaSetDevice(S->device);
+        cudaStream_t st = S->ctx->stream;
+        // sample: every k-th work item of the cost-sorted list (stays sorted)
+        const int nit = S->v.n_ev_items;
+        const int want = std::max(8192, nit / 16);
+        const int k = std::max(1, nit / want);
+        std::vector<int2> items((size_t)nit);
+        int2 *d_items = nullptr;
+        int *d_counter = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        std::vector<int2> sample;
+        if (cudaMemcpy(items.data(), S->v.d_evitems, sizeof(int2) * (size_t)nit, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            rc = BT_ERR_CUDA;
+        } else {
+            for (int i = 0; i < nit; i += k) sample.push_back(items[(size_t)i]);
+            if (cudaMalloc(&d_items, sizeof(int2) * sample.size()) != cudaSuccess ||
+                cudaMalloc(&d_counter, sizeof(int)) != cudaSuccess ||
+                cudaMemcpy(d_items, sample.data(), sizeof(int2) * sample.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+                rc = BT_ERR_CUDA;
+        }
+        const int tpts[3] = {1, 2, 4}, tiles[3] = {512, 1024, 2048}, disp[2] = {BT_DISPATCH_GRID, BT_DISPATCH_QUEUE};
+        for (int di = 0; di < 2 && rc == BT_OK; di++)
+            for (int ti = 0; ti < 3 && rc == BT_OK; ti++)
+                for (int li = 0; li < 3 && rc == BT_OK; li++) {
+                    bt::MixedTargetsArgs a = mixed_targets_args(S->v);
+                    a.items = d_items;
+                    a.nitems = (int)sample.size();
+                    a.tpt = tpts[ti];
+                    a.tile = tiles[li];
+                    a.queue = disp[di] == BT_DISPATCH_QUEUE ? d_counter : nullptr;
+                    float bestms = 0.0f;
+                    for (int r = 0; r < 3; r++) {      // one warm-up launch, then the faster of two
+                        if (a.queue && cudaMemsetAsync(d_counter, 0, sizeof(int), st) != cudaSuccess) { rc = BT_ERR_CUDA; break; }
+                        cudaEventRecord(e0, st);
+                        bt::launch_eval_targets_mixed(S->v.kernel, a, st);
+                        cudaEventRecord(e1, st);
+                        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) { rc = BT_ERR_CUDA; break; }
+                        g_launches += 1;
+                        float ms = 0.0f;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        if (r == 1 || (r == 2 && ms < bestms)) bestms = ms;
+                    }
+                    bt_tuning t;
+                    t.targets_per_thread = tpts[ti]; t.source_tile = tiles[li]; t.dispatch = disp[di]; t.ms = bestms;
+                    res.push_back(t);
+                }
+        if (rc != BT_OK) set_err("CUDA error while timing the tile shapes: %s", cudaGetErrorString(cudaGetLastError()));
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (d_items) cudaFree(d_items);
+        if (d_counter) cudaFree(d_counter);
+        cudaGetLastError();
+    }
+    bt_session_destroy(sess);
+    if (rc != BT_OK) return rc;
+    size_t bi = 0;
+    for (size_t i = 1; i < res.size(); i++)
+        if (res[i].ms < res[bi].ms) bi = i;
+    *best = res[bi];
+    if (trials)
+        for (int i = 0; i < maxTrials && i < (int)res.size(); i++) trials[i] = res[(size_t)i];
+    if (numTrials) *numTrials = std::min((int)res.size(), trials ? maxTrials : (int)res.size());
+    return bt_tuning_set(opts->device, kernel, approximation, best);
 }
 
 }  // extern "C"

@@ -69,17 +69,15 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
     s = t;
 }
 
-constexpr int MX_THREADS = 128;
-// Register budget of the evaluation kernels: BT_MX_MIN_BLOCKS resident blocks
+constexpr int MX_THREADS = 128;                 // threads of the grid-output kernel
+// Register budget of the grid-output kernel: BT_MX_MIN_BLOCKS resident blocks
 // per SM (unset: the compiler's choice).
 #ifdef BT_MX_MIN_BLOCKS
 #define BT_MX_BOUNDS __launch_bounds__(MX_THREADS, BT_MX_MIN_BLOCKS)
 #else
 #define BT_MX_BOUNDS __launch_bounds__(MX_THREADS)
 #endif
-constexpr int MX_TPT = 2;                       // targets per thread
-constexpr int MX_CHUNK = MX_THREADS * MX_TPT;   // targets per work item
-constexpr int MX_TILE = 1024;
+constexpr int MX_TILE = 1024;                   // sources per tile of the grid-output kernel
 
 // Far field of one source cluster (degree NP1-1) for NT targets at (x,y,z),
 // relative to the target centre; g = grid coordinates relative to the same
@@ -300,16 +298,16 @@ __device__ __forceinline__ f2_t kf2_acc(f2_t r2, f2_t q, f2_t S, f2_t kc2)
     return f2_fma(q, f2_mul(f2_mul(rinv, t), e), S);
 }
 
-// One tile against the thread's MX_TPT targets (x, y, z in the source
+// One tile against the thread's TPT targets (x, y, z in the source
 // leaf's frame).  NEAR: also the smallest r2 per target (mn), which tells
 // whether the tile holds a close pair.
-template <int KT, bool NEAR>
+template <int KT, bool NEAR, int TPT>
 __device__ __forceinline__ void pp_tile(const Tile tl, int cm4, const float *x, const float *y, const float *z,
                                         float kc, float *s, float *mn)
 {
-    f2_t X[MX_TPT], Y[MX_TPT], Z[MX_TPT], S[MX_TPT];
+    f2_t X[TPT], Y[TPT], Z[TPT], S[TPT];
 #pragma unroll
-    for (int t = 0; t < MX_TPT; t++) {
+    for (int t = 0; t < TPT; t++) {
         X[t] = f2_make(x[t], x[t]);
         Y[t] = f2_make(y[t], y[t]);
         Z[t] = f2_make(z[t], z[t]);
@@ -326,7 +324,7 @@ __device__ __forceinline__ void pp_tile(const Tile tl, int cm4, const float *x, 
         for (int hh = 0; hh < 2; hh++) {
             const f2_t px = hh ? PX.y : PX.x, py = hh ? PY.y : PY.x, pz = hh ? PZ.y : PZ.x, pq = hh ? PQ.y : PQ.x;
 #pragma unroll
-            for (int t = 0; t < MX_TPT; t++) {
+            for (int t = 0; t < TPT; t++) {
                 const f2_t dx = f2_sub(X[t], px), dy = f2_sub(Y[t], py), dz = f2_sub(Z[t], pz);
                 const f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
                 if (NEAR) {
@@ -339,7 +337,7 @@ __device__ __forceinline__ void pp_tile(const Tile tl, int cm4, const float *x, 
         }
     }
 #pragma unroll
-    for (int t = 0; t < MX_TPT; t++) {
+    for (int t = 0; t < TPT; t++) {
         float a, b;
         f2_split(S[t], a, b);
         s[t] = a + b;
@@ -373,7 +371,7 @@ __device__ __noinline__ float pp_tile_close(const Tile tl, int cm, float x, floa
     return s;
 }
 
-// Particle-output evaluation, mixed precision.  Each thread owns MX_TPT
+// Particle-output evaluation, mixed precision.  Each thread owns TPT
 // targets of a work item (target leaf, chunk of MX_CHUNK targets).
 // Blocks of a work-queue launch take items (cost-sorted, longest first) from
 // a device counter until the queue is empty; without a queue, block b
@@ -387,18 +385,18 @@ __device__ __forceinline__ int next_item(int *queue, int *slot)
     return w;
 }
 
-template <int KT, bool HERM>
+template <int KT, bool HERM, int TPT>
 __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const int2 it, float *smf)
 {
     const int u = it.x;
     const int tnode = a.leaf_node[u];
     const int tb = a.t_ibeg[tnode], tn = a.t_numpar[tnode];
-    float x[MX_TPT], y[MX_TPT], z[MX_TPT];
-    bool act[MX_TPT];
-    int tid[MX_TPT];
+    float x[TPT], y[TPT], z[TPT];
+    bool act[TPT];
+    int tid[TPT];
 #pragma unroll
-    for (int t = 0; t < MX_TPT; t++) {
-        int ti = it.y * MX_CHUNK + t * MX_THREADS + threadIdx.x;
+    for (int t = 0; t < TPT; t++) {
+        int ti = it.y * MX_CHUNK + t * (MX_CHUNK / TPT) + threadIdx.x;
         act[t] = ti < tn;
         tid[t] = tb + (act[t] ? ti : 0);
         float4 tp = a.tpos[tid[t]];
@@ -407,9 +405,9 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
     const double trad = a.t_rad[tnode];
     const double cx = a.t_ctr[3 * tnode], cy = a.t_ctr[3 * tnode + 1], cz = a.t_ctr[3 * tnode + 2];
     const float kc = (float)a.kc;
-    double acc[MX_TPT];
+    double acc[TPT];
 #pragma unroll
-    for (int t = 0; t < MX_TPT; t++) acc[t] = 0.0;
+    for (int t = 0; t < TPT; t++) acc[t] = 0.0;
 
     // far field: source clusters
     for (int64_t e = a.a_off[u]; e < a.a_off[u + 1]; e++) {
@@ -424,7 +422,7 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
             double c = ax == 0 ? cx : ax == 1 ? cy : cz;
             g[ax * np1 + (i % np1)] = (float)(gs[i] - c);
         }
-        float v[MX_TPT];
+        float v[TPT];
         if (HERM) {
             const float *Qs = a.Q32[deg] + (size_t)s * 8 * P;
             for (int i = threadIdx.x; i < 8 * P; i += blockDim.x) {
@@ -432,78 +430,81 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
                 q[i] = Qs[i] * (m == 7 ? 15.0f : m >= 4 ? 3.0f : 1.0f);
             }
             __syncthreads();
-            pc_cluster_herm_dispatch<KT, MX_TPT>(np1, x, y, z, g, q, kc, (float)a.kp, v);
+            pc_cluster_herm_dispatch<KT, TPT>(np1, x, y, z, g, q, kc, (float)a.kp, v);
         } else {
             const float *Qs = a.Q32[deg] + (size_t)s * P;
             for (int i = threadIdx.x; i < P; i += blockDim.x) q[i] = Qs[i];
             __syncthreads();
-            pc_cluster_dispatch<KT, MX_TPT>(np1, x, y, z, g, q, kc, v);
+            pc_cluster_dispatch<KT, TPT>(np1, x, y, z, g, q, kc, v);
         }
 #pragma unroll
-        for (int t = 0; t < MX_TPT; t++) acc[t] += (double)v[t];
+        for (int t = 0; t < TPT; t++) acc[t] += (double)v[t];
         __syncthreads();
     }
     // near field: source leaves, particles relative to their leaf centre
-    const Tile tl{smf, smf + MX_TILE, smf + 2 * MX_TILE, smf + 3 * MX_TILE};
+    // fixed array strides (the tile length only bounds the loop): a runtime
+    // stride costs the Coulomb kernel 16 registers and a resident block
+    const int tile = a.tile;
+    const Tile tl{smf, smf + MX_TILE_MAX, smf + 2 * MX_TILE_MAX, smf + 3 * MX_TILE_MAX};
     for (int64_t e = a.d_off[u]; e < a.d_off[u + 1]; e++) {
         const int s = a.d_idx[e];
         const bool near = a.d_flag[e] != 0;
         const int sb = a.s_ibeg[s], sn = a.s_numpar[s];
         const float ox = (float)(a.s_ctr[3 * s] - cx), oy = (float)(a.s_ctr[3 * s + 1] - cy),
                     oz = (float)(a.s_ctr[3 * s + 2] - cz);
-        float xs[MX_TPT], ys[MX_TPT], zs[MX_TPT];   // targets in the source leaf's frame
+        float xs[TPT], ys[TPT], zs[TPT];   // targets in the source leaf's frame
 #pragma unroll
-        for (int t = 0; t < MX_TPT; t++) { xs[t] = x[t] - ox; ys[t] = y[t] - oy; zs[t] = z[t] - oz; }
+        for (int t = 0; t < TPT; t++) { xs[t] = x[t] - ox; ys[t] = y[t] - oy; zs[t] = z[t] - oz; }
         // at least the smallest normal float, so that a coincident pair (r2
         // == 0 after flushing) always takes the FP64 path with the skipping
         // rule, also between single-particle leaves of radius 0
         const double rr = MX_CLOSE_FRAC * (trad + a.s_rad[s]);
         const float thr2 = fmaxf((float)(rr * rr), FLT_MIN);
-        for (int c0 = 0; c0 < sn; c0 += MX_TILE) {
-            const int cm = min(MX_TILE, sn - c0), cm4 = (cm + 3) & ~3;
+        for (int c0 = 0; c0 < sn; c0 += tile) {
+            const int cm = min(tile, sn - c0), cm4 = (cm + 3) & ~3;
             for (int i = threadIdx.x; i < cm4; i += blockDim.x) {
                 const float4 p = i < cm ? a.spos[sb + c0 + i] : make_float4(MX_PAD_POS, MX_PAD_POS, MX_PAD_POS, 0.0f);
                 tl.x[i] = p.x; tl.y[i] = p.y; tl.z[i] = p.z; tl.q[i] = p.w;
             }
             __syncthreads();
-            float sum[MX_TPT], mn[MX_TPT];
+            float sum[TPT], mn[TPT];
             if (near) {
 #pragma unroll
-                for (int t = 0; t < MX_TPT; t++) mn[t] = FLT_MAX;
-                pp_tile<KT, true>(tl, cm4, xs, ys, zs, kc, sum, mn);
+                for (int t = 0; t < TPT; t++) mn[t] = FLT_MAX;
+                pp_tile<KT, true, TPT>(tl, cm4, xs, ys, zs, kc, sum, mn);
                 bool close = false;
 #pragma unroll
-                for (int t = 0; t < MX_TPT; t++) close |= act[t] && mn[t] < thr2;
+                for (int t = 0; t < TPT; t++) close |= act[t] && mn[t] < thr2;
                 if (__any_sync(0xffffffffu, close)) {
 #pragma unroll
-                    for (int t = 0; t < MX_TPT; t++)
+                    for (int t = 0; t < TPT; t++)
                         if (act[t] && mn[t] < thr2)
                             sum[t] = pp_tile_close<KT>(tl, cm, xs[t], ys[t], zs[t], kc, thr2, a.tx64[tid[t]],
                                                        a.ty64[tid[t]], a.tz64[tid[t]], a.sx64, a.sy64, a.sz64,
                                                        a.sq64, sb + c0, a.kp, &acc[t]);
                 }
             } else {
-                pp_tile<KT, false>(tl, cm4, xs, ys, zs, kc, sum, mn);
+                pp_tile<KT, false, TPT>(tl, cm4, xs, ys, zs, kc, sum, mn);
             }
 #pragma unroll
-            for (int t = 0; t < MX_TPT; t++) acc[t] += (double)sum[t];
+            for (int t = 0; t < TPT; t++) acc[t] += (double)sum[t];
             __syncthreads();
         }
     }
 #pragma unroll
-    for (int t = 0; t < MX_TPT; t++)
+    for (int t = 0; t < TPT; t++)
         if (act[t]) a.pot[tid[t]] = acc[t];
 }
 
-template <int KT, bool HERM>
-__global__ void BT_MX_BOUNDS
+template <int KT, bool HERM, int TPT>
+__global__ void __launch_bounds__(MX_CHUNK / TPT)
 k_eval_targets_mixed(MixedTargetsArgs a)
 {
     extern __shared__ float smf[];
     __shared__ int slot;
     int w = a.queue ? next_item(a.queue, &slot) : blockIdx.x;
     while (w < a.nitems) {
-        targets_item<KT, HERM>(a, a.items[w], smf);
+        targets_item<KT, HERM, TPT>(a, a.items[w], smf);
         if (!a.queue) break;
         w = next_item(a.queue, &slot);
     }
@@ -614,48 +615,60 @@ void launch_to_f32(size_t n, const double *src, float *dst, cudaStream_t st)
 
 int mixed_targets_chunk() { return MX_CHUNK; }
 
-static size_t mixed_smem(int max_np1, bool herm = false)
+// Shared memory of the evaluation kernels: the far-field staging (grid
+// coordinates and proxy charges of one cluster) or the near-field tile,
+// whose four arrays sit MX_TILE_MAX floats apart in the particle-output
+// kernel (tile_stride) whatever the tile length.
+static size_t mixed_smem(int max_np1, bool herm, int tile_stride)
 {
     size_t far = sizeof(float) * (size_t)(3 * 16 + (herm ? 8 : 1) * max_np1 * max_np1 * max_np1);
-    size_t near = sizeof(float4) * MX_TILE;
+    size_t near = sizeof(float4) * (size_t)tile_stride;
     return far > near ? far : near;
 }
 
 // Grid of a work-queue launch: as many blocks as are resident at once.
 template <typename K>
-static int queue_grid(K kernel, size_t smem, int nitems)
+static int queue_grid(K kernel, int threads, size_t smem, int nitems)
 {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, MX_THREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     int g = sms * (per_sm > 0 ? per_sm : 1);
     return g < nitems ? g : nitems;
 }
 
-template <int KT, bool HERM>
+template <int KT, bool HERM, int TPT>
 static void eval_targets_mixed_t(const MixedTargetsArgs &a, cudaStream_t st)
 {
-    size_t sm = mixed_smem(a.max_np1, HERM);
-    cudaFuncSetAttribute(k_eval_targets_mixed<KT, HERM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int grid = a.queue ? queue_grid(k_eval_targets_mixed<KT, HERM>, sm, a.nitems) : a.nitems;
-    k_eval_targets_mixed<KT, HERM><<<grid, MX_THREADS, sm, st>>>(a);
+    size_t sm = mixed_smem(a.max_np1, HERM, MX_TILE_MAX);
+    cudaFuncSetAttribute(k_eval_targets_mixed<KT, HERM, TPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int grid = a.queue ? queue_grid(k_eval_targets_mixed<KT, HERM, TPT>, MX_CHUNK / TPT, sm, a.nitems) : a.nitems;
+    k_eval_targets_mixed<KT, HERM, TPT><<<grid, MX_CHUNK / TPT, sm, st>>>(a);
+}
+
+template <int KT, bool HERM>
+static void eval_targets_mixed_h(const MixedTargetsArgs &a, cudaStream_t st)
+{
+    if (a.tpt == 1) eval_targets_mixed_t<KT, HERM, 1>(a, st);
+    else if (a.tpt == 4) eval_targets_mixed_t<KT, HERM, 4>(a, st);
+    else eval_targets_mixed_t<KT, HERM, 2>(a, st);
 }
 
 void launch_eval_targets_mixed(int kernel, const MixedTargetsArgs &a, cudaStream_t st)
 {
     if (a.nitems <= 0) return;
-    if (kernel == 1) a.herm ? eval_targets_mixed_t<1, true>(a, st) : eval_targets_mixed_t<1, false>(a, st);
-    else if (kernel == 2) a.herm ? eval_targets_mixed_t<2, true>(a, st) : eval_targets_mixed_t<2, false>(a, st);
-    else a.herm ? eval_targets_mixed_t<3, true>(a, st) : eval_targets_mixed_t<3, false>(a, st);
+    if (kernel == 1) a.herm ? eval_targets_mixed_h<1, true>(a, st) : eval_targets_mixed_h<1, false>(a, st);
+    else if (kernel == 2) a.herm ? eval_targets_mixed_h<2, true>(a, st) : eval_targets_mixed_h<2, false>(a, st);
+    else a.herm ? eval_targets_mixed_h<3, true>(a, st) : eval_targets_mixed_h<3, false>(a, st);
 }
 
 template <int KT>
 static void eval_grids_mixed_t(const MixedGridsArgs &a, cudaStream_t st)
 {
-    size_t sm = mixed_smem(a.n + 1);
+    size_t sm = mixed_smem(a.n + 1, false, MX_TILE);
     cudaFuncSetAttribute(k_eval_grids_mixed<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int grid = a.queue ? queue_grid(k_eval_grids_mixed<KT>, sm, a.nitems) : a.nitems;
+    int grid = a.queue ? queue_grid(k_eval_grids_mixed<KT>, MX_THREADS, sm, a.nitems) : a.nitems;
     k_eval_grids_mixed<KT><<<grid, MX_THREADS, sm, st>>>(a);
 }
 

@@ -15,6 +15,17 @@ constexpr int MX_MAX_DEG = 12;
 #endif
 constexpr double MX_CLOSE_FRAC = BT_CLOSE_FRAC;
 
+// Tile shapes of the particle-output kernel (chosen by the autotuner): a
+// work item is MX_CHUNK targets of one target leaf, evaluated by
+// MX_CHUNK / tpt threads with tpt targets each; the near field streams
+// source leaves through shared memory in tiles of `tile` particles.
+constexpr int MX_CHUNK = 256;
+constexpr int MX_TILE_MAX = 2048;
+inline bool mixed_shape_valid(int tpt, int tile)
+{
+    return (tpt == 1 || tpt == 2 || tpt == 4) && (tile == 512 || tile == 1024 || tile == MX_TILE_MAX);
+}
+
 struct MixedTargetsArgs {
     int n, max_np1, nitems;
     const int2 *items;
@@ -38,6 +49,7 @@ struct MixedTargetsArgs {
     double kc;                                  // mixed_kernel_constant()
     double kp;                                  // kernel parameter (FP64 close pairs)
     double *pot;
+    int tpt, tile;                              // targets per thread, near-field source tile
 };
 
 struct MixedGridsArgs {

@@ -94,7 +94,8 @@ typedef struct bt_options {
                              pointers (FP64) and output is a device pointer          */
     int tree_build;       /* BT_TREE_GPU (default) or BT_TREE_HOST: where the trees
                              are built; both give the same trees and particle order  */
-    int dispatch;         /* mixed evaluation kernels: BT_DISPATCH_AUTO (default),
+    int dispatch;         /* mixed evaluation kernels: BT_DISPATCH_AUTO (default: the
+                             autotuned dispatch, else one block per work item),
                              BT_DISPATCH_QUEUE (persistent blocks taking cost-sorted
                              work items from a device counter) or BT_DISPATCH_GRID
                              (one block per work item); results are identical     */
@@ -182,6 +183,46 @@ int bt_session_create(int numSystems, const long long *targetOffsets, const long
 int bt_session_eval(bt_session *session, const double *sourceValue, double *outputArray,
                     bt_report *report);
 int bt_session_destroy(bt_session *session);
+
+/* Autotuning of the mixed-precision particle-output kernel (no counterpart
+ * in the reference).  Its tile shape -- targets per thread (1, 2 or 4, with
+ * 256 / targets_per_thread threads per block, so a work item is always 256
+ * targets of one leaf), near-field sources per shared-memory tile (512,
+ * 1024 or 2048) and dispatch (one block per work item, or persistent blocks
+ * on a device work queue) -- is picked by timing every candidate on the
+ * caller's own workload.  The chosen shape is installed for (device,
+ * kernel, approximation): later evaluations and sessions on that device
+ * with BT_DISPATCH_AUTO use it (an explicit dispatch option still wins). */
+typedef struct bt_tuning {
+    int targets_per_thread;   /* 1, 2 or 4                                         */
+    int source_tile;          /* 512, 1024 or 2048                                 */
+    int dispatch;             /* BT_DISPATCH_GRID or BT_DISPATCH_QUEUE             */
+    float ms;                 /* kernel time on the tuning sample (0: not measured) */
+} bt_tuning;
+
+/* Builds the problem as bt_session_create does (same arguments; opts must
+ * select BT_PRECISION_MIXED), evaluates it once, then times the
+ * particle-output kernel in all 18 shapes on a sample of its work items
+ * (every k-th of the cost-sorted list, about a sixteenth of a large
+ * problem).  best receives the fastest shape; trials (may be NULL)
+ * receives up to maxTrials measured shapes and *numTrials their count. */
+int bt_autotune(int numSystems, const long long *targetOffsets, const long long *sourceOffsets,
+                const double *targetX, const double *targetY, const double *targetZ,
+                const double *sourceX, const double *sourceY, const double *sourceZ,
+                const double *sourceValue, int kernel, double kernelParam,
+                int approximation, int compute_type, double theta, int interpOrder,
+                int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck,
+                const bt_options *opts, bt_tuning *best, bt_tuning *trials, int maxTrials,
+                int *numTrials);
+
+/* Installs a shape for (device, kernel, approximation), e.g. one saved
+ * from an earlier bt_autotune; NULL removes it (defaults: 2 targets per
+ * thread, 1024-source tiles, one block per work item). */
+int bt_tuning_set(int device, int kernel, int approximation, const bt_tuning *tuning);
+
+/* The shape in use for (device, kernel, approximation): the installed one,
+ * or the defaults with ms = 0.  *installed (may be NULL) tells which. */
+int bt_tuning_get(int device, int kernel, int approximation, bt_tuning *tuning, int *installed);
 
 /* Allocation-free evaluation (no counterpart in the reference).
  *
