@@ -28,6 +28,7 @@
 #include "bt_learned.h"
 #include "bt_gputree.h"
 #include "bt_ss.h"
+#include "bt_tc.h"
 #include "bt_host.h"
 
 namespace {
@@ -90,6 +91,7 @@ std::mutex g_ctx_mu;
 struct EvalShape {
     bool queue = false;
     int tpt = 2, tile = 1024;
+    bool tc_up = true;      // leaf P2M of the mixed Lagrange path on the tensor cores
 };
 
 // Autotuned shapes per device, kernel and approximation (bt_autotune,
@@ -518,6 +520,8 @@ struct DevPlan {
     bool mixed = false, herm = false, need_src_clusters = false, need_tgt_grids = false;
     bool queue = false;     // mixed kernels on a device work queue
     int tpt = 2, tile = 1024;   // tile shape of the mixed particle-output kernel
+    bool tc_up = false;         // leaf P2M on the tensor cores (bt_tc.cu)
+    int *d_err = nullptr;       // set by a tensor-core kernel whose bounded wait expired
     int n = 0, P = 0, ns = 0, nt = 0, max_np1 = 0, kernel = 0;
     double kp = 0.0;
     int S_n = 0, S_nleaves = 0, S_max_depth = 0, T_n = 0, T_nleaves = 0, T_max_depth = 0;
@@ -541,6 +545,24 @@ struct DevPlan {
     double *d_hpartial = nullptr;           // their partial moments
     int n_hchunks = 0, n_hred = 0;
 };
+
+// BT_ERR_TIMEOUT if a tensor-core kernel of the last evaluation gave up
+// waiting for its MMAs (its flag is cleared at the start of every evaluation).
+int check_device_error(const DevPlan &v, cudaStream_t st)
+{
+    if (!v.tc_up || !v.d_err) return BT_OK;
+    int flag = 0;
+    if (cudaMemcpyAsync(&flag, v.d_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        set_err("reading the device error flag failed");
+        return BT_ERR_CUDA;
+    }
+    if (flag) {
+        set_err("a tensor-core wait expired in the upward pass");
+        return BT_ERR_TIMEOUT;
+    }
+    return BT_OK;
+}
 
 // Arguments of the mixed particle-output kernel of a prepared plan.
 bt::MixedTargetsArgs mixed_targets_args(const DevPlan &v)
@@ -639,6 +661,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     }
     if (ev) CK(record(0));
     // upward pass
+    if (v.tc_up) CK(cudaMemsetAsync(v.d_err, 0, sizeof(int), st));
     if (need_src_clusters && ns > 0 && v.ss) {
         // subtraction: proxies of q*w (Q) and of w (W) by the same passes
         const double *charges[2] = {v.d_qw, v.d_sw};
@@ -666,6 +689,10 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
             bt::launch_p2m_hermite(n, v.n_hchunks, v.d_hchunks, v.n_hred, v.d_hred, d_sgrid, d_slen, d_ww, d_sx, d_sy,
                                    d_sz, d_sq, d_Q, v.d_hpartial, st);
             launches += v.n_hred > 0 ? 2 : 1;
+        } else if (v.tc_up && bt::p2m_tc_supported(n)) {
+            bt::launch_p2m_tc(n, v.S_nleaves, d_sleaves, d_sibeg, d_snum, d_sgrid, d_sx, d_sy, d_sz, d_sq, d_Q, v.d_err,
+                              st);
+            launches++;
         } else {
             bt::launch_p2m(n, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
                            d_sz, d_sq, d_Q, st);
@@ -687,8 +714,12 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         // proxy charges at the other degrees chosen per interaction
         for (size_t i = 0; i < xdeg.size(); i++) {
             const int d = xdeg[i];
-            bt::launch_p2m(d, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww, d_sx,
-                           d_sy, d_sz, d_sq, d_xQ[i], st);
+            if (v.tc_up && bt::p2m_tc_supported(d))
+                bt::launch_p2m_tc(d, v.S_nleaves, d_sleaves, d_sibeg, d_snum, d_xgrid[i], d_sx, d_sy, d_sz, d_sq,
+                                  d_xQ[i], v.d_err, st);
+            else
+                bt::launch_p2m(d, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww,
+                               d_sx, d_sy, d_sz, d_sq, d_xQ[i], st);
             launches++;
             for (int l = v.S_max_depth - 1; l >= 0; l--) {
                 int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
@@ -957,8 +988,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     L.add(&d_cpoff, pl.g_cp.rows + 1); L.add(&d_cpidx, pl.g_cp.off[pl.g_cp.rows]);
     L.add(&d_evitems, ev_items.size()); L.add(&d_griditems, grid_items.size()); L.add(&d_l2pitems, l2p_items.size());
     L.add(&d_out, nt);
-    int *d_queue;           // work-queue counters of the two evaluation kernels
-    L.add(&d_queue, 2);
+    int *d_queue;           // work-queue counters of the two evaluation kernels, then the error flag
+    L.add(&d_queue, 3);
     // subtraction: target charges and source weights in tree order, q*w,
     // the weight proxies and the weight field, a staging buffer for the
     // caller-order inputs, and the source order when the host built the tree
@@ -1066,6 +1097,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.queue = shape.queue;
         v.tpt = shape.tpt;
         v.tile = shape.tile;
+        v.tc_up = shape.tc_up && mixed && !herm;
         v.n = n; v.P = P; v.ns = ns; v.nt = nt; v.max_np1 = max_np1; v.kernel = o.kernel; v.kp = o.kp;
         v.S_n = S.n; v.S_nleaves = S.nleaves; v.S_max_depth = S.max_depth;
         v.T_n = T.n; v.T_nleaves = T.nleaves; v.T_max_depth = T.max_depth;
@@ -1117,6 +1149,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.d_cpidx = d_cpidx;
         v.d_order = d_order;
         v.d_queue = d_queue;
+        v.d_err = d_queue + 2;
         v.d_mxdidx = d_mxdidx;
         v.d_mxcpidx = d_mxcpidx;
         v.d_aoff = d_aoff;
@@ -1147,6 +1180,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         if (!out_on_device && nt > 0)
             CK(cudaMemcpyAsync(out, d_out, sizeof(double) * nt, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        rc = check_device_error(v, st);
+        if (rc != BT_OK) goto done;
         g_launches += launches;
         if (rep) {
             float a = 0, b = 0, c = 0, d = 0;
@@ -1407,7 +1442,12 @@ int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double 
     // device counter measured 2.5 % slower for the 16M clustered system
     // (cost-sorted items are already dispatched longest first by the block
     // scheduler).  An explicit dispatch option overrides the tuned one.
+    if (opts && opts->upward != BT_UPWARD_AUTO && opts->upward != BT_UPWARD_FP64) {
+        set_err("invalid upward %d", opts->upward);
+        return BT_ERR_PARAM;
+    }
     shape = tuned_shape(opts ? opts->device : 0, prm.kernel, prm.approx);
+    shape.tc_up = !(opts && opts->upward == BT_UPWARD_FP64);
     if (opts && opts->dispatch == BT_DISPATCH_QUEUE) shape.queue = true;
     if (opts && opts->dispatch == BT_DISPATCH_GRID) shape.queue = false;
     if (learned && (prm.precision != BT_PRECISION_MIXED || prm.ctype != PARTICLE_CLUSTER || prm.approx != LAGRANGE ||
@@ -2268,6 +2308,8 @@ int bt_session_eval(bt_session *session, const double *sourceValue, double *outp
         return BT_ERR_CUDA;
     }
     g_launches += S->graph_kernels;
+    const int erc = check_device_error(S->v, st);
+    if (erc != BT_OK) return erc;
     if (report) {
         *report = S->base;
         float a = 0, b = 0, c = 0, d = 0;

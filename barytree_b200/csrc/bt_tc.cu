@@ -1,0 +1,322 @@
+// bt_tc.cu -- tensor-core (tcgen05) contractions of barytree_b200.
+//
+// Leaf P2M of the mixed-precision path as a GEMM on the 5th-generation tensor
+// cores.  With Lx, Ly, Lz the barycentric Lagrange bases of a particle on the
+// leaf's Chebyshev grid (src/clusters/clusters.c:800-1004),
+//   Q[k1, k2, k3] = sum_i (q_i Lx_i[k1]) (Ly_i[k2] Lz_i[k3]),
+// i.e. D[m, k1] = sum_i A[m, i] B[k1, i] with m = (k2, k3) (M = (n+1)^2 rows,
+// padded to 128), k1 the N dimension (n+1 columns, padded to 16) and the
+// leaf's particles the K dimension.  Operands are split into TF32 pairs
+// (x = hi + lo) and accumulated as hi*hi + hi*lo + lo*hi in FP32 (3xTF32,
+// about FP32 accuracy per product); the accumulator lives in tensor memory.
+//
+// One CTA per leaf, 128 threads.  Per chunk of 32 particles the threads
+// evaluate the bases, form the operands, round them to TF32 pairs and store
+// them in shared memory in the canonical K-major layout without swizzling
+// (8-row x 16-byte core matrices; the two core matrices of one 8-wide K step
+// 128 bytes apart, 8-row groups 256 bytes apart).  Thread 0 issues 12
+// tcgen05.mma (4 K steps x 3 products) and commits them to an mbarrier; the
+// threads evaluate the next chunk's bases while the tensor core works.
+// Bases are FP64 (exact-node rule included), stored as FP32; a product a*b
+// splits into hi = tf32(a*b) and the TF32 rounding of the exact FP32 rest
+// fma(a, b, -hi).
+//
+// The tensor core's FP32 accumulation does not round to nearest, so long
+// FP32 sums drift (about 1e-6 relative over a 2000-particle leaf): each chunk
+// therefore sums into fresh accumulators, hi*hi apart from the small cross
+// products, and the threads fold every chunk into FP64 registers (about
+// 1.4e-7 relative, a few times the FP32 rounding of the proxies).  Every
+// mbarrier wait is bounded: on expiry the kernel records the failure, frees
+// its tensor memory and returns without writing.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bt_kernels.cuh"
+#include "bt_tc.h"
+
+namespace bt {
+
+namespace {
+
+constexpr int TC_THREADS = 128;
+constexpr int TC_M = 128;                  // MMA rows: (k2, k3) pairs, padded
+constexpr int TC_N = 16;                   // MMA columns: k1, padded
+constexpr int TC_KC = 32;                  // particles per chunk
+constexpr int TC_KSTEPS = TC_KC / 8;       // one tcgen05.mma (kind::tf32) covers K = 8
+constexpr int TC_MAXNP1 = 11;              // (n+1)^2 <= 128
+constexpr uint32_t TC_TMEM_COLS = 32;      // accumulators: hi*hi in columns 0-15, cross products in 16-31
+constexpr long long TC_WAIT_LIMIT = 1LL << 22;
+
+// Shared-memory layout (bytes).  A tile: 128 rows x 32 tf32; B tile: 16 x 32.
+constexpr uint32_t A_BYTES = TC_M * TC_KC * 4;                  // 16 KB
+constexpr uint32_t B_BYTES = TC_N * TC_KC * 4;                  // 2 KB
+constexpr uint32_t OFF_A = 0;                                   // [hi, lo]
+constexpr uint32_t OFF_B = OFF_A + 2 * A_BYTES;                 // [hi, lo]
+constexpr uint32_t OFF_L = OFF_B + 2 * B_BYTES;                 // float [3][TC_KC][TC_MAXNP1]
+constexpr uint32_t OFF_Q = OFF_L + 3 * TC_KC * TC_MAXNP1 * 4;   // float [TC_KC]
+constexpr uint32_t OFF_NODES = OFF_Q + TC_KC * 4;               // double [3][TC_MAXNP1]
+constexpr uint32_t OFF_BAR = (OFF_NODES + 3 * TC_MAXNP1 * 8 + 15) / 16 * 16;   // uint64
+constexpr uint32_t OFF_MISC = OFF_BAR + 16;                     // tmem address, status
+constexpr uint32_t TC_SMEM = OFF_MISC + 16;
+
+// byte offset of element (row, k) of a K-major tile with `rows` rows
+__device__ __forceinline__ uint32_t kmajor_off(int rows, int row, int k)
+{
+    return (uint32_t)((k >> 3) * rows * 32 + (row >> 3) * 256 + ((k >> 2) & 1) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// a*b = hi + lo in two TF32 values: hi the product rounded to TF32, lo the
+// rest (exact in FP32 by the fused multiply-add) rounded to TF32
+__device__ __forceinline__ void split_tf32(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+    hi = tf32_rna(a * b);
+    lo = tf32_rna(fmaf(a, b, -__uint_as_float(hi)));
+}
+
+// Shared-memory matrix descriptor: no swizzle, K-major; LBO = distance of the
+// two core matrices of one K step, SBO = distance of 8-row groups; bits 46-47
+// hold the descriptor version of sm_100.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr)
+{
+    uint64_t d = (uint64_t)((addr & 0x3FFFF) >> 4);
+    d |= (uint64_t)(128 >> 4) << 16;
+    d |= (uint64_t)(256 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor, kind::tf32: D FP32 (bits 4-5 = 1), A and B TF32
+// (bits 7-9 and 10-12 = 2), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                              ((uint32_t)(TC_M >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(TC_IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait for the completion of phase `parity` of an mbarrier.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long it = 0; it < TC_WAIT_LIMIT; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int NP1>
+__global__ void __launch_bounds__(TC_THREADS)
+k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int *__restrict__ numpar,
+         const double *__restrict__ grid, const double *__restrict__ sx, const double *__restrict__ sy,
+         const double *__restrict__ sz, const double *__restrict__ sq, double *__restrict__ Q, int *err)
+{
+    constexpr int n = NP1 - 1, ROWS = NP1 * NP1, P = ROWS * NP1;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    float *Lb = reinterpret_cast<float *>(sm + OFF_L);          // [axis][particle][k]
+    float *qs = reinterpret_cast<float *>(sm + OFF_Q);
+    double *nodes = reinterpret_cast<double *>(sm + OFF_NODES);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
+    uint32_t *misc = reinterpret_cast<uint32_t *>(sm + OFF_MISC);  // [0] tmem address, [1] status
+    unsigned char *Ah = sm + OFF_A, *Al = Ah + A_BYTES, *Bh = sm + OFF_B, *Bl = Bh + B_BYTES;
+    const int t = threadIdx.x, warp = t >> 5;
+    const int node = leaves[blockIdx.x];
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(misc)),
+                     "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        misc[1] = 1;
+    }
+    for (int i = t; i < 3 * NP1; i += TC_THREADS) nodes[i] = grid[(size_t)node * 3 * NP1 + i];
+    // padding rows of the operand tiles stay zero
+    for (uint32_t o = t * 16; o < OFF_L; o += TC_THREADS * 16) *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = misc[0];
+
+    const int b0 = ibeg[node], m = numpar[node];
+    const int nch = (m + TC_KC - 1) / TC_KC;
+    const int k2 = t % NP1, k3 = t / NP1;      // this thread's A row (valid for t < ROWS)
+    double acc[NP1];                           // this row of Q (TMEM lane t), FP64 across chunks
+#pragma unroll
+    for (int k = 0; k < NP1; k++) acc[k] = 0.0;
+    bool ok = true;
+    const uint32_t bar_a = smem_addr(bar);
+    uint32_t wpar = 0;                         // parity of the last wait (repeated once if it expired)
+    // chunk c: products hi*hi into accumulator columns 0-15 and the two
+    // cross products into columns 16-31, from zero (short FP32 sums on the
+    // tensor core); once its MMAs have completed the threads fold the chunk
+    // into FP64 registers.  The bases of chunk c+1 are evaluated while the
+    // tensor core works on chunk c.
+    for (int c = 0; c <= nch && ok; c++) {
+        if (c < nch) {
+            const int cm = min(TC_KC, m - c * TC_KC);
+            if (t < 3 * TC_KC) {
+                const int i = t / 3, ax = t % 3;
+                double L[NP1];
+                if (i < cm) {
+                    const double *src = ax == 0 ? sx : ax == 1 ? sy : sz;
+                    lagrange_basis(n, nodes + ax * NP1, src[b0 + c * TC_KC + i], L);
+                    if (ax == 0) qs[i] = (float)sq[b0 + c * TC_KC + i];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < NP1; k++) L[k] = 0.0;
+                    if (ax == 0) qs[i] = 0.0f;
+                }
+#pragma unroll
+                for (int k = 0; k < NP1; k++) Lb[(ax * TC_KC + i) * TC_MAXNP1 + k] = (float)L[k];
+            }
+        }
+        if (c >= 1) {
+            // chunk c-1: wait for its MMAs, then fold its accumulators
+            wpar = (uint32_t)((c - 1) & 1);
+            if (t == 0) misc[1] = bar_wait(bar_a, wpar) ? 1u : 0u;
+            __syncthreads();
+            if (misc[1] == 0) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                "[%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int k = 0; k < NP1; k++)
+                acc[k] += (double)__uint_as_float(r[k]) + (double)__uint_as_float(r[16 + k]);
+        } else {
+            __syncthreads();
+        }
+        if (c == nch) break;
+        // operands of chunk c (the tensor core has finished reading chunk c-1's)
+        if (t < ROWS) {
+#pragma unroll
+            for (int k4 = 0; k4 < TC_KC; k4 += 4) {
+                uint32_t h[4], l[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int i = k4 + j;
+                    split_tf32(Lb[(TC_KC + i) * TC_MAXNP1 + k2], Lb[(2 * TC_KC + i) * TC_MAXNP1 + k3], h[j], l[j]);
+                }
+                const uint32_t o = kmajor_off(TC_M, t, k4);
+                *reinterpret_cast<uint4 *>(Ah + o) = make_uint4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<uint4 *>(Al + o) = make_uint4(l[0], l[1], l[2], l[3]);
+            }
+        }
+        {
+            // B rows: thread t covers row k1 = t / 8, particles 4 (t % 8) .. +3
+            const int k1 = t >> 3, k4 = (t & 7) * 4;
+            uint32_t h[4] = {0, 0, 0, 0}, l[4] = {0, 0, 0, 0};
+            if (k1 < NP1) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) split_tf32(qs[k4 + j], Lb[(k4 + j) * TC_MAXNP1 + k1], h[j], l[j]);
+            }
+            const uint32_t o = kmajor_off(TC_N, k1, k4);
+            *reinterpret_cast<uint4 *>(Bh + o) = make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4 *>(Bl + o) = make_uint4(l[0], l[1], l[2], l[3]);
+        }
+        // make the operands visible to the tensor core (async proxy); the
+        // barrier also orders the accumulator loads above before the MMAs
+        // that overwrite those columns
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t ah = smem_addr(Ah), al = smem_addr(Al), bh = smem_addr(Bh), bl = smem_addr(Bl);
+#pragma unroll
+            for (int s = 0; s < TC_KSTEPS; s++) {
+                const uint32_t oa = s * TC_M * 32, ob = s * TC_N * 32;
+                mma_tf32(tmem, smem_desc(ah + oa), smem_desc(bh + ob), s > 0 ? 1u : 0u);
+                mma_tf32(tmem + 16, smem_desc(ah + oa), smem_desc(bl + ob), s > 0 ? 1u : 0u);
+                mma_tf32(tmem + 16, smem_desc(al + oa), smem_desc(bh + ob), 1u);
+            }
+            mma_commit(bar_a);
+        }
+    }
+    if (ok) {
+        if (t < ROWS) {
+#pragma unroll
+            for (int k1 = 0; k1 < NP1; k1++) Q[(size_t)node * P + k1 + NP1 * t] = acc[k1];
+        }
+    } else if (t == 0) {
+        atomicExch(err, 1);
+        // one more bounded wait for the MMAs in flight before the memory is released
+        bar_wait(bar_a, wpar);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+    }
+}
+
+template <int NP1>
+void p2m_tc_t(int nleaves, const int *leaves, const int *ibeg, const int *numpar, const double *grid,
+              const double *sx, const double *sy, const double *sz, const double *sq, double *Q, int *err,
+              cudaStream_t st)
+{
+    cudaFuncSetAttribute(k_p2m_tc<NP1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+    k_p2m_tc<NP1><<<nleaves, TC_THREADS, TC_SMEM, st>>>(leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err);
+}
+
+}  // namespace
+
+bool p2m_tc_supported(int n) { return n >= 1 && n + 1 <= TC_MAXNP1; }
+
+void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const int *numpar, const double *grid,
+                   const double *sx, const double *sy, const double *sz, const double *sq, double *Q, int *err,
+                   cudaStream_t st)
+{
+    if (nleaves <= 0) return;
+    switch (n + 1) {
+#define BT_TC(N) case N: p2m_tc_t<N>(nleaves, leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err, st); return;
+        BT_TC(2) BT_TC(3) BT_TC(4) BT_TC(5) BT_TC(6) BT_TC(7) BT_TC(8) BT_TC(9) BT_TC(10) BT_TC(11)
+#undef BT_TC
+    }
+}
+
+}  // namespace bt

@@ -1,0 +1,17 @@
+// bt_tc.h -- tensor-core (tcgen05) kernels of barytree_b200 (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace bt {
+
+// Leaf P2M (Lagrange) on the tensor cores in 3xTF32 with FP32 accumulation,
+// for degrees with (n+1)^2 <= 128.  Same output layout as launch_p2m
+// (Q[node * P + k1 + (n+1) (k2 + (n+1) k3)], FP64).  *err is set to 1 if a
+// bounded wait for the tensor core expired (the leaf's Q is then not written).
+bool p2m_tc_supported(int n);
+void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const int *numpar, const double *grid,
+                   const double *sx, const double *sy, const double *sz, const double *sq, double *Q, int *err,
+                   cudaStream_t st);
+
+}  // namespace bt

@@ -291,6 +291,8 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="skip the session (graph replay) measurement")
     ap.add_argument("--dispatch", choices=["auto", "queue", "grid"], default="auto",
                     help="mixed evaluation kernels: persistent blocks on a device work queue, or one block per item")
+    ap.add_argument("--upward", choices=["auto", "fp64"], default="auto",
+                    help="mixed Lagrange upward pass: tensor-core leaf P2M (auto) or FP64 SIMT")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default tile shape instead of autotuning it on this workload")
     ap.add_argument("--n", type=int, default=None,
@@ -335,7 +337,8 @@ def main():
                   kernel=cfg["kernel"], kernel_param=cfg["kp"], approximation=cfg["approx"],
                   compute_type=cfg["ctype"], theta=cfg["theta"], degree=cfg["degree"], max_source_leaf=cfg["leaf"],
                   max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=local,
-                  dispatch={"auto": B.DISPATCH_AUTO, "queue": B.DISPATCH_QUEUE, "grid": B.DISPATCH_GRID}[args.dispatch])
+                  dispatch={"auto": B.DISPATCH_AUTO, "queue": B.DISPATCH_QUEUE, "grid": B.DISPATCH_GRID}[args.dispatch],
+                  upward=B.UPWARD_FP64 if args.upward == "fp64" else B.UPWARD_AUTO)
 
     # device-resident inputs (targets are separate arrays with the same coordinates)
     d_in = [torch.from_numpy(a).to(dev) for a in (x, y, z, x.copy(), y.copy(), z.copy(), q)]
@@ -378,7 +381,7 @@ def main():
         t0 = time.perf_counter()
         systems = ([(x[a:b], y[a:b], z[a:b], x[a:b], y[a:b], z[a:b], q[a:b]) for a, b in zip(off[:-1], off[1:])]
                    if batch else [(x, y, z, x, y, z, q)])
-        tune_kw = {k: v for k, v in common.items() if k not in ("precision", "dispatch")}
+        tune_kw = {k: v for k, v in common.items() if k not in ("precision", "dispatch", "upward")}
         best, trials = B.autotune(systems, **tune_kw)
         tuning = {"best": best, "trials": len(trials), "seconds": round(time.perf_counter() - t0, 2),
                   "default_ms": next((t["ms"] for t in trials if t["targets_per_thread"] == 2 and
@@ -485,7 +488,7 @@ def main():
             "data": "synthetic (seeded numpy PCG64 with the configuration's distribution)",
             "config": {"workload": cfg["workload"], "config_id": args.config, "precision": args.precision,
                        "degree_policy": policy, "tolerance": args.tolerance, "dispatch": args.dispatch,
-                       "tile_shape": tuning,
+                       "tile_shape": tuning, "upward": args.upward,
                        "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"{world} independent " + ("batch(es)" if batch else "system(s)") + ", one per GPU",
                        "systems": len(off) - 1 if batch else 1,

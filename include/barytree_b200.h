@@ -99,10 +99,14 @@ typedef struct bt_options {
                              BT_DISPATCH_QUEUE (persistent blocks taking cost-sorted
                              work items from a device counter) or BT_DISPATCH_GRID
                              (one block per work item); results are identical     */
+    int upward;           /* mixed Lagrange upward pass: BT_UPWARD_AUTO (default: leaf
+                             P2M on the tensor cores in 3xTF32 where (n+1)^2 <= 128)
+                             or BT_UPWARD_FP64 (FP64 SIMT, as the FP64 path)         */
 } bt_options;
 
 enum { BT_TREE_GPU = 0, BT_TREE_HOST = 1 };
 enum { BT_DISPATCH_AUTO = 0, BT_DISPATCH_QUEUE = 1, BT_DISPATCH_GRID = 2 };
+enum { BT_UPWARD_AUTO = 0, BT_UPWARD_FP64 = 1 };
 
 /* Per-call report (all optional: pass NULL). */
 typedef struct bt_report {

@@ -1,0 +1,76 @@
+"""GPU tests of the tensor-core leaf P2M (tcgen05, 3xTF32) of the mixed
+Lagrange path, against the FP64 SIMT P2M (option BT_UPWARD_FP64) and the
+FP64 direct sum.
+
+The two upward passes must agree to within a few FP32 roundings at every
+degree the tensor-core kernel covers ((n+1)^2 <= 128): 5e-7 relative in the
+potentials, where the proxy charges carry about 1.4e-7 (3xTF32 products,
+short FP32 sums on the tensor core, FP64 across 32-particle chunks); the
+potentials must keep the mixed path's accuracy against the direct sum.  They must not be bit-identical there (proof that the
+tensor-core kernel ran); at degrees 11 and 12 the FP64 kernel serves both
+settings and the potentials are identical.  Every leaf exercises the
+exact-node rule: its extreme particles sit on the end nodes of its grid.
+"""
+import numpy as np
+import pytest
+
+import barytree_b200 as B
+from conftest import uniform_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("degree", list(range(1, 13)))
+def test_tensor_core_p2m_against_fp64_p2m(degree):
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(21, 80000)
+    kw = dict(theta=0.7, degree=degree, max_source_leaf=500, max_target_leaf=500, size_check=1.0,
+              precision=B.PRECISION_MIXED)
+    tc, rep = B.treecode(tx, ty, tz, sx, sy, sz, sq, return_report=True, **kw)
+    f64 = B.treecode(tx, ty, tz, sx, sy, sz, sq, upward=B.UPWARD_FP64, **kw)
+    assert rep["pc_ptwise"] > 0
+    if degree <= 10:
+        assert not np.array_equal(tc, f64)
+        assert _rel(tc, f64) < 5e-7
+    else:
+        assert np.array_equal(tc, f64)
+    idx = np.arange(0, len(tx), 80)
+    exact = B.direct(tx[idx], ty[idx], tz[idx], sx, sy, sz, sq)
+    assert _rel(tc[idx], exact) <= 1.05 * _rel(f64[idx], exact) + 3e-7
+
+
+@pytest.mark.parametrize("kernel,kp", [(B.Kernel.YUKAWA, 0.5), (B.Kernel.REGULARIZED_COULOMB, 1e-3)])
+def test_tensor_core_p2m_other_kernels(kernel, kp):
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(22, 60000, targets="other")
+    kw = dict(kernel=kernel, kernel_param=kp, theta=0.7, degree=7, max_source_leaf=400, max_target_leaf=400,
+              size_check=1.0, precision=B.PRECISION_MIXED)
+    tc = B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw)
+    f64 = B.treecode(tx, ty, tz, sx, sy, sz, sq, upward=B.UPWARD_FP64, **kw)
+    assert _rel(tc, f64) < 5e-7
+
+
+def test_tensor_core_p2m_with_learned_degrees_and_sessions():
+    from barytree_b200 import selector
+    selector.install_default()
+    rng = np.random.default_rng(23)
+    n = 400000
+    c = rng.uniform(-0.6, 0.6, (4, 3))
+    pts = np.concatenate([rng.normal(c[k], 0.1, (n // 5, 3)) for k in range(4)] + [rng.uniform(-1, 1, (n // 5, 3))])
+    pts = np.clip(pts, -1, 1)
+    x, y, z = pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy()
+    q = rng.uniform(-1, 1, len(x))
+    kw = dict(theta=0.7, degree=10, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
+              precision=B.PRECISION_MIXED, degree_policy=B.DEGREE_LEARNED, tolerance=1e-6)
+    tc = B.treecode(x, y, z, x, y, z, q, **kw)
+    f64 = B.treecode(x, y, z, x, y, z, q, upward=B.UPWARD_FP64, **kw)
+    assert _rel(tc, f64) < 5e-7
+    idx = np.arange(0, len(x), 400)
+    exact = B.direct(x[idx], y[idx], z[idx], x, y, z, q)
+    assert _rel(tc[idx], exact) < 1e-6
+    sess = B.Session([(x, y, z, x, y, z, q)], **kw)
+    (s_out,) = sess.evaluate(q)
+    sess.close()
+    assert np.array_equal(s_out, tc)

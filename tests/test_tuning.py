@@ -59,3 +59,11 @@ def test_autotune_needs_mixed_precision():
                              B.ctypes.byref(best), None, 0, None)
     assert rc == B.BT_ERR_UNSUPPORTED
     assert "BT_PRECISION_MIXED" in B.last_error()
+
+
+def test_invalid_upward_option_is_a_parameter_error():
+    rng = np.random.default_rng(1)
+    x, y, z, q = (rng.uniform(-1, 1, 50) for _ in range(4))
+    with pytest.raises(B.BaryTreeError) as e:
+        B.treecode(x, y, z, x, y, z, q, precision=B.PRECISION_MIXED, upward=7)
+    assert e.value.code == B.BT_ERR_PARAM and "upward" in B.last_error()
