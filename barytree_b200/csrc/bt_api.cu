@@ -50,6 +50,21 @@ double now_ms()
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Host-side phase times on stderr when the environment variable
+// BARYTREE_B200_TIMING is set (diagnostics; device phases are in bt_report).
+struct PhaseTimer {
+    bool on;
+    double t;
+    PhaseTimer() : on(getenv("BARYTREE_B200_TIMING") != nullptr), t(now_ms()) {}
+    void mark(const char *what)
+    {
+        if (!on) return;
+        const double n = now_ms();
+        fprintf(stderr, "[barytree_b200] %-34s %9.3f ms\n", what, n - t);
+        t = n;
+    }
+};
+
 // Grow-only device arena per device, reused across calls so steady-state
 // calls do not touch cudaMalloc.
 struct Arena {
@@ -254,19 +269,24 @@ void hermite_ww(int n, double *ww)
     ww[n] = -ww[0];
 }
 
+// Chebyshev grids of every node: x0 + (cos(i pi / n) + 1) / 2 (x1 - x0) per
+// axis, the same operations as bt_cheb_nodes (src/clusters/clusters.c:857-862)
+// with the n+1 factors (cos + 1) / 2 computed once per call.
 void fill_grids(const bt_tree &t, int n, std::vector<double> &grid, std::vector<double> &len)
 {
-    int np1 = n + 1;
-    grid.assign((size_t)t.n * 3 * np1, 0.0);
-    len.assign((size_t)t.n * 3, 0.0);
+    const int np1 = n + 1;
+    double h[BT_MAX_DEGREE + 1];
+    for (int i = 0; i <= n; i++) h[i] = (cos(i * M_PI / n) + 1.0) / 2.0;
+    grid.resize((size_t)t.n * 3 * np1);
+    len.resize((size_t)t.n * 3);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < t.n; i++) {
         double *g = grid.data() + (size_t)i * 3 * np1;
-        bt_cheb_nodes(n, t.x0[i], t.x1[i], g);
-        bt_cheb_nodes(n, t.y0[i], t.y1[i], g + np1);
-        bt_cheb_nodes(n, t.z0[i], t.z1[i], g + 2 * np1);
-        len[3 * i] = t.x1[i] - t.x0[i];
-        len[3 * i + 1] = t.y1[i] - t.y0[i];
-        len[3 * i + 2] = t.z1[i] - t.z0[i];
+        const double lo[3] = {t.x0[i], t.y0[i], t.z0[i]}, hi[3] = {t.x1[i], t.y1[i], t.z1[i]};
+        for (int a = 0; a < 3; a++) {
+            for (int k = 0; k <= n; k++) g[a * np1 + k] = lo[a] + h[k] * (hi[a] - lo[a]);
+            len[3 * (size_t)i + a] = hi[a] - lo[a];
+        }
     }
 }
 
@@ -454,12 +474,14 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
                    const double *sq, bool inputs_on_device, DevParts &dp)
 {
     cudaStream_t st = ctx->stream;
+    PhaseTimer pt;
     const bt_params &o = pl.prm;
     const int nt = (int)sys.toff[sys.n], ns = (int)sys.soff[sys.n];
     long long launches = 0;
     bool same = sys.toff == sys.soff && o.maxs == o.maxt;
     if (same && !inputs_on_device)
         same = same_host(tx, sx, (size_t)nt) && same_host(ty, sy, (size_t)nt) && same_host(tz, sz, (size_t)nt);
+    pt.mark("setup: compare target/source arrays");
     const bool check_on_device = same && inputs_on_device && !(tx == sx && ty == sy && tz == sz);
     double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx = nullptr, *d_ty = nullptr, *d_tz = nullptr;
     int *d_sord, *d_tord = nullptr;
@@ -489,6 +511,7 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
     int e = bt::gpu_build_forest(sys.n, sys.soff.data(), sx, sy, sz, sq, o.maxs, sa, d_work, wbytes, &pl.st, st,
                                  &launches);
     const char *which = "source";
+    pt.mark("setup: source tree (GPU)");
     if (!e && !same) {
         bt::GtArrays ta{d_tx, d_ty, d_tz, nullptr, d_tord};
         which = "target";
@@ -510,7 +533,9 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
     } else {
         dp.tx = d_tx; dp.ty = d_ty; dp.tz = d_tz; dp.order = d_tord;
     }
+    pt.mark("setup: target tree");
     bt_plan_lists(&pl);
+    pt.mark("setup: interaction lists (host)");
     return BT_OK;
 }
 
@@ -850,6 +875,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     cudaStream_t st = ctx->stream;
     int rc = BT_OK;
     double t0 = now_ms();
+    PhaseTimer pt;
     long long launches = 0;
 
     std::vector<double> sgrid, slen, tgrid, tlen;
@@ -872,6 +898,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     for (int d : xdeg) max_np1 = std::max(max_np1, d + 1);
     double ww[BT_MAX_DEGREE + 1];
     hermite_ww(n, ww);
+    pt.mark("plan: Chebyshev grids");
 
     // work items
     const bool need_src_clusters = (o.ctype != CLUSTER_PARTICLE);
@@ -965,6 +992,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     int2 *d_evitems, *d_griditems, *d_l2pitems;
     int *d_order;
     double *d_out;
+    pt.mark("plan: work items and list arrays");
     Layout L;
     if (dp) {
         d_sx = (double *)dp->sx; d_sy = (double *)dp->sy; d_sz = (double *)dp->sz; d_sq = (double *)dp->sq;
@@ -1175,6 +1203,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             CK(cudaStreamSynchronize(st));
             goto done;
         }
+        pt.mark("plan: device arrays and uploads");
         rc = issue_plan(v, st, ev, out_on_device ? out : d_out, launches);
         if (rc != BT_OK) goto done;
         if (!out_on_device && nt > 0)
@@ -1182,6 +1211,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         CK(cudaStreamSynchronize(st));
         rc = check_device_error(v, st);
         if (rc != BT_OK) goto done;
+        pt.mark("evaluation (device, synchronised)");
         g_launches += launches;
         if (rep) {
             float a = 0, b = 0, c = 0, d = 0;
@@ -1239,6 +1269,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         return BT_ERR_PARAM;
     }
     const bt_tree &S = pl.st, &T = pl.tt;
+    PhaseTimer pt;
     const int64_t ne = pl.t_approx.off[pl.t_approx.rows];
     std::vector<unsigned char> choice(ne > 0 ? ne : 1);
     cudaStream_t st = ctx->stream;
@@ -1247,12 +1278,12 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         std::vector<double> sctr, srad, tctr, trad;
         node_geometry(S, sctr, srad);
         node_geometry(T, tctr, trad);
-        const int64_t CH = 1 << 18;
         double *d_sq, *d_mom, *d_sctr, *d_tctr, *d_srad, *d_trad;
         int *d_sibeg, *d_snum, *d_tnum, *d_idx, *d_unit, *d_snch, *d_sch, *d_sleaves, *d_slvl;
         int64_t *d_off;
-        float *d_feat, *d_w, *d_act, *d_pred;
+        float *d_feat, *d_w, *d_pred;
         unsigned char *d_choice;
+        pt.mark("selection: node geometry (host)");
         Layout L;
         if (dp) d_sq = (double *)dp->sq;
         else L.add(&d_sq, pl.src.n);
@@ -1261,7 +1292,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         L.add(&d_snch, S.n); L.add(&d_sch, 8 * (size_t)S.n); L.add(&d_sleaves, S.nleaves);
         L.add(&d_slvl, S.lvl_off ? S.lvl_off[S.max_depth] : 0);
         L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
-        L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size()); L.add(&d_act, 3 * (size_t)CH * bt::MLP_H);
+        L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size());
         L.add(&d_pred, (size_t)ne * bt::MLP_OUT); L.add(&d_choice, ne);
         if (!arena.reserve(L.total())) {
             set_err(arena.fixed ? "degree selection needs more scratch than the static array holds"
@@ -1288,11 +1319,8 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             fa.t_numpar = d_tnum; fa.s_numpar = d_snum;
             bt::launch_features(fa, ne, d_feat, st);
             launches++;
-            for (int64_t c0 = 0; c0 < ne; c0 += CH) {
-                int B = (int)std::min<int64_t>(CH, ne - c0);
-                bt::mlp_forward(d_w, B, d_feat + c0 * bt::MLP_IN, d_act, d_pred + c0 * bt::MLP_OUT, st);
-                launches += 4;
-            }
+            bt::mlp_infer(d_w, ne, d_feat, d_pred, st);
+            launches++;
             bt::launch_select(ne, d_pred, d_feat, (float)(log10(tol) - SELECT_MARGIN_DECADES), d_choice, st);
             launches++;
             CK(cudaGetLastError());
@@ -1301,6 +1329,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             g_launches += launches;
         }
     }
+    pt.mark("selection: features + MLP (GPU)");
     {
         // rewrite the target-leaf lists: chosen degree per kept entry, direct
         // evaluation for the rest (appended to the direct list)
@@ -1356,6 +1385,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         pl.a_deg = (unsigned char *)malloc(adeg.size() + 1);
         memcpy(pl.a_deg, adeg.data(), adeg.size());
     }
+    pt.mark("selection: list rewrite (host)");
 done:
     return rc;
 }
@@ -1543,10 +1573,12 @@ int eval_common(const Systems &sys, const double *tx, const double *ty, const do
     }
     const DevParts *dpp = gpu_tree ? &dp : nullptr;
     double t1 = now_ms();
+    PhaseTimer pt;
     if (rep) {
         rep->ms_setup = t1 - t0;
         rep->ms_total = t1 - t0;
         count_interactions(pl, rep);
+        pt.mark("setup: interaction counts (host)");
     }
     if (learned) {
         rc = select_degrees(ctx, *arena, pl, tol, dpp);
@@ -1555,7 +1587,9 @@ int eval_common(const Systems &sys, const double *tx, const double *ty, const do
             return rc;
         }
         if (rep) {
+            pt.t = now_ms();
             count_learned(pl, rep);
+            pt.mark("selection: counts (host)");
             rep->ms_setup = now_ms() - t0;
         }
     }
@@ -2029,17 +2063,16 @@ int bt_mlp_predict(const float *weights, const float *features, long n, float *o
     if (rc != BT_OK) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t st = ctx->stream;
-    float *d_w, *d_x, *d_act, *d_yh;
+    float *d_w, *d_x, *d_yh;
     Layout L;
-    L.add(&d_w, bt::MLP_NWEIGHTS); L.add(&d_x, (size_t)n * bt::MLP_IN); L.add(&d_act, 3 * (size_t)n * bt::MLP_H);
-    L.add(&d_yh, (size_t)n * bt::MLP_OUT);
+    L.add(&d_w, bt::MLP_NWEIGHTS); L.add(&d_x, (size_t)n * bt::MLP_IN); L.add(&d_yh, (size_t)n * bt::MLP_OUT);
     if (!ctx->arena.reserve(L.total())) { set_err("device allocation failed"); return BT_ERR_CUDA; }
     L.bind(ctx->arena);
     {
         CK(cudaMemcpyAsync(d_w, weights, sizeof(float) * bt::MLP_NWEIGHTS, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(d_x, features, sizeof(float) * (size_t)n * bt::MLP_IN, cudaMemcpyHostToDevice, st));
-        bt::mlp_forward(d_w, (int)n, d_x, d_act, d_yh, st);
-        g_launches += 4;
+        bt::mlp_infer(d_w, n, d_x, d_yh, st);
+        g_launches += 1;
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out, d_yh, sizeof(float) * (size_t)n * bt::MLP_OUT, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
