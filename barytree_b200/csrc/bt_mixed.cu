@@ -211,20 +211,6 @@ __device__ __forceinline__ void pc_cluster_herm(const float *x, const float *y, 
     for (int t = 0; t < NT; t++) out[t] = s[t] - c[t];
 }
 
-template <int KT, int NT>
-__device__ void pc_cluster_herm_dispatch(int np1, const float *x, const float *y, const float *z, const float *g,
-                                         const float *q, float kc, float kp, float *out)
-{
-    switch (np1) {
-#define BT_CASE(N) case N: pc_cluster_herm<KT, N, NT>(x, y, z, g, q, kc, kp, out); return;
-        BT_CASE(2) BT_CASE(3) BT_CASE(4) BT_CASE(5) BT_CASE(6) BT_CASE(7) BT_CASE(8)
-        BT_CASE(9) BT_CASE(10) BT_CASE(11) BT_CASE(12) BT_CASE(13)
-#undef BT_CASE
-    }
-#pragma unroll
-    for (int t = 0; t < NT; t++) out[t] = 0.f;
-}
-
 // Near-field tiles.  FP32 leaf-relative coordinates carry an absolute error
 // of about 6e-8 of the leaf size, a large relative error for a pair much
 // closer than the leaf size, and such a pair dominates its target's
@@ -268,6 +254,100 @@ __device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c)
     f2_t r;
     asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
     return r;
+}
+
+// Hermite far field with the targets in packed pairs (NT even, Coulomb and
+// regularised Coulomb): the same operations as pc_cluster_herm lane by lane,
+// in f32x2 instructions, so the results are identical and the FMA-pipe work
+// per evaluation halves.  qd holds each moment twice ({q, q}, same staging
+// scales as pc_cluster_herm).
+template <int KT, int NP1, int NT>
+__device__ __forceinline__ void pc_cluster_herm_f2(const float *x, const float *y, const float *z, const float *g,
+                                                   const f2_t *qd, float kc, float *out)
+{
+    constexpr int P = NP1 * NP1 * NP1, NPR = NT / 2;
+    f2_t gx[NPR][NP1];
+#pragma unroll
+    for (int p = 0; p < NPR; p++)
+#pragma unroll
+        for (int k = 0; k < NP1; k++) gx[p][k] = f2_make(x[2 * p] - g[k], x[2 * p + 1] - g[k]);
+    float s[NT], c[NT];
+#pragma unroll
+    for (int t = 0; t < NT; t++) { s[t] = 0.f; c[t] = 0.f; }
+    const f2_t kc2 = f2_make(kc, kc), one = f2_make(1.0f, 1.0f), zero = f2_make(0.0f, 0.0f);
+    int j = 0;
+    for (int k3 = 0; k3 < NP1; k3++) {
+        const float gz = g[2 * NP1 + k3];
+        for (int k2 = 0; k2 < NP1; k2++) {
+            const float gy = g[NP1 + k2];
+            f2_t dy[NPR], dz[NPR], dyz[NPR], dydz[NPR], row[NPR];
+#pragma unroll
+            for (int p = 0; p < NPR; p++) {
+                dy[p] = f2_make(y[2 * p] - gy, y[2 * p + 1] - gy);
+                dz[p] = f2_make(z[2 * p] - gz, z[2 * p + 1] - gz);
+                dyz[p] = f2_fma(dy[p], dy[p], f2_mul(dz[p], dz[p]));
+                if (KT == 3) dyz[p] = f2_fma(one, kc2, dyz[p]);
+                dydz[p] = f2_mul(dy[p], dz[p]);
+                row[p] = zero;
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < NP1; k1++) {
+                const int jj = j + k1;
+                const f2_t q0 = qd[jj], q1 = qd[P + jj], q2 = qd[2 * P + jj], q3 = qd[3 * P + jj];
+                const f2_t q4 = qd[4 * P + jj], q5 = qd[5 * P + jj], q6 = qd[6 * P + jj], q7 = qd[7 * P + jj];
+#pragma unroll
+                for (int p = 0; p < NPR; p++) {
+                    const f2_t dx = gx[p][k1];
+                    const f2_t r2 = f2_fma(dx, dx, dyz[p]);
+                    float ra, rb;
+                    f2_split(r2, ra, rb);
+                    const f2_t rinv = f2_make(rsqrt_apx(ra), rsqrt_apx(rb));
+                    const f2_t rinv2 = f2_mul(rinv, rinv);
+                    const f2_t dxdy = f2_mul(dx, dy[p]), dxdz = f2_mul(dx, dz[p]);
+                    const f2_t a1 = f2_fma(q1, dx, f2_fma(q2, dy[p], f2_mul(q3, dz[p])));
+                    const f2_t a2 = f2_fma(q4, dxdy, f2_fma(q5, dydz[p], f2_mul(q6, dxdz)));
+                    const f2_t a3 = f2_mul(f2_mul(q7, dxdy), dz[p]);
+                    const f2_t r3 = f2_mul(rinv, rinv2), r5 = f2_mul(r3, rinv2), r7 = f2_mul(r5, rinv2);
+                    row[p] = f2_fma(rinv, q0, f2_fma(r3, a1, f2_fma(r5, a2, f2_fma(r7, a3, row[p]))));
+                }
+            }
+            j += NP1;
+#pragma unroll
+            for (int p = 0; p < NPR; p++) {
+                float lo, hi;
+                f2_split(row[p], lo, hi);
+                kahan_add(s[2 * p], c[2 * p], lo);
+                kahan_add(s[2 * p + 1], c[2 * p + 1], hi);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = s[t] - c[t];
+}
+
+// Packed Hermite far field for this kernel type and target count?
+template <int KT, int NT>
+__host__ __device__ constexpr bool herm_packed() { return KT != 2 && NT % 2 == 0; }
+
+// q: the staged moments, as {q, q} pairs when herm_packed<KT, NT>().
+template <int KT, int NT>
+__device__ void pc_cluster_herm_dispatch(int np1, const float *x, const float *y, const float *z, const float *g,
+                                         const float *q, float kc, float kp, float *out)
+{
+    switch (np1) {
+#define BT_CASE(N)                                                                                         \
+    case N:                                                                                                \
+        if constexpr (herm_packed<KT, NT>())                                                               \
+            pc_cluster_herm_f2<KT, N, NT>(x, y, z, g, reinterpret_cast<const f2_t *>(q), kc, out);         \
+        else                                                                                               \
+            pc_cluster_herm<KT, N, NT>(x, y, z, g, q, kc, kp, out);                                        \
+        return;
+        BT_CASE(2) BT_CASE(3) BT_CASE(4) BT_CASE(5) BT_CASE(6) BT_CASE(7) BT_CASE(8)
+        BT_CASE(9) BT_CASE(10) BT_CASE(11) BT_CASE(12) BT_CASE(13)
+#undef BT_CASE
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = 0.f;
 }
 
 // Near-field source tile in shared memory, structure of arrays (x', y', z'
@@ -427,7 +507,9 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
             const float *Qs = a.Q32[deg] + (size_t)s * 8 * P;
             for (int i = threadIdx.x; i < 8 * P; i += blockDim.x) {
                 const int m = i / P;
-                q[i] = Qs[i] * (m == 7 ? 15.0f : m >= 4 ? 3.0f : 1.0f);
+                const float v = Qs[i] * (m == 7 ? 15.0f : m >= 4 ? 3.0f : 1.0f);
+                if constexpr (herm_packed<KT, TPT>()) reinterpret_cast<f2_t *>(q)[i] = f2_make(v, v);
+                else q[i] = v;
             }
             __syncthreads();
             pc_cluster_herm_dispatch<KT, TPT>(np1, x, y, z, g, q, kc, (float)a.kp, v);
@@ -621,7 +703,8 @@ int mixed_targets_chunk() { return MX_CHUNK; }
 // kernel (tile_stride) whatever the tile length.
 static size_t mixed_smem(int max_np1, bool herm, int tile_stride)
 {
-    size_t far = sizeof(float) * (size_t)(3 * 16 + (herm ? 8 : 1) * max_np1 * max_np1 * max_np1);
+    // Hermite moments are staged as {q, q} pairs (packed far field)
+    size_t far = sizeof(float) * (size_t)(3 * 16 + (herm ? 16 : 1) * max_np1 * max_np1 * max_np1);
     size_t near = sizeof(float4) * (size_t)tile_stride;
     return far > near ? far : near;
 }
