@@ -78,6 +78,14 @@ constexpr int MX_THREADS = 128;                 // threads of the grid-output ke
 #define BT_MX_BOUNDS __launch_bounds__(MX_THREADS)
 #endif
 constexpr int MX_TILE = 1024;                   // sources per tile of the grid-output kernel
+// Register budget of the 2-targets-per-thread Lagrange particle-output
+// kernel (Coulomb, regularised Coulomb): room for 6 resident blocks per SM.
+// Left to itself the compiler takes 94 registers (5 blocks) for the packed
+// far field, which measured 21 % slower on the 16M system; at 80 registers
+// (a few bytes of spill) it runs 1.4 % faster than the scalar far field.
+#ifndef BT_MX_MIN_BLOCKS_T2
+#define BT_MX_MIN_BLOCKS_T2 6
+#endif
 
 // Far field of one source cluster (degree NP1-1) for NT targets at (x,y,z),
 // relative to the target centre; g = grid coordinates relative to the same
@@ -110,7 +118,11 @@ __device__ __forceinline__ void pc_cluster(const float *x, const float *y, const
             for (int k1 = 0; k1 < NP1; k1++) {
                 float qq = q[j + k1];
 #pragma unroll
-                for (int t = 0; t < NT; t++) row[t] += kf_far<KT>(fmaf(gx[t][k1], gx[t][k1], dyz[t]), qq, kc);
+                for (int t = 0; t < NT; t++) {
+                    const float r2 = fmaf(gx[t][k1], gx[t][k1], dyz[t]);
+                    if (KT == 2) row[t] += kf_far<KT>(r2, qq, kc);
+                    else row[t] = fmaf(qq, rsqrt_apx(KT == 3 ? r2 + kc : r2), row[t]);
+                }
             }
             j += NP1;
 #pragma unroll
@@ -119,20 +131,6 @@ __device__ __forceinline__ void pc_cluster(const float *x, const float *y, const
     }
 #pragma unroll
     for (int t = 0; t < NT; t++) out[t] = s[t] - c[t];
-}
-
-template <int KT, int NT>
-__device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, const float *z, const float *g,
-                                    const float *q, float kc, float *out)
-{
-    switch (np1) {
-#define BT_CASE(N) case N: pc_cluster<KT, N, NT>(x, y, z, g, q, kc, out); return;
-        BT_CASE(2) BT_CASE(3) BT_CASE(4) BT_CASE(5) BT_CASE(6) BT_CASE(7) BT_CASE(8)
-        BT_CASE(9) BT_CASE(10) BT_CASE(11) BT_CASE(12) BT_CASE(13)
-#undef BT_CASE
-    }
-#pragma unroll
-    for (int t = 0; t < NT; t++) out[t] = 0.f;
 }
 
 // Hermite far field of one source cluster for NT targets (FP32; moments
@@ -256,6 +254,61 @@ __device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c)
     return r;
 }
 
+// Lagrange far field with the targets in packed pairs (NT even, Coulomb and
+// regularised Coulomb): pc_cluster's operations lane by lane in f32x2
+// instructions (identical results); qd holds each proxy charge twice.
+template <int KT, int NP1, int NT>
+__device__ __forceinline__ void pc_cluster_f2(const float *x, const float *y, const float *z, const float *g,
+                                              const f2_t *qd, float kc, float *out)
+{
+    constexpr int NPR = NT / 2;
+    f2_t gx[NPR][NP1];
+#pragma unroll
+    for (int p = 0; p < NPR; p++)
+#pragma unroll
+        for (int k = 0; k < NP1; k++) gx[p][k] = f2_make(x[2 * p] - g[k], x[2 * p + 1] - g[k]);
+    float s[NT], c[NT];
+#pragma unroll
+    for (int t = 0; t < NT; t++) { s[t] = 0.f; c[t] = 0.f; }
+    const f2_t kc2 = f2_make(kc, kc), one = f2_make(1.0f, 1.0f), zero = f2_make(0.0f, 0.0f);
+    int j = 0;
+    for (int k3 = 0; k3 < NP1; k3++) {
+        const float gz = g[2 * NP1 + k3];
+        for (int k2 = 0; k2 < NP1; k2++) {
+            const float gy = g[NP1 + k2];
+            f2_t dyz[NPR], row[NPR];
+#pragma unroll
+            for (int p = 0; p < NPR; p++) {
+                const f2_t dy = f2_make(y[2 * p] - gy, y[2 * p + 1] - gy), dz = f2_make(z[2 * p] - gz, z[2 * p + 1] - gz);
+                dyz[p] = f2_fma(dy, dy, f2_mul(dz, dz));
+                row[p] = zero;
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < NP1; k1++) {
+                const f2_t qq = qd[j + k1];
+#pragma unroll
+                for (int p = 0; p < NPR; p++) {
+                    f2_t r2 = f2_fma(gx[p][k1], gx[p][k1], dyz[p]);
+                    if (KT == 3) r2 = f2_fma(one, kc2, r2);
+                    float a, b;
+                    f2_split(r2, a, b);
+                    row[p] = f2_fma(qq, f2_make(rsqrt_apx(a), rsqrt_apx(b)), row[p]);
+                }
+            }
+            j += NP1;
+#pragma unroll
+            for (int p = 0; p < NPR; p++) {
+                float lo, hi;
+                f2_split(row[p], lo, hi);
+                kahan_add(s[2 * p], c[2 * p], lo);
+                kahan_add(s[2 * p + 1], c[2 * p + 1], hi);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = s[t] - c[t];
+}
+
 // Hermite far field with the targets in packed pairs (NT even, Coulomb and
 // regularised Coulomb): the same operations as pc_cluster_herm lane by lane,
 // in f32x2 instructions, so the results are identical and the FMA-pipe work
@@ -325,11 +378,33 @@ __device__ __forceinline__ void pc_cluster_herm_f2(const float *x, const float *
     for (int t = 0; t < NT; t++) out[t] = s[t] - c[t];
 }
 
-// Packed Hermite far field for this kernel type and target count?
+// Packed far field (Lagrange and Hermite) for this kernel type and target count?
 template <int KT, int NT>
-__host__ __device__ constexpr bool herm_packed() { return KT != 2 && NT % 2 == 0; }
+__host__ __device__ constexpr bool far_packed() { return KT != 2 && NT % 2 == 0; }
 
-// q: the staged moments, as {q, q} pairs when herm_packed<KT, NT>().
+// q: the staged proxy charges, as {q, q} pairs when far_packed<KT, NT>().
+template <int KT, int NT>
+__device__ void pc_cluster_dispatch(int np1, const float *x, const float *y, const float *z, const float *g,
+                                    const float *q, float kc, float *out)
+{
+    switch (np1) {
+#define BT_CASE(N)                                                                                         \
+    case N:                                                                                                \
+        if constexpr (far_packed<KT, NT>())                                                                \
+            pc_cluster_f2<KT, N, NT>(x, y, z, g, reinterpret_cast<const f2_t *>(q), kc, out);              \
+        else                                                                                               \
+            pc_cluster<KT, N, NT>(x, y, z, g, q, kc, out);                                                 \
+        return;
+        BT_CASE(2) BT_CASE(3) BT_CASE(4) BT_CASE(5) BT_CASE(6) BT_CASE(7) BT_CASE(8)
+        BT_CASE(9) BT_CASE(10) BT_CASE(11) BT_CASE(12) BT_CASE(13)
+#undef BT_CASE
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) out[t] = 0.f;
+}
+
+
+// q: the staged moments, as {q, q} pairs when far_packed<KT, NT>().
 template <int KT, int NT>
 __device__ void pc_cluster_herm_dispatch(int np1, const float *x, const float *y, const float *z, const float *g,
                                          const float *q, float kc, float kp, float *out)
@@ -337,7 +412,7 @@ __device__ void pc_cluster_herm_dispatch(int np1, const float *x, const float *y
     switch (np1) {
 #define BT_CASE(N)                                                                                         \
     case N:                                                                                                \
-        if constexpr (herm_packed<KT, NT>())                                                               \
+        if constexpr (far_packed<KT, NT>())                                                               \
             pc_cluster_herm_f2<KT, N, NT>(x, y, z, g, reinterpret_cast<const f2_t *>(q), kc, out);         \
         else                                                                                               \
             pc_cluster_herm<KT, N, NT>(x, y, z, g, q, kc, kp, out);                                        \
@@ -508,14 +583,17 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
             for (int i = threadIdx.x; i < 8 * P; i += blockDim.x) {
                 const int m = i / P;
                 const float v = Qs[i] * (m == 7 ? 15.0f : m >= 4 ? 3.0f : 1.0f);
-                if constexpr (herm_packed<KT, TPT>()) reinterpret_cast<f2_t *>(q)[i] = f2_make(v, v);
+                if constexpr (far_packed<KT, TPT>()) reinterpret_cast<f2_t *>(q)[i] = f2_make(v, v);
                 else q[i] = v;
             }
             __syncthreads();
             pc_cluster_herm_dispatch<KT, TPT>(np1, x, y, z, g, q, kc, (float)a.kp, v);
         } else {
             const float *Qs = a.Q32[deg] + (size_t)s * P;
-            for (int i = threadIdx.x; i < P; i += blockDim.x) q[i] = Qs[i];
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                if constexpr (far_packed<KT, TPT>()) reinterpret_cast<f2_t *>(q)[i] = f2_make(Qs[i], Qs[i]);
+                else q[i] = Qs[i];
+            }
             __syncthreads();
             pc_cluster_dispatch<KT, TPT>(np1, x, y, z, g, q, kc, v);
         }
@@ -579,8 +657,7 @@ __device__ __forceinline__ void targets_item(const MixedTargetsArgs &a, const in
 }
 
 template <int KT, bool HERM, int TPT>
-__global__ void __launch_bounds__(MX_CHUNK / TPT)
-k_eval_targets_mixed(MixedTargetsArgs a)
+__device__ __forceinline__ void eval_targets_mixed_body(const MixedTargetsArgs &a)
 {
     extern __shared__ float smf[];
     __shared__ int slot;
@@ -590,6 +667,20 @@ k_eval_targets_mixed(MixedTargetsArgs a)
         if (!a.queue) break;
         w = next_item(a.queue, &slot);
     }
+}
+
+template <int KT, bool HERM, int TPT>
+__global__ void __launch_bounds__(MX_CHUNK / TPT) k_eval_targets_mixed(MixedTargetsArgs a)
+{
+    eval_targets_mixed_body<KT, HERM, TPT>(a);
+}
+
+// The same kernel under the register budget of BT_MX_MIN_BLOCKS_T2 resident
+// blocks (2 targets per thread, Lagrange, Coulomb and regularised Coulomb).
+template <int KT, bool HERM, int TPT>
+__global__ void __launch_bounds__(MX_CHUNK / TPT, BT_MX_MIN_BLOCKS_T2) k_eval_targets_mixed_rb(MixedTargetsArgs a)
+{
+    eval_targets_mixed_body<KT, HERM, TPT>(a);
 }
 
 // Grid-output evaluation (M2L from source clusters + CP from source leaves)
@@ -703,8 +794,8 @@ int mixed_targets_chunk() { return MX_CHUNK; }
 // kernel (tile_stride) whatever the tile length.
 static size_t mixed_smem(int max_np1, bool herm, int tile_stride)
 {
-    // Hermite moments are staged as {q, q} pairs (packed far field)
-    size_t far = sizeof(float) * (size_t)(3 * 16 + (herm ? 16 : 1) * max_np1 * max_np1 * max_np1);
+    // proxy charges are staged as {q, q} pairs (packed far field)
+    size_t far = sizeof(float) * (size_t)(3 * 16 + (herm ? 16 : 2) * max_np1 * max_np1 * max_np1);
     size_t near = sizeof(float4) * (size_t)tile_stride;
     return far > near ? far : near;
 }
@@ -725,9 +816,11 @@ template <int KT, bool HERM, int TPT>
 static void eval_targets_mixed_t(const MixedTargetsArgs &a, cudaStream_t st)
 {
     size_t sm = mixed_smem(a.max_np1, HERM, MX_TILE_MAX);
-    cudaFuncSetAttribute(k_eval_targets_mixed<KT, HERM, TPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int grid = a.queue ? queue_grid(k_eval_targets_mixed<KT, HERM, TPT>, MX_CHUNK / TPT, sm, a.nitems) : a.nitems;
-    k_eval_targets_mixed<KT, HERM, TPT><<<grid, MX_CHUNK / TPT, sm, st>>>(a);
+    auto kernel = k_eval_targets_mixed<KT, HERM, TPT>;
+    if constexpr (TPT == 2 && !HERM && KT != 2) kernel = k_eval_targets_mixed_rb<KT, HERM, TPT>;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int grid = a.queue ? queue_grid(kernel, MX_CHUNK / TPT, sm, a.nitems) : a.nitems;
+    kernel<<<grid, MX_CHUNK / TPT, sm, st>>>(a);
 }
 
 template <int KT, bool HERM>
