@@ -86,6 +86,21 @@ constexpr int MX_TILE = 1024;                   // sources per tile of the grid-
 #ifndef BT_MX_MIN_BLOCKS_T2
 #define BT_MX_MIN_BLOCKS_T2 6
 #endif
+// Yukawa: 6 blocks (80 registers, 24 bytes of spill) measured 2 % faster
+// than the compiler's 96 registers on the 1M cluster-cluster system; for the
+// Hermite kernels 5 blocks measured the same as the compiler's choice.
+#ifndef BT_MX_MIN_BLOCKS_YUK
+#define BT_MX_MIN_BLOCKS_YUK 6
+#endif
+#ifndef BT_MX_MIN_BLOCKS_HERM
+#define BT_MX_MIN_BLOCKS_HERM 0
+#endif
+// resident-block budget of the 2-targets-per-thread kernel (0: the compiler's choice)
+template <int KT, bool HERM>
+__host__ __device__ constexpr int rb_blocks()
+{
+    return HERM ? BT_MX_MIN_BLOCKS_HERM : KT == 2 ? BT_MX_MIN_BLOCKS_YUK : BT_MX_MIN_BLOCKS_T2;
+}
 
 // Far field of one source cluster (degree NP1-1) for NT targets at (x,y,z),
 // relative to the target centre; g = grid coordinates relative to the same
@@ -678,7 +693,7 @@ __global__ void __launch_bounds__(MX_CHUNK / TPT) k_eval_targets_mixed(MixedTarg
 // The same kernel under the register budget of BT_MX_MIN_BLOCKS_T2 resident
 // blocks (2 targets per thread, Lagrange, Coulomb and regularised Coulomb).
 template <int KT, bool HERM, int TPT>
-__global__ void __launch_bounds__(MX_CHUNK / TPT, BT_MX_MIN_BLOCKS_T2) k_eval_targets_mixed_rb(MixedTargetsArgs a)
+__global__ void __launch_bounds__(MX_CHUNK / TPT, rb_blocks<KT, HERM>()) k_eval_targets_mixed_rb(MixedTargetsArgs a)
 {
     eval_targets_mixed_body<KT, HERM, TPT>(a);
 }
@@ -817,7 +832,7 @@ static void eval_targets_mixed_t(const MixedTargetsArgs &a, cudaStream_t st)
 {
     size_t sm = mixed_smem(a.max_np1, HERM, MX_TILE_MAX);
     auto kernel = k_eval_targets_mixed<KT, HERM, TPT>;
-    if constexpr (TPT == 2 && !HERM && KT != 2) kernel = k_eval_targets_mixed_rb<KT, HERM, TPT>;
+    if constexpr (TPT == 2 && rb_blocks<KT, HERM>() > 0) kernel = k_eval_targets_mixed_rb<KT, HERM, TPT>;
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     int grid = a.queue ? queue_grid(kernel, MX_CHUNK / TPT, sm, a.nitems) : a.nitems;
     kernel<<<grid, MX_CHUNK / TPT, sm, st>>>(a);

@@ -95,7 +95,8 @@ def make_inputs(cfg, seed):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms from the
+    warm-up through the timed regions."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -115,6 +116,15 @@ class ClockSampler:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+
+    def wait_first_sample(self, limit_s=5.0):
+        """Block until nvidia-smi has written a sample: its start-up (NVML
+        initialisation) must not overlap a timed region."""
+        t0 = time.perf_counter()
+        while self.proc is not None and time.perf_counter() - t0 < limit_s:
+            if os.path.getsize(self.path) > 0:
+                return
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -387,20 +397,24 @@ def main():
                   "default_ms": next((t["ms"] for t in trials if t["targets_per_thread"] == 2 and
                                       t["source_tile"] == 1024 and t["dispatch"] == B.DISPATCH_GRID), None)}
 
+    # clocks are sampled from the warm-up through both timed regions; the
+    # sampler is started (and has answered once) before the warm-up, because
+    # nvidia-smi's start-up stalls the GPU for tens of milliseconds
+    clocks = ClockSampler(local)
+    clocks.start()
+    clocks.wait_first_sample()
     for _ in range(args.warmup):
         step_device()
         step_host()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
     launches0 = B.kernel_launch_count()
     ms_dev, reps = timed(step_device, args.steps)
     launches = B.kernel_launch_count() - launches0
-    clock_info = clocks.stop()
     torch.cuda.synchronize()
     ms_e2e, _ = timed(step_host, args.steps)
+    clock_info = clocks.stop()
     if world > 1:
         dist.barrier()
     ms_dev, ms_e2e = max_over_ranks([ms_dev, ms_e2e], world, dev)
