@@ -102,11 +102,14 @@ struct DeviceCtx {
 DeviceCtx g_ctx[16];
 std::mutex g_ctx_mu;
 
-// Tile shape and dispatch of the mixed particle-output kernel.
-struct EvalShape {
+// Per-call choices that shape the device sequence: tile shape and dispatch
+// of the mixed particle-output kernel, the upward-pass kernel, and the
+// share of the target leaves this call evaluates.
+struct EvalConfig {
     bool queue = false;
     int tpt = 2, tile = 1024;
     bool tc_up = true;      // leaf P2M of the mixed Lagrange path on the tensor cores
+    int shard = 0, nshards = 1;
 };
 
 // Autotuned shapes per device, kernel and approximation (bt_autotune,
@@ -120,9 +123,9 @@ bool tune_key_ok(int device, int kernel, int approx)
     return device >= 0 && device < 16 && kernel >= 0 && kernel < 16 && approx >= 0 && approx < 3;
 }
 
-EvalShape tuned_shape(int device, int kernel, int approx)
+EvalConfig tuned_shape(int device, int kernel, int approx)
 {
-    EvalShape sh;
+    EvalConfig sh;
     if (!tune_key_ok(device, kernel, approx)) return sh;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (g_has_tuned[device][kernel][approx]) {
@@ -546,6 +549,7 @@ struct DevPlan {
     bool queue = false;     // mixed kernels on a device work queue
     int tpt = 2, tile = 1024;   // tile shape of the mixed particle-output kernel
     bool tc_up = false;         // leaf P2M on the tensor cores (bt_tc.cu)
+    bool sharded = false;       // this call evaluates a share of the target leaves (others get 0)
     int *d_err = nullptr;       // set by a tensor-core kernel whose bounded wait expired
     int n = 0, P = 0, ns = 0, nt = 0, max_np1 = 0, kernel = 0;
     double kp = 0.0;
@@ -790,7 +794,8 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     }
     CK(cudaGetLastError());
     if (ev) CK(record(2));
-    // particle-output evaluation (PC, PP)
+    // particle-output evaluation (PC, PP); a shard leaves the other targets at 0
+    if (nt > 0 && v.sharded) CK(cudaMemsetAsync(d_pot, 0, sizeof(double) * (size_t)nt, st));
     if (nt > 0 && v.ss) {
         bt::SsTargetsArgs a;
         a.n = n; a.nitems = v.n_ev_items; a.items = d_evitems; a.leaf_node = d_tleaves;
@@ -863,7 +868,7 @@ done:
 // execute = false: prepare only (uploads done, the device sequence not
 // issued), for capture into a graph by the caller.
 int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on_device, bt_report *rep,
-             const DevParts *dp = nullptr, const EvalShape &shape = EvalShape(), DevPlan *dv_out = nullptr, bool execute = true,
+             const DevParts *dp = nullptr, const EvalConfig &shape = EvalConfig(), DevPlan *dv_out = nullptr, bool execute = true,
              const SsIn *ss = nullptr)
 {
     const bt_params &o = pl.prm;
@@ -926,6 +931,21 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     // evaluate in FP64
     const bool mixed = o.precision == BT_PRECISION_MIXED && !ssm && (!herm || o.ctype == PARTICLE_CLUSTER) &&
                        o.kernel <= REGULARIZED_COULOMB;
+    if (shape.nshards > 1) {
+        // target sharding: contiguous runs of target leaves (tree order) of
+        // about equal cost; leaf u belongs to the shard that holds the middle
+        // of its cost interval
+        double total = 0.0;
+        for (int u = 0; u < T.nleaves; u++) total += leaf_cost[u];
+        double before = 0.0;
+        for (int u = 0; u < T.nleaves; u++) {
+            const double mid = before + 0.5 * leaf_cost[u];
+            before += leaf_cost[u];
+            int k = total > 0 ? (int)(mid / total * shape.nshards) : u % shape.nshards;
+            if (k >= shape.nshards) k = shape.nshards - 1;
+            if (k != shape.shard) leaf_count[u] = 0;
+        }
+    }
     std::vector<int2> ev_items =
         make_items(T.nleaves, leaf_count.data(), mixed ? bt::mixed_targets_chunk() : 128, leaf_cost);
     std::vector<int2> grid_items, l2p_items;
@@ -1126,6 +1146,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.tpt = shape.tpt;
         v.tile = shape.tile;
         v.tc_up = shape.tc_up && mixed && !herm;
+        v.sharded = shape.nshards > 1;
         v.n = n; v.P = P; v.ns = ns; v.nt = nt; v.max_np1 = max_np1; v.kernel = o.kernel; v.kp = o.kp;
         v.S_n = S.n; v.S_nleaves = S.nleaves; v.S_max_depth = S.max_depth;
         v.T_n = T.n; v.T_nleaves = T.nleaves; v.T_max_depth = T.max_depth;
@@ -1446,7 +1467,7 @@ int static_scratch_arena(int device, Arena **out)
 
 // Checks the options and applies them to prm: precision, learned degree
 // policy and its tolerance, dispatch of the mixed evaluation kernels.
-int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double &tol, EvalShape &shape)
+int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double &tol, EvalConfig &shape)
 {
     if (opts && opts->precision != BT_PRECISION_FP64 && opts->precision != BT_PRECISION_MIXED) {
         set_err("invalid precision %d", opts->precision);
@@ -1478,6 +1499,21 @@ int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double 
     }
     shape = tuned_shape(opts ? opts->device : 0, prm.kernel, prm.approx);
     shape.tc_up = !(opts && opts->upward == BT_UPWARD_FP64);
+    if (opts && opts->shard_count > 1) {
+        if (opts->shard_index < 0 || opts->shard_index >= opts->shard_count) {
+            set_err("shard index %d outside [0, %d)", opts->shard_index, opts->shard_count);
+            return BT_ERR_PARAM;
+        }
+        if (prm.ctype != PARTICLE_CLUSTER) {
+            set_err("target sharding is provided for particle-cluster evaluations");
+            return BT_ERR_UNSUPPORTED;
+        }
+        shape.shard = opts->shard_index;
+        shape.nshards = opts->shard_count;
+    } else if (opts && opts->shard_count < 0) {
+        set_err("invalid shard count %d", opts->shard_count);
+        return BT_ERR_PARAM;
+    }
     if (opts && opts->dispatch == BT_DISPATCH_QUEUE) shape.queue = true;
     if (opts && opts->dispatch == BT_DISPATCH_GRID) shape.queue = false;
     if (learned && (prm.precision != BT_PRECISION_MIXED || prm.ctype != PARTICLE_CLUSTER || prm.approx != LAGRANGE ||
@@ -1510,7 +1546,7 @@ int eval_common(const Systems &sys, const double *tx, const double *ty, const do
     }
     int device = opts ? opts->device : 0;
     bool learned = false;
-    EvalShape shape;
+    EvalConfig shape;
     double tol = 1e-6;
     rc = parse_options(opts, prm, learned, tol, shape);
     if (rc != BT_OK) return rc;
@@ -2250,7 +2286,7 @@ int bt_session_create(int numSystems, const long long *targetOffsets, const long
         return BT_ERR_UNSUPPORTED;
     }
     bool learned = false;
-    EvalShape shape;
+    EvalConfig shape;
     double tol = 1e-6;
     rc = parse_options(opts, prm, learned, tol, shape);
     if (rc != BT_OK) return rc;
@@ -2398,7 +2434,7 @@ int bt_tuning_get(int device, int kernel, int approximation, bt_tuning *t, int *
     if (has) {
         *t = g_tuned[device][kernel][approximation];
     } else {
-        const EvalShape d;
+        const EvalConfig d;
         t->targets_per_thread = d.tpt; t->source_tile = d.tile;
         t->dispatch = d.queue ? BT_DISPATCH_QUEUE : BT_DISPATCH_GRID; t->ms = 0.0f;
     }

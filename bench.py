@@ -231,6 +231,16 @@ def max_over_ranks(ms, world, device):
     return [float(v) for v in t]
 
 
+def combine_shards(pot, world):
+    """Sum the ranks' partial potentials in place (each target is nonzero on
+    exactly one rank): the one collective of a target-sharded system."""
+    if world <= 1:
+        return pot
+    import torch.distributed as dist
+    dist.all_reduce(pot, op=dist.ReduceOp.SUM)
+    return pot
+
+
 def job_throughput(n_per_rank, world, ms_per_step):
     """Whole-job targets/s: every rank evaluates its own system of n_per_rank
     targets (weak scaling), the step lasting as long as the slowest rank."""
@@ -303,6 +313,9 @@ def main():
                     help="mixed evaluation kernels: persistent blocks on a device work queue, or one block per item")
     ap.add_argument("--upward", choices=["auto", "fp64"], default="auto",
                     help="mixed Lagrange upward pass: tensor-core leaf P2M (auto) or FP64 SIMT")
+    ap.add_argument("--shard", action="store_true",
+                    help="strong scaling: all ranks share one system, each evaluates its target shard, "
+                         "one all-reduce combines the potentials (default: one independent system per rank)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default tile shape instead of autotuning it on this workload")
     ap.add_argument("--n", type=int, default=None,
@@ -332,9 +345,13 @@ def main():
     B.lib()
 
     dev = torch.device("cuda", local)
-    x, y, z, q, off = make_inputs(cfg, seed=rank)
+    shard = args.shard and world > 1
+    x, y, z, q, off = make_inputs(cfg, seed=0 if args.shard else rank)
     n = len(x)
     batch = off is not None
+    if shard and batch:
+        raise SystemExit("--shard covers single systems (configurations 1-3 and 5)")
+    ranks_n = n if args.shard else world * n        # targets of the whole job
     prec = B.PRECISION_MIXED if args.precision == "mixed" else B.PRECISION_FP64
     policy = args.degree_policy
     if policy == "auto":
@@ -348,7 +365,8 @@ def main():
                   compute_type=cfg["ctype"], theta=cfg["theta"], degree=cfg["degree"], max_source_leaf=cfg["leaf"],
                   max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=local,
                   dispatch={"auto": B.DISPATCH_AUTO, "queue": B.DISPATCH_QUEUE, "grid": B.DISPATCH_GRID}[args.dispatch],
-                  upward=B.UPWARD_FP64 if args.upward == "fp64" else B.UPWARD_AUTO)
+                  upward=B.UPWARD_FP64 if args.upward == "fp64" else B.UPWARD_AUTO,
+                  shard=(rank, world) if shard else None)
 
     # device-resident inputs (targets are separate arrays with the same coordinates)
     d_in = [torch.from_numpy(a).to(dev) for a in (x, y, z, x.copy(), y.copy(), z.copy(), q)]
@@ -361,14 +379,20 @@ def main():
         return B.treecode_ptr(n, n, *ptrs, out_ptr, inputs_on_device=on_device, **kw)
 
     def step_device():
-        return call([t.data_ptr() for t in d_in[3:6] + d_in[:3] + d_in[6:]], d_out.data_ptr(), True, **common)
+        rep = call([t.data_ptr() for t in d_in[3:6] + d_in[:3] + d_in[6:]], d_out.data_ptr(), True, **common)
+        if shard:
+            combine_shards(d_out, world)
+        return rep
 
     # pinned host buffers for the end-to-end path
     h_in = [torch.from_numpy(a.copy()).pin_memory() for a in (x, y, z, x, y, z, q)]
     h_out = torch.empty(n, dtype=torch.float64).pin_memory()
 
     def step_host():
-        return call([t.data_ptr() for t in h_in[3:6] + h_in[:3] + h_in[6:]], h_out.data_ptr(), False, **common)
+        rep = call([t.data_ptr() for t in h_in[3:6] + h_in[:3] + h_in[6:]], h_out.data_ptr(), False, **common)
+        if shard:
+            h_out.copy_(combine_shards(h_out.to(dev), world).cpu())
+        return rep
 
     def timed(step, k):
         """K steps, each bracketed by CUDA events on the current stream; L2 flushed between steps."""
@@ -452,11 +476,14 @@ def main():
         plain.update(precision=B.PRECISION_FP64, degree_policy=B.DEGREE_FIXED, dispatch=B.DISPATCH_AUTO)
 
         def step_plain():
-            return call([t.data_ptr() for t in d_in[3:6] + d_in[:3] + d_in[6:]], d_out.data_ptr(), True, **plain)
+            rep = call([t.data_ptr() for t in d_in[3:6] + d_in[:3] + d_in[6:]], d_out.data_ptr(), True, **plain)
+            if shard:
+                combine_shards(d_out, world)
+            return rep
         step_plain()
         ms_plain, preps = timed(step_plain, 1)
         (ms_plain,) = max_over_ranks([ms_plain], world, dev)
-        fp64_plain = {"value": world * n / (ms_plain * 1e-3), "unit": "targets/s", "ms_per_step": ms_plain,
+        fp64_plain = {"value": ranks_n / (ms_plain * 1e-3), "unit": "targets/s", "ms_per_step": ms_plain,
                       "steps": 1, "degree": cfg["degree"],
                       "rel_l2_vs_fp64_direct": accuracy(d_out.cpu().numpy())[0],
                       "ms_eval_kernel": preps[-1]["ms_eval_kernel"],
@@ -466,7 +493,7 @@ def main():
     # built once, then per evaluation the charges go host->device, one CUDA
     # graph replays the whole device sequence, potentials come back
     graph = None
-    if not args.no_graph:
+    if not args.no_graph and not shard:
         bounds = off if batch else np.array([0, n])
         systems = [(x[a:b], y[a:b], z[a:b], x[a:b], y[a:b], z[a:b], q[a:b]) for a, b in zip(bounds[:-1], bounds[1:])]
         sess = B.Session(systems, **common)
@@ -493,18 +520,21 @@ def main():
         w = {1: 10.0, 2: 13.0, 3: 11.0}[cfg["kernel"]]
         mufu_per_eval = 2 if cfg["kernel"] == 2 else 1
         sfu = prec == B.PRECISION_MIXED and cfg["approx"] == 1
-        value = job_throughput(n, world, ms_dev / args.steps)
-        e2e = job_throughput(n, world, ms_e2e / args.steps)
+        value = ranks_n / (ms_dev / args.steps * 1e-3)
+        e2e = ranks_n / (ms_e2e / args.steps * 1e-3)
         line = {
             "metric": "targets/s", "value": value, "unit": "targets/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
+            "scaling": "strong" if args.shard else "weak",
             "vs_baseline": None, "dtype": "f64" if prec == B.PRECISION_FP64 else "f32+f64",
             "data": "synthetic (seeded numpy PCG64 with the configuration's distribution)",
             "config": {"workload": cfg["workload"], "config_id": args.config, "precision": args.precision,
                        "degree_policy": policy, "tolerance": args.tolerance, "dispatch": args.dispatch,
                        "tile_shape": tuning, "upward": args.upward,
                        "l2": "flushed between steps (256 MB write)",
-                       "parallelism": f"{world} independent " + ("batch(es)" if batch else "system(s)") + ", one per GPU",
+                       "parallelism": (f"one system, target shards over {world} GPU(s), one all-reduce of the "
+                                       "potentials" if args.shard else
+                                       f"{world} independent " + ("batch(es)" if batch else "system(s)") + ", one per GPU"),
                        "systems": len(off) - 1 if batch else 1,
                        "rel_l2_vs_fp64_direct": rel_l2, "rel_max_vs_fp64_direct": rel_max,
                        "direct_sample_targets": n_checked},

@@ -102,6 +102,13 @@ typedef struct bt_options {
     int upward;           /* mixed Lagrange upward pass: BT_UPWARD_AUTO (default: leaf
                              P2M on the tensor cores in 3xTF32 where (n+1)^2 <= 128)
                              or BT_UPWARD_FP64 (FP64 SIMT, as the FP64 path)         */
+    /* Target sharding (particle-cluster): with shard_count > 1 the call
+     * evaluates shard_index's share of the target leaves (contiguous in tree
+     * order, equal estimated cost) and leaves the other potentials 0; the sum
+     * of the outputs of all shards is the unsharded result, bit for bit.
+     * Trees, lists and proxies are built in full by every shard.            */
+    int shard_index;
+    int shard_count;
 } bt_options;
 
 enum { BT_TREE_GPU = 0, BT_TREE_HOST = 1 };

@@ -1,0 +1,60 @@
+"""GPU tests of target sharding (bt_options.shard_index / shard_count), the
+multi-GPU decomposition of one particle-cluster system: every shard builds
+the trees, lists and proxies, evaluates a contiguous run of target leaves of
+about equal cost and leaves the other potentials 0, so one all-reduce (sum)
+over the shards gives the result.  Here the shards run one after another on
+one GPU: their sum must equal the unsharded potentials bit for bit, every
+target must come from exactly one shard, and the shards' costs must be
+balanced."""
+import numpy as np
+import pytest
+
+import barytree_b200 as B
+from conftest import uniform_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _clustered(n, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-0.6, 0.6, (4, 3))
+    pts = np.concatenate([rng.normal(c[k], 0.12, (n // 5, 3)) for k in range(4)] + [rng.uniform(-1, 1, (n // 5, 3))])
+    pts = np.clip(pts, -1, 1)
+    return pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy(), rng.uniform(-1, 1, len(pts))
+
+
+@pytest.mark.parametrize("precision,nshards", [(B.PRECISION_FP64, 2), (B.PRECISION_MIXED, 3), (B.PRECISION_MIXED, 4)])
+def test_sum_of_shards_is_the_unsharded_result(precision, nshards):
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(31, 120000, targets="other")
+    kw = dict(theta=0.7, degree=6, max_source_leaf=500, max_target_leaf=500, size_check=1.0, precision=precision)
+    full = B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw)
+    parts = [B.treecode(tx, ty, tz, sx, sy, sz, sq, shard=(k, nshards), **kw) for k in range(nshards)]
+    assert np.array_equal(np.sum(parts, axis=0), full)
+    nonzero = np.array([p != 0 for p in parts])
+    assert np.all(nonzero.sum(axis=0) == 1)          # every target from exactly one shard
+    counts = nonzero.sum(axis=1)
+    assert counts.min() > 0.5 * len(tx) / nshards    # balanced (uniform inputs: cost ~ targets)
+
+
+def test_sharded_learned_degrees_and_sessions():
+    from barytree_b200 import selector
+    selector.install_default()
+    x, y, z, q = _clustered(300000, 32)
+    kw = dict(theta=0.7, degree=10, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
+              precision=B.PRECISION_MIXED, degree_policy=B.DEGREE_LEARNED, tolerance=1e-6)
+    full = B.treecode(x, y, z, x, y, z, q, **kw)
+    parts = [B.treecode(x, y, z, x, y, z, q, shard=(k, 2), **kw) for k in range(2)]
+    assert np.array_equal(parts[0] + parts[1], full)
+    sparts = []
+    for k in range(2):
+        s = B.Session([(x, y, z, x, y, z, q)], shard=(k, 2), **kw)
+        sparts.append(s.evaluate(q)[0])
+        s.close()
+    assert np.array_equal(sparts[0] + sparts[1], full)
+
+
+def test_one_shard_is_the_unsharded_call():
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(33, 50000)
+    kw = dict(theta=0.7, degree=5, max_source_leaf=400, max_target_leaf=400, precision=B.PRECISION_MIXED)
+    assert np.array_equal(B.treecode(tx, ty, tz, sx, sy, sz, sq, shard=(0, 1), **kw),
+                          B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw))

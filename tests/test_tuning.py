@@ -67,3 +67,14 @@ def test_invalid_upward_option_is_a_parameter_error():
     with pytest.raises(B.BaryTreeError) as e:
         B.treecode(x, y, z, x, y, z, q, precision=B.PRECISION_MIXED, upward=7)
     assert e.value.code == B.BT_ERR_PARAM and "upward" in B.last_error()
+
+
+def test_shard_arguments_are_checked_before_any_device_use():
+    rng = np.random.default_rng(2)
+    x, y, z, q = (rng.uniform(-1, 1, 60) for _ in range(4))
+    with pytest.raises(B.BaryTreeError) as e:
+        B.treecode(x, y, z, x, y, z, q, precision=B.PRECISION_MIXED, shard=(3, 3))
+    assert e.value.code == B.BT_ERR_PARAM
+    with pytest.raises(B.BaryTreeError) as e:
+        B.treecode(x, y, z, x, y, z, q, compute_type=B.ComputeType.CLUSTER_CLUSTER, shard=(0, 2))
+    assert e.value.code == B.BT_ERR_UNSUPPORTED
