@@ -399,16 +399,19 @@ class Session:
 
 def autotune(systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
              compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
-             max_target_leaf=2000, size_check=1.0, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0):
+             max_target_leaf=2000, size_check=1.0, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0,
+             upward=UPWARD_AUTO, shard=None):
     """bt_autotune: times the mixed particle-output kernel's 18 tile shapes on
     this workload (a list of systems (tx, ty, tz, sx, sy, sz, sq), as for
-    Session) and installs the fastest for (device, kernel, approximation).
-    Returns (best, trials) as dicts."""
+    Session; with shard, on that target shard's work) and installs the
+    fastest for (device, kernel, approximation).  Returns (best, trials) as
+    dicts."""
     systems = [tuple(map(_c, s)) for s in systems]
     toff = np.concatenate([[0], np.cumsum([len(s[0]) for s in systems])]).astype(np.int64)
     soff = np.concatenate([[0], np.cumsum([len(s[3]) for s in systems])]).astype(np.int64)
     cat = [_c(np.concatenate([s[i] for s in systems])) for i in range(7)]
-    opts = Options(PRECISION_MIXED, int(degree_policy), float(tolerance), int(device), 0, TREE_GPU, DISPATCH_AUTO)
+    opts = Options(PRECISION_MIXED, int(degree_policy), float(tolerance), int(device), 0, TREE_GPU, DISPATCH_AUTO,
+                   int(upward), *_shard(shard))
     best = Tuning()
     trials = (Tuning * 32)()
     nt = ctypes.c_int(0)

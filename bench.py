@@ -295,7 +295,7 @@ def run_reference_arm(args, cfg, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def main():
+def make_parser():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -321,7 +321,30 @@ def main():
     ap.add_argument("--n", type=int, default=None,
                     help="particles (default: the configuration's N); smaller systems of the same "
                          "distribution for profiling captures")
-    args = ap.parse_args()
+    return ap
+
+
+def eval_kwargs(B, cfg, args, policy, device, shard):
+    """Keyword arguments of every library call of one run (treecode_ptr,
+    treecode_batch_ptr, Session, autotune)."""
+    prec = B.PRECISION_MIXED if args.precision == "mixed" else B.PRECISION_FP64
+    return dict(degree_policy=B.DEGREE_LEARNED if policy == "learned" else B.DEGREE_FIXED,
+                tolerance=args.tolerance,
+                kernel=cfg["kernel"], kernel_param=cfg["kp"], approximation=cfg["approx"],
+                compute_type=cfg["ctype"], theta=cfg["theta"], degree=cfg["degree"], max_source_leaf=cfg["leaf"],
+                max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=device,
+                dispatch={"auto": B.DISPATCH_AUTO, "queue": B.DISPATCH_QUEUE, "grid": B.DISPATCH_GRID}[args.dispatch],
+                upward=B.UPWARD_FP64 if args.upward == "fp64" else B.UPWARD_AUTO,
+                shard=shard)
+
+
+def autotune_kwargs(common):
+    """The autotuner takes the run's arguments except precision (always mixed) and dispatch (tuned)."""
+    return {k: v for k, v in common.items() if k not in ("precision", "dispatch")}
+
+
+def main():
+    args = make_parser().parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.n:
         cfg["n_override"] = args.n
@@ -359,14 +382,7 @@ def main():
     if policy == "learned":
         from barytree_b200 import selector
         selector.install_default()
-    common = dict(degree_policy=B.DEGREE_LEARNED if policy == "learned" else B.DEGREE_FIXED,
-                  tolerance=args.tolerance,
-                  kernel=cfg["kernel"], kernel_param=cfg["kp"], approximation=cfg["approx"],
-                  compute_type=cfg["ctype"], theta=cfg["theta"], degree=cfg["degree"], max_source_leaf=cfg["leaf"],
-                  max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=local,
-                  dispatch={"auto": B.DISPATCH_AUTO, "queue": B.DISPATCH_QUEUE, "grid": B.DISPATCH_GRID}[args.dispatch],
-                  upward=B.UPWARD_FP64 if args.upward == "fp64" else B.UPWARD_AUTO,
-                  shard=(rank, world) if shard else None)
+    common = eval_kwargs(B, cfg, args, policy, local, (rank, world) if shard else None)
 
     # device-resident inputs (targets are separate arrays with the same coordinates)
     d_in = [torch.from_numpy(a).to(dev) for a in (x, y, z, x.copy(), y.copy(), z.copy(), q)]
@@ -415,8 +431,7 @@ def main():
         t0 = time.perf_counter()
         systems = ([(x[a:b], y[a:b], z[a:b], x[a:b], y[a:b], z[a:b], q[a:b]) for a, b in zip(off[:-1], off[1:])]
                    if batch else [(x, y, z, x, y, z, q)])
-        tune_kw = {k: v for k, v in common.items() if k not in ("precision", "dispatch", "upward")}
-        best, trials = B.autotune(systems, **tune_kw)
+        best, trials = B.autotune(systems, **autotune_kwargs(common))
         tuning = {"best": best, "trials": len(trials), "seconds": round(time.perf_counter() - t0, 2),
                   "default_ms": next((t["ms"] for t in trials if t["targets_per_thread"] == 2 and
                                       t["source_tile"] == 1024 and t["dispatch"] == B.DISPATCH_GRID), None)}
