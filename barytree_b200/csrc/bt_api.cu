@@ -565,6 +565,10 @@ struct DevPlan {
     unsigned char *d_mxdflag = nullptr, *d_adeg = nullptr;
     double *d_xgrid[BT_MAX_DEGREE + 1] = {}, *d_xQ[BT_MAX_DEGREE + 1] = {};
     float *d_xQ32[BT_MAX_DEGREE + 1] = {};
+    // extra degree i: the leaves and per-level internal nodes that need its proxies
+    int *d_xleaves[BT_MAX_DEGREE + 1] = {}, *d_xlvl[BT_MAX_DEGREE + 1] = {};
+    std::vector<int> xleaf_n;
+    std::vector<std::vector<int>> xlvl_off;
     double *d_out = nullptr;    // potentials in caller order (run_plan's own buffer)
     bool ss = false;                        // singularity subtraction
     double kp2 = 0.0, ss_c = 0.0;           // kernel_params[1]; correction constant
@@ -743,17 +747,21 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         // proxy charges at the other degrees chosen per interaction
         for (size_t i = 0; i < xdeg.size(); i++) {
             const int d = xdeg[i];
-            if (v.tc_up && bt::p2m_tc_supported(d))
-                bt::launch_p2m_tc(d, v.S_nleaves, d_sleaves, d_sibeg, d_snum, d_xgrid[i], d_sx, d_sy, d_sz, d_sq,
-                                  d_xQ[i], v.d_err, st);
-            else
-                bt::launch_p2m(d, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww,
-                               d_sx, d_sy, d_sz, d_sq, d_xQ[i], st);
-            launches++;
+            const int nl = v.xleaf_n[i];
+            if (nl > 0) {
+                if (v.tc_up && bt::p2m_tc_supported(d))
+                    bt::launch_p2m_tc(d, nl, v.d_xleaves[i], d_sibeg, d_snum, d_xgrid[i], d_sx, d_sy, d_sz, d_sq,
+                                      d_xQ[i], v.d_err, st);
+                else
+                    bt::launch_p2m(d, false, nl, v.d_xleaves[i], v.S_n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww,
+                                   d_sx, d_sy, d_sz, d_sq, d_xQ[i], st);
+                launches++;
+            }
+            const std::vector<int> &lo = v.xlvl_off[i];
             for (int l = v.S_max_depth - 1; l >= 0; l--) {
-                int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
+                int cnt = lo[l + 1] - lo[l];
                 if (cnt > 0) {
-                    bt::launch_m2m(d, cnt, d_slvl + v.S_lvl_off[l], d_snch, d_sch, d_xgrid[i], d_xQ[i], st);
+                    bt::launch_m2m(d, cnt, v.d_xlvl[i] + lo[l], d_snch, d_sch, d_xgrid[i], d_xQ[i], st);
                     launches++;
                 }
             }
@@ -898,6 +906,38 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         xgrid.resize(xdeg.size());
         std::vector<double> tmp;
         for (size_t i = 0; i < xdeg.size(); i++) fill_grids(S, xdeg[i], xgrid[i], tmp);
+    }
+    // Each extra degree needs proxies only at the source nodes some
+    // interaction uses it for: its P2M and M2M run over the leaves and
+    // internal nodes under those nodes (pre-order numbering: a node's
+    // children come after it, so one forward sweep marks the subtrees).
+    std::vector<std::vector<int>> xleaves(xdeg.size()), xlvl(xdeg.size()), xlvl_off(xdeg.size());
+    if (!xdeg.empty() && S.n > 0) {
+        const size_t X = xdeg.size();
+        int slot[BT_MAX_DEGREE + 1];
+        for (int d = 0; d <= BT_MAX_DEGREE; d++) slot[d] = -1;
+        for (size_t i = 0; i < X; i++) slot[xdeg[i]] = (int)i;
+        std::vector<unsigned char> need((size_t)S.n * X, 0);
+        for (int64_t k = 0; k < n_approx; k++) {
+            const int sl = slot[pl.a_deg[k]];
+            if (sl >= 0) need[(size_t)pl.t_approx.idx[k] * X + sl] = 1;
+        }
+        for (int v = 0; v < S.n; v++)
+            for (int c = 0; c < S.nchild[v]; c++) {
+                const int ch = S.child[8 * (size_t)v + c];
+                for (size_t i = 0; i < X; i++) need[(size_t)ch * X + i] |= need[(size_t)v * X + i];
+            }
+        for (size_t i = 0; i < X; i++) {
+            for (int u = 0; u < S.nleaves; u++)
+                if (need[(size_t)S.leaves[u] * X + i]) xleaves[i].push_back(S.leaves[u]);
+            xlvl_off[i].assign(S.max_depth + 1, 0);
+            for (int l = 0; l < S.max_depth; l++) {
+                if (S.lvl_off)
+                    for (int k = S.lvl_off[l]; k < S.lvl_off[l + 1]; k++)
+                        if (need[(size_t)S.lvl_nodes[k] * X + i]) xlvl[i].push_back(S.lvl_nodes[k]);
+                xlvl_off[i][l + 1] = (int)xlvl[i].size();
+            }
+        }
     }
     int max_np1 = n + 1;
     for (int d : xdeg) max_np1 = std::max(max_np1, d + 1);
@@ -1063,6 +1103,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     double *d_xgrid[BT_MAX_DEGREE + 1] = {}, *d_xQ[BT_MAX_DEGREE + 1] = {};
     double *d_srad = nullptr, *d_trad = nullptr;
     float *d_xQ32[BT_MAX_DEGREE + 1] = {};
+    int *d_xleaves[BT_MAX_DEGREE + 1] = {}, *d_xlvl[BT_MAX_DEGREE + 1] = {};
     if (mixed) {
         L.add(&d_spos, ns); L.add(&d_tpos, nt);
         if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P * nq);
@@ -1076,6 +1117,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             L.add(&d_xgrid[i], xgrid[i].size());
             L.add(&d_xQ[i], (size_t)S.n * Pd);
             L.add(&d_xQ32[i], (size_t)S.n * Pd);
+            L.add(&d_xleaves[i], xleaves[i].size());
+            L.add(&d_xlvl[i], xlvl[i].size());
         }
     }
 
@@ -1135,7 +1178,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             UP(d_mxdflag, mx_dflag.data(), mx_dflag.size());
             if (pl.a_deg) UP(d_adeg, pl.a_deg, n_approx);
             UP(d_srad, S.rad, S.n); UP(d_trad, T.rad, T.n);
-            for (size_t i = 0; i < xdeg.size(); i++) UP(d_xgrid[i], xgrid[i].data(), xgrid[i].size());
+            for (size_t i = 0; i < xdeg.size(); i++) {
+                UP(d_xgrid[i], xgrid[i].data(), xgrid[i].size());
+                UP(d_xleaves[i], xleaves[i].data(), xleaves[i].size());
+                UP(d_xlvl[i], xlvl[i].data(), xlvl[i].size());
+            }
             UP(d_mxcpoff, mx_cpoff.data(), mx_cpoff.size()); UP(d_mxcpidx, mx_cpidx.data(), mx_cpidx.size());
         }
 #undef UP
@@ -1215,7 +1262,12 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.d_Q32 = d_Q32;
         v.d_mxdflag = d_mxdflag;
         v.d_adeg = d_adeg;
-        for (int k = 0; k <= BT_MAX_DEGREE; k++) { v.d_xgrid[k] = d_xgrid[k]; v.d_xQ[k] = d_xQ[k]; v.d_xQ32[k] = d_xQ32[k]; }
+        for (int k = 0; k <= BT_MAX_DEGREE; k++) {
+            v.d_xgrid[k] = d_xgrid[k]; v.d_xQ[k] = d_xQ[k]; v.d_xQ32[k] = d_xQ32[k];
+            v.d_xleaves[k] = d_xleaves[k]; v.d_xlvl[k] = d_xlvl[k];
+        }
+        for (size_t i = 0; i < xdeg.size(); i++) v.xleaf_n.push_back((int)xleaves[i].size());
+        v.xlvl_off = xlvl_off;
         if (dv_out) {
             *dv_out = v;
             dv_out->d_out = d_out;

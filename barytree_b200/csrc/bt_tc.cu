@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "bt_kernels.cuh"
 #include "bt_tc.h"
@@ -47,6 +48,7 @@ constexpr int TC_KSTEPS = TC_KC / 8;       // one tcgen05.mma (kind::tf32) cover
 constexpr int TC_MAXNP1 = 11;              // (n+1)^2 <= 128
 constexpr uint32_t TC_TMEM_COLS = 32;      // accumulators: hi*hi in columns 0-15, cross products in 16-31
 constexpr long long TC_WAIT_LIMIT = 1LL << 22;
+constexpr long long TC_TEST_WAIT_LIMIT = 1LL << 10;   // the failure-path test's wait
 
 // Shared-memory layout (bytes).  A tile: 128 rows x 32 tf32; B tile: 16 x 32.
 constexpr uint32_t A_BYTES = TC_M * TC_KC * 4;                  // 16 KB
@@ -117,9 +119,9 @@ __device__ __forceinline__ void mma_commit(uint32_t bar)
 }
 
 // Bounded wait for the completion of phase `parity` of an mbarrier.
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity)
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, long long limit = TC_WAIT_LIMIT)
 {
-    for (long long it = 0; it < TC_WAIT_LIMIT; it++) {
+    for (long long it = 0; it < limit; it++) {
         uint32_t done;
         asm volatile(
             "{\n\t"
@@ -139,7 +141,8 @@ template <int NP1>
 __global__ void __launch_bounds__(TC_THREADS)
 k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int *__restrict__ numpar,
          const double *__restrict__ grid, const double *__restrict__ sx, const double *__restrict__ sy,
-         const double *__restrict__ sz, const double *__restrict__ sq, double *__restrict__ Q, int *err)
+         const double *__restrict__ sz, const double *__restrict__ sq, double *__restrict__ Q, int *err,
+         int expire_test)
 {
     constexpr int n = NP1 - 1, ROWS = NP1 * NP1, P = ROWS * NP1;
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -179,6 +182,14 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
     bool ok = true;
     const uint32_t bar_a = smem_addr(bar);
     uint32_t wpar = 0;                         // parity of the last wait (repeated once if it expired)
+    if (expire_test) {
+        // failure-path test: wait, before any MMA is issued, on a phase that
+        // nothing completes; the bounded wait expires and the kernel takes
+        // its error exit
+        if (t == 0) misc[1] = bar_wait(bar_a, 0u, TC_TEST_WAIT_LIMIT) ? 1u : 0u;
+        __syncthreads();
+        ok = misc[1] != 0;
+    }
     // chunk c: products hi*hi into accumulator columns 0-15 and the two
     // cross products into columns 16-31, from zero (short FP32 sums on the
     // tensor core); once its MMAs have completed the threads fold the chunk
@@ -284,7 +295,7 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
     } else if (t == 0) {
         atomicExch(err, 1);
         // one more bounded wait for the MMAs in flight before the memory is released
-        bar_wait(bar_a, wpar);
+        if (!expire_test) bar_wait(bar_a, wpar);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -299,8 +310,12 @@ void p2m_tc_t(int nleaves, const int *leaves, const int *ibeg, const int *numpar
               const double *sx, const double *sy, const double *sz, const double *sq, double *Q, int *err,
               cudaStream_t st)
 {
+    // BARYTREE_B200_TEST_EXPIRE_TC_WAIT=1 makes every block's first wait run
+    // out (no MMA in flight), to test the timeout path end to end
+    const int expire_now = getenv("BARYTREE_B200_TEST_EXPIRE_TC_WAIT") != nullptr;
     cudaFuncSetAttribute(k_p2m_tc<NP1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
-    k_p2m_tc<NP1><<<nleaves, TC_THREADS, TC_SMEM, st>>>(leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err);
+    k_p2m_tc<NP1><<<nleaves, TC_THREADS, TC_SMEM, st>>>(leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err,
+                                                          expire_now);
 }
 
 }  // namespace

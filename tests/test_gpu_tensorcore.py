@@ -74,3 +74,19 @@ def test_tensor_core_p2m_with_learned_degrees_and_sessions():
     (s_out,) = sess.evaluate(q)
     sess.close()
     assert np.array_equal(s_out, tc)
+
+
+def test_expired_tensor_core_wait_is_reported_and_the_context_survives(monkeypatch):
+    """Failure path without a fault: with BARYTREE_B200_TEST_EXPIRE_TC_WAIT
+    set, every block of the tensor-core P2M waits (bounded) on an mbarrier
+    phase that nothing completes, before issuing any MMA; the call must
+    return BT_ERR_TIMEOUT, and the next call must work."""
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(24, 20000)
+    kw = dict(theta=0.7, degree=6, max_source_leaf=400, max_target_leaf=400, precision=B.PRECISION_MIXED)
+    good = B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw)
+    monkeypatch.setenv("BARYTREE_B200_TEST_EXPIRE_TC_WAIT", "1")
+    with pytest.raises(B.BaryTreeError) as e:
+        B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw)
+    assert e.value.code == B.BT_ERR_TIMEOUT and "tensor-core wait expired" in B.last_error()
+    monkeypatch.delenv("BARYTREE_B200_TEST_EXPIRE_TC_WAIT")
+    assert np.array_equal(B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw), good)
