@@ -67,6 +67,7 @@ DEGREE_FIXED, DEGREE_LEARNED = 0, 1
 TREE_GPU, TREE_HOST = 0, 1
 DISPATCH_AUTO, DISPATCH_QUEUE, DISPATCH_GRID = 0, 1, 2
 UPWARD_AUTO, UPWARD_FP64 = 0, 1
+SYMMETRY_AUTO, SYMMETRY_OFF = 0, 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -77,7 +78,7 @@ class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("degree_policy", ctypes.c_int), ("tolerance", ctypes.c_double),
                 ("device", ctypes.c_int), ("inputs_on_device", ctypes.c_int), ("tree_build", ctypes.c_int),
                 ("dispatch", ctypes.c_int), ("upward", ctypes.c_int), ("shard_index", ctypes.c_int),
-                ("shard_count", ctypes.c_int)]
+                ("shard_count", ctypes.c_int), ("symmetry", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):
@@ -291,7 +292,7 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
              theta=0.7, degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
              precision=PRECISION_FP64, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0,
              tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, return_report=False,
-             singularity=Singularity.SKIPPING, target_q=None, source_w=None, beta=-1.0, upward=UPWARD_AUTO, shard=None):
+             singularity=Singularity.SKIPPING, target_q=None, source_w=None, beta=-1.0, upward=UPWARD_AUTO, shard=None, symmetry=SYMMETRY_AUTO):
     """Extended entry point (bt_eval_ex): options for precision / degree policy /
     tree build and a report.  kernel_param may be a sequence (two parameters
     for regularized Coulomb/Yukawa, atan, MQ); singularity subtraction takes
@@ -301,7 +302,7 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
     sw = _c(source_w) if source_w is not None else None
     kp = _c(np.atleast_1d(np.asarray(kernel_param, dtype=np.float64)))
     out = np.zeros(len(tx))
-    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, int(tree_build), int(dispatch), int(upward), *_shard(shard))
+    opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, int(tree_build), int(dispatch), int(upward), *_shard(shard), int(symmetry))
     rep = Report()
     rc = lib().bt_eval_ex(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(tq), _p(sx), _p(sy), _p(sz), _p(sq), _p(sw),
                           _p(out), int(kernel), len(kp), _p(kp), int(singularity), int(approximation),
@@ -314,7 +315,7 @@ def treecode(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0
 def treecode_batch(systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
                    compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
                    max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64, degree_policy=DEGREE_FIXED,
-                   tolerance=1e-6, device=0, tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, return_report=False, upward=UPWARD_AUTO, shard=None):
+                   tolerance=1e-6, device=0, tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, return_report=False, upward=UPWARD_AUTO, shard=None, symmetry=SYMMETRY_AUTO):
     """bt_eval_batch over a list of systems (tx, ty, tz, sx, sy, sz, sq); returns one potential array per system."""
     systems = [tuple(map(_c, s)) for s in systems]
     toff = np.concatenate([[0], np.cumsum([len(s[0]) for s in systems])]).astype(np.int64)
@@ -326,7 +327,7 @@ def treecode_batch(systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximati
                              compute_type=compute_type, theta=theta, degree=degree, max_source_leaf=max_source_leaf,
                              max_target_leaf=max_target_leaf, size_check=size_check, precision=precision,
                              degree_policy=degree_policy, tolerance=tolerance, device=device, tree_build=tree_build,
-                             dispatch=dispatch, upward=upward, shard=shard)
+                             dispatch=dispatch, upward=upward, shard=shard, symmetry=symmetry)
     pots = [out[toff[k]:toff[k + 1]].copy() for k in range(len(systems))]
     return (pots, rep) if return_report else pots
 
@@ -336,13 +337,13 @@ def treecode_batch_ptr(nsys, target_offsets, source_offsets, tx, ty, tz, sx, sy,
                        compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
                        max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64, degree_policy=DEGREE_FIXED,
                        tolerance=1e-6, device=0, inputs_on_device=False, tree_build=TREE_GPU,
-                       dispatch=DISPATCH_AUTO, upward=UPWARD_AUTO, shard=None):
+                       dispatch=DISPATCH_AUTO, upward=UPWARD_AUTO, shard=None, symmetry=SYMMETRY_AUTO):
     """bt_eval_batch on raw addresses; offsets are host int64 arrays of nsys+1 entries."""
     cast = lambda a: ctypes.cast(ctypes.c_void_p(int(a)), _dp)  # noqa: E731
     toff = np.ascontiguousarray(target_offsets, dtype=np.int64)
     soff = np.ascontiguousarray(source_offsets, dtype=np.int64)
     opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), int(bool(inputs_on_device)),
-                   int(tree_build), int(dispatch), int(upward), *_shard(shard))
+                   int(tree_build), int(dispatch), int(upward), *_shard(shard), int(symmetry))
     rep = Report()
     rc = lib().bt_eval_batch(int(nsys), toff.ctypes.data_as(_llp), soff.ctypes.data_as(_llp), cast(tx), cast(ty),
                              cast(tz), cast(sx), cast(sy), cast(sz), cast(sq), cast(out), int(kernel),
@@ -363,12 +364,12 @@ class Session:
     def __init__(self, systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
                  compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
                  max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64, degree_policy=DEGREE_FIXED,
-                 tolerance=1e-6, device=0, dispatch=DISPATCH_AUTO, upward=UPWARD_AUTO, shard=None):
+                 tolerance=1e-6, device=0, dispatch=DISPATCH_AUTO, upward=UPWARD_AUTO, shard=None, symmetry=SYMMETRY_AUTO):
         systems = [tuple(map(_c, s)) for s in systems]
         self.toff = np.concatenate([[0], np.cumsum([len(s[0]) for s in systems])]).astype(np.int64)
         self.soff = np.concatenate([[0], np.cumsum([len(s[3]) for s in systems])]).astype(np.int64)
         cat = [_c(np.concatenate([s[i] for s in systems])) for i in range(7)]
-        opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, TREE_GPU, int(dispatch), int(upward), *_shard(shard))
+        opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), 0, TREE_GPU, int(dispatch), int(upward), *_shard(shard), int(symmetry))
         h = ctypes.c_void_p()
         rc = lib().bt_session_create(len(systems), self.toff.ctypes.data_as(_llp), self.soff.ctypes.data_as(_llp),
                                      *(_p(a) for a in cat), int(kernel), float(kernel_param), int(approximation),
@@ -400,7 +401,7 @@ class Session:
 def autotune(systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=Approximation.LAGRANGE,
              compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7, degree=8, max_source_leaf=2000,
              max_target_leaf=2000, size_check=1.0, degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0,
-             upward=UPWARD_AUTO, shard=None):
+             upward=UPWARD_AUTO, shard=None, symmetry=SYMMETRY_AUTO):
     """bt_autotune: times the mixed particle-output kernel's 18 tile shapes on
     this workload (a list of systems (tx, ty, tz, sx, sy, sz, sq), as for
     Session; with shard, on that target shard's work) and installs the
@@ -411,7 +412,7 @@ def autotune(systems, kernel=Kernel.COULOMB, kernel_param=0.0, approximation=App
     soff = np.concatenate([[0], np.cumsum([len(s[3]) for s in systems])]).astype(np.int64)
     cat = [_c(np.concatenate([s[i] for s in systems])) for i in range(7)]
     opts = Options(PRECISION_MIXED, int(degree_policy), float(tolerance), int(device), 0, TREE_GPU, DISPATCH_AUTO,
-                   int(upward), *_shard(shard))
+                   int(upward), *_shard(shard), int(symmetry))
     best = Tuning()
     trials = (Tuning * 32)()
     nt = ctypes.c_int(0)
@@ -469,11 +470,11 @@ def treecode_ptr(nt, ns, tx, ty, tz, sx, sy, sz, sq, out, kernel=Kernel.COULOMB,
                  approximation=Approximation.LAGRANGE, compute_type=ComputeType.PARTICLE_CLUSTER, theta=0.7,
                  degree=8, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0, precision=PRECISION_FP64,
                  degree_policy=DEGREE_FIXED, tolerance=1e-6, device=0, inputs_on_device=False,
-                 tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, upward=UPWARD_AUTO, shard=None):
+                 tree_build=TREE_GPU, dispatch=DISPATCH_AUTO, upward=UPWARD_AUTO, shard=None, symmetry=SYMMETRY_AUTO):
     """bt_eval on raw addresses (ints): device pointers when inputs_on_device, else host pointers."""
     cast = lambda a: ctypes.cast(ctypes.c_void_p(int(a)), _dp)  # noqa: E731
     opts = Options(int(precision), int(degree_policy), float(tolerance), int(device), int(bool(inputs_on_device)),
-                   int(tree_build), int(dispatch), int(upward), *_shard(shard))
+                   int(tree_build), int(dispatch), int(upward), *_shard(shard), int(symmetry))
     rep = Report()
     rc = lib().bt_eval(int(nt), int(ns), cast(tx), cast(ty), cast(tz), cast(sx), cast(sy), cast(sz), cast(sq),
                        cast(out), int(kernel), float(kernel_param), int(approximation), int(compute_type),

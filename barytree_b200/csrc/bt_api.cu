@@ -29,6 +29,7 @@
 #include "bt_gputree.h"
 #include "bt_ss.h"
 #include "bt_tc.h"
+#include "bt_sym.h"
 #include "bt_host.h"
 
 namespace {
@@ -110,6 +111,7 @@ struct EvalConfig {
     int tpt = 2, tile = 1024;
     bool tc_up = true;      // leaf P2M of the mixed Lagrange path on the tensor cores
     int shard = 0, nshards = 1;
+    bool sym = true;        // symmetric near-field pairs once for both sides (bt_sym.cu)
 };
 
 // Autotuned shapes per device, kernel and approximation (bt_autotune,
@@ -449,6 +451,7 @@ void build_plan(bt_plan &pl, const Systems &sys, const double *tx, const double 
         bt_parts_init(&pl.tgt, nt, pl.src.x, pl.src.y, pl.src.z, nullptr);
         memcpy(pl.tgt.order, pl.src.order, sizeof(int) * (size_t)nt);
         bt_tree_copy(&pl.tt, &pl.st);
+        pl.same_tree = 1;
     } else {
         bt_parts_init(&pl.tgt, nt, tx, ty, tz, nullptr);
         bt_forest_build(&pl.tt, &pl.tgt, sys.n, sys.toff.data(), pl.prm.maxt);
@@ -532,6 +535,7 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
     dp.sx = d_sx; dp.sy = d_sy; dp.sz = d_sz; dp.sq = d_sq; dp.sorder = d_sord;
     if (same) {
         bt_tree_copy(&pl.tt, &pl.st);
+        pl.same_tree = 1;
         dp.tx = d_sx; dp.ty = d_sy; dp.tz = d_sz; dp.order = d_sord;
     } else {
         dp.tx = d_tx; dp.ty = d_ty; dp.tz = d_tz; dp.order = d_tord;
@@ -550,6 +554,11 @@ struct DevPlan {
     int tpt = 2, tile = 1024;   // tile shape of the mixed particle-output kernel
     bool tc_up = false;         // leaf P2M on the tensor cores (bt_tc.cu)
     bool sharded = false;       // this call evaluates a share of the target leaves (others get 0)
+    // symmetric near-field pairs (bt_sym.cu)
+    int sym_npairs = 0;
+    int2 *d_sym_pairs = nullptr;
+    int64_t *d_sym_slot = nullptr, *d_sym_in_off = nullptr, *d_sym_in_slot = nullptr;
+    float *d_sym_partial = nullptr;
     int *d_err = nullptr;       // set by a tensor-core kernel whose bounded wait expired
     int n = 0, P = 0, ns = 0, nt = 0, max_np1 = 0, kernel = 0;
     double kp = 0.0;
@@ -817,6 +826,18 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         const bt::MixedTargetsArgs a = mixed_targets_args(v);
         bt::launch_eval_targets_mixed(v.kernel, a, st);
         launches++;
+        if (v.sym_npairs > 0) {
+            bt::SymArgs y;
+            y.npairs = v.sym_npairs; y.pair = v.d_sym_pairs; y.slot = v.d_sym_slot;
+            y.ibeg = v.d_sibeg; y.numpar = v.d_snum; y.ctr = v.d_sctr; y.pos = v.d_spos;
+            y.partial = v.d_sym_partial; y.kc = (float)bt::mixed_kernel_constant(v.kernel, v.kp);
+            bt::launch_pp_sym(v.kernel, y, st);
+            bt::SymGatherArgs g;
+            g.nleaves = v.T_nleaves; g.leaf_node = v.d_tleaves; g.ibeg = v.d_sibeg; g.numpar = v.d_snum;
+            g.in_off = v.d_sym_in_off; g.in_slot = v.d_sym_in_slot; g.partial = v.d_sym_partial; g.pot = d_pot;
+            bt::launch_sym_gather(g, st);
+            launches += 2;
+        }
     } else if (nt > 0) {
         bt::EvalTargetsArgs a;
         a.n = n; a.nitems = v.n_ev_items; a.items = d_evitems; a.leaf_node = d_tleaves;
@@ -1032,7 +1053,92 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             }
         }
     }
+    pt.mark("plan: work items and near-field lists");
+    // Symmetric near-field pairs: with the targets being the sources and a
+    // symmetric kernel, leaf pairs {A, B} (A != B) that hold each other as
+    // near-field entries with no possible close pair are evaluated once for
+    // both sides (bt_sym.cu) and leave the per-target lists.
+    std::vector<int2> sym_pairs;
+    std::vector<int64_t> sym_slot, sym_in_off, sym_in_slot;
+    int64_t sym_total = 0;
+    int max_leaf = 0;
+    for (int u = 0; u < T.nleaves; u++) max_leaf = std::max(max_leaf, T.numpar[T.leaves[u]]);
+    if (mixed && pl.same_tree && shape.sym && shape.nshards <= 1 && max_leaf <= bt::SYM_MAX_LEAF &&
+        (o.kernel == COULOMB || o.kernel == REGULARIZED_COULOMB) && T.nleaves > 1) {
+        std::vector<int> unit_of(T.n, -1);
+        for (int u = 0; u < T.nleaves; u++) unit_of[T.leaves[u]] = u;
+        const int64_t ne = mx_doff[T.nleaves];
+        std::vector<unsigned char> sym(ne, 0);
+        // each unit's far partners, sorted, for the reverse look-ups
+        std::vector<int> far(ne);
+        std::vector<int64_t> far_end(T.nleaves);
+#pragma omp parallel for schedule(static)
+        for (int u = 0; u < T.nleaves; u++) {
+            int64_t w = mx_doff[u];
+            for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++)
+                if (!mx_dflag[k]) far[w++] = mx_didx[k];
+            std::sort(far.begin() + mx_doff[u], far.begin() + w);
+            far_end[u] = w;
+        }
+#pragma omp parallel for schedule(static)
+        for (int u = 0; u < T.nleaves; u++) {
+            const int A = T.leaves[u];
+            for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) {
+                const int B = mx_didx[k];
+                if (mx_dflag[k] || B == A || unit_of[B] < 0) continue;
+                const int ub = unit_of[B];
+                sym[k] = std::binary_search(far.begin() + mx_doff[ub], far.begin() + far_end[ub], A) ? 1 : 0;
+            }
+        }
+        // pairs {A, B} with A < B in unit order, then list order (leaves are
+        // of similar size, so the pairs need no cost ordering)
+        for (int u = 0; u < T.nleaves; u++) {
+            const int A = T.leaves[u];
+            for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++)
+                if (sym[k] && A < mx_didx[k]) sym_pairs.push_back(make_int2(A, mx_didx[k]));
+        }
+        if (!sym_pairs.empty()) {
+            // each pair's partial sums: A's particles, then B's; per leaf the
+            // slices addressed to it, in pair order
+            std::vector<int64_t> in_cnt(T.nleaves + 1, 0);
+            sym_slot.resize(sym_pairs.size());
+            for (size_t k = 0; k < sym_pairs.size(); k++) {
+                const int2 p = sym_pairs[k];
+                sym_slot[k] = sym_total;
+                sym_total += S.numpar[p.x] + S.numpar[p.y];
+                in_cnt[unit_of[p.x] + 1]++;
+                in_cnt[unit_of[p.y] + 1]++;
+            }
+            for (int u = 0; u < T.nleaves; u++) in_cnt[u + 1] += in_cnt[u];
+            sym_in_off = in_cnt;
+            sym_in_slot.assign((size_t)sym_in_off[T.nleaves], 0);
+            std::vector<int64_t> fill(sym_in_off.begin(), sym_in_off.end() - 1);
+            for (size_t k = 0; k < sym_pairs.size(); k++) {
+                sym_in_slot[fill[unit_of[sym_pairs[k].x]]++] = sym_slot[k];
+                sym_in_slot[fill[unit_of[sym_pairs[k].y]]++] = sym_slot[k] + S.numpar[sym_pairs[k].x];
+            }
+            // both directions leave the per-target near-field lists
+            std::vector<int64_t> noff(T.nleaves + 1, 0);
+            for (int u = 0; u < T.nleaves; u++) {
+                int64_t c = 0;
+                for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) c += sym[k] ? 0 : 1;
+                noff[u + 1] = noff[u] + c;
+            }
+            std::vector<int> nidx((size_t)noff[T.nleaves]);
+            std::vector<unsigned char> nflag((size_t)noff[T.nleaves]);
+#pragma omp parallel for schedule(static)
+            for (int u = 0; u < T.nleaves; u++) {
+                int64_t w = noff[u];
+                for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++)
+                    if (!sym[k]) { nidx[w] = mx_didx[k]; nflag[w] = mx_dflag[k]; w++; }
+            }
+            mx_doff.swap(noff);
+            mx_didx.swap(nidx);
+            mx_dflag.swap(nflag);
+        }
+    }
 
+    pt.mark("plan: symmetric near-field pairs");
     // Hermite upward pass: particle chunks of every source node
     std::vector<bt::HermChunk> hchunks;
     std::vector<int3> hred;
@@ -1052,7 +1158,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     int2 *d_evitems, *d_griditems, *d_l2pitems;
     int *d_order;
     double *d_out;
-    pt.mark("plan: work items and list arrays");
+    pt.mark("plan: Hermite chunks, device layout");
     Layout L;
     if (dp) {
         d_sx = (double *)dp->sx; d_sy = (double *)dp->sy; d_sz = (double *)dp->sz; d_sq = (double *)dp->sq;
@@ -1104,6 +1210,9 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     double *d_srad = nullptr, *d_trad = nullptr;
     float *d_xQ32[BT_MAX_DEGREE + 1] = {};
     int *d_xleaves[BT_MAX_DEGREE + 1] = {}, *d_xlvl[BT_MAX_DEGREE + 1] = {};
+    int2 *d_sym_pairs = nullptr;
+    int64_t *d_sym_slot = nullptr, *d_sym_in_off = nullptr, *d_sym_in_slot = nullptr;
+    float *d_sym_partial = nullptr;
     if (mixed) {
         L.add(&d_spos, ns); L.add(&d_tpos, nt);
         if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P * nq);
@@ -1112,6 +1221,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         L.add(&d_mxcpoff, mx_cpoff.size()); L.add(&d_mxcpidx, mx_cpidx.size());
         if (pl.a_deg) L.add(&d_adeg, n_approx);
         L.add(&d_srad, S.n); L.add(&d_trad, T.n);
+        if (!sym_pairs.empty()) {
+            L.add(&d_sym_pairs, sym_pairs.size()); L.add(&d_sym_slot, sym_slot.size());
+            L.add(&d_sym_in_off, sym_in_off.size()); L.add(&d_sym_in_slot, sym_in_slot.size());
+            L.add(&d_sym_partial, (size_t)sym_total);
+        }
         for (size_t i = 0; i < xdeg.size(); i++) {
             size_t Pd = (size_t)(xdeg[i] + 1) * (xdeg[i] + 1) * (xdeg[i] + 1);
             L.add(&d_xgrid[i], xgrid[i].size());
@@ -1176,6 +1290,10 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
             UP(d_mxdflag, mx_dflag.data(), mx_dflag.size());
+            if (!sym_pairs.empty()) {
+                UP(d_sym_pairs, sym_pairs.data(), sym_pairs.size()); UP(d_sym_slot, sym_slot.data(), sym_slot.size());
+                UP(d_sym_in_off, sym_in_off.data(), sym_in_off.size()); UP(d_sym_in_slot, sym_in_slot.data(), sym_in_slot.size());
+            }
             if (pl.a_deg) UP(d_adeg, pl.a_deg, n_approx);
             UP(d_srad, S.rad, S.n); UP(d_trad, T.rad, T.n);
             for (size_t i = 0; i < xdeg.size(); i++) {
@@ -1194,6 +1312,9 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.tile = shape.tile;
         v.tc_up = shape.tc_up && mixed && !herm;
         v.sharded = shape.nshards > 1;
+        v.sym_npairs = (int)sym_pairs.size();
+        v.d_sym_pairs = d_sym_pairs; v.d_sym_slot = d_sym_slot; v.d_sym_in_off = d_sym_in_off;
+        v.d_sym_in_slot = d_sym_in_slot; v.d_sym_partial = d_sym_partial;
         v.n = n; v.P = P; v.ns = ns; v.nt = nt; v.max_np1 = max_np1; v.kernel = o.kernel; v.kp = o.kp;
         v.S_n = S.n; v.S_nleaves = S.nleaves; v.S_max_depth = S.max_depth;
         v.T_n = T.n; v.T_nleaves = T.nleaves; v.T_max_depth = T.max_depth;
@@ -1551,6 +1672,11 @@ int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double 
     }
     shape = tuned_shape(opts ? opts->device : 0, prm.kernel, prm.approx);
     shape.tc_up = !(opts && opts->upward == BT_UPWARD_FP64);
+    if (opts && opts->symmetry != BT_SYMMETRY_AUTO && opts->symmetry != BT_SYMMETRY_OFF) {
+        set_err("invalid symmetry %d", opts->symmetry);
+        return BT_ERR_PARAM;
+    }
+    shape.sym = !(opts && opts->symmetry == BT_SYMMETRY_OFF);
     if (opts && opts->shard_count > 1) {
         if (opts->shard_index < 0 || opts->shard_index >= opts->shard_count) {
             set_err("shard index %d outside [0, %d)", opts->shard_index, opts->shard_count);

@@ -72,6 +72,7 @@ typedef struct {
     bt_csr g_cp;            /* per target node: source nodes evaluated onto the grid (CP) */
     unsigned char *a_deg;   /* per t_approx entry: interpolation degree (NULL: prm.degree) */
     long long sel_hist[14]; /* learned selection: entries per degree, [13] = direct instead */
+    int same_tree;          /* the targets are the sources: tt is a copy of st            */
 } bt_plan;
 
 /* bt_params.c */

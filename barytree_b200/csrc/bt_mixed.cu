@@ -22,24 +22,11 @@
 #include <cfloat>
 #include <cstdint>
 
+#include "bt_f2.cuh"
 #include "bt_kernels.cuh"
 #include "bt_mixed.h"
 
 namespace bt {
-
-__device__ __forceinline__ float rsqrt_apx(float x)
-{
-    float y;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-__device__ __forceinline__ float ex2_apx(float x)
-{
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
 
 // Kernel value for a well-separated pair.  kc: Yukawa -kappa*log2(e);
 // regularised Coulomb eps^2; unused for Coulomb.
@@ -234,40 +221,6 @@ __device__ __forceinline__ void pc_cluster_herm(const float *x, const float *y, 
 // the close pair's magnitude).  Close pairs occur only between leaves whose
 // boxes lie within that distance (flagged per near-field entry); the other
 // entries run pp_tile_far with no test at all.
-// Packed FP32 pairs (sm_100 f32x2 instructions): one instruction applies the
-// same operation to two FP32 values held in a 64-bit register pair, which
-// halves the issue slots of the near-field arithmetic.  Flush-to-zero like
-// the rest of this file.
-typedef unsigned long long f2_t;
-
-__device__ __forceinline__ f2_t f2_make(float lo, float hi)
-{
-    f2_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ void f2_split(f2_t v, float &lo, float &hi)
-{
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b)
-{
-    f2_t r;
-    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b)
-{
-    f2_t r;
-    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c)
-{
-    f2_t r;
-    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
-}
 
 // Lagrange far field with the targets in packed pairs (NT even, Coulomb and
 // regularised Coulomb): pc_cluster's operations lane by lane in f32x2

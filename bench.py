@@ -316,6 +316,8 @@ def make_parser():
     ap.add_argument("--shard", action="store_true",
                     help="strong scaling: all ranks share one system, each evaluates its target shard, "
                          "one all-reduce combines the potentials (default: one independent system per rank)")
+    ap.add_argument("--symmetry", choices=["auto", "off"], default="auto",
+                    help="mixed path with targets = sources: near-field leaf pairs once for both sides (auto) or not")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default tile shape instead of autotuning it on this workload")
     ap.add_argument("--n", type=int, default=None,
@@ -335,7 +337,7 @@ def eval_kwargs(B, cfg, args, policy, device, shard):
                 max_target_leaf=cfg["leaf"], size_check=cfg["sc"], precision=prec, device=device,
                 dispatch={"auto": B.DISPATCH_AUTO, "queue": B.DISPATCH_QUEUE, "grid": B.DISPATCH_GRID}[args.dispatch],
                 upward=B.UPWARD_FP64 if args.upward == "fp64" else B.UPWARD_AUTO,
-                shard=shard)
+                shard=shard, symmetry=B.SYMMETRY_OFF if args.symmetry == "off" else B.SYMMETRY_AUTO)
 
 
 def autotune_kwargs(common):
@@ -545,7 +547,7 @@ def main():
             "data": "synthetic (seeded numpy PCG64 with the configuration's distribution)",
             "config": {"workload": cfg["workload"], "config_id": args.config, "precision": args.precision,
                        "degree_policy": policy, "tolerance": args.tolerance, "dispatch": args.dispatch,
-                       "tile_shape": tuning, "upward": args.upward,
+                       "tile_shape": tuning, "upward": args.upward, "symmetry": args.symmetry,
                        "l2": "flushed between steps (256 MB write)",
                        "parallelism": (f"one system, target shards over {world} GPU(s), one all-reduce of the "
                                        "potentials" if args.shard else

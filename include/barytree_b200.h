@@ -105,15 +105,24 @@ typedef struct bt_options {
     /* Target sharding (particle-cluster): with shard_count > 1 the call
      * evaluates shard_index's share of the target leaves (contiguous in tree
      * order, equal estimated cost) and leaves the other potentials 0; the sum
-     * of the outputs of all shards is the unsharded result, bit for bit.
+     * of the outputs of all shards is the unsharded result with
+     * BT_SYMMETRY_OFF, bit for bit (shards do not pair leaves across shards).
      * Trees, lists and proxies are built in full by every shard.            */
     int shard_index;
     int shard_count;
+    int symmetry;         /* mixed path, targets = sources (all of a batch's systems),
+                             Coulomb or regularized Coulomb, leaves of at most 2048
+                             particles, not sharded: BT_SYMMETRY_AUTO (default)
+                             evaluates each pair of near-field leaves that list each
+                             other (and can hold no close pair) once for both sides;
+                             BT_SYMMETRY_OFF evaluates every direction separately.
+                             Results agree to FP32 rounding and are deterministic.  */
 } bt_options;
 
 enum { BT_TREE_GPU = 0, BT_TREE_HOST = 1 };
 enum { BT_DISPATCH_AUTO = 0, BT_DISPATCH_QUEUE = 1, BT_DISPATCH_GRID = 2 };
 enum { BT_UPWARD_AUTO = 0, BT_UPWARD_FP64 = 1 };
+enum { BT_SYMMETRY_AUTO = 0, BT_SYMMETRY_OFF = 1 };
 
 /* Per-call report (all optional: pass NULL). */
 typedef struct bt_report {

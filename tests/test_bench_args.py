@@ -14,7 +14,7 @@ import bench
 
 @pytest.mark.parametrize("config", sorted(bench.CONFIGS))
 @pytest.mark.parametrize("argv", [[], ["--precision", "fp64"], ["--dispatch", "queue", "--upward", "fp64"],
-                                  ["--shard"]])
+                                  ["--shard"], ["--symmetry", "off"]])
 def test_every_call_accepts_the_run_arguments(config, argv):
     args = bench.make_parser().parse_args(["--config", str(config)] + argv)
     cfg = bench.CONFIGS[config]

@@ -1,0 +1,78 @@
+"""GPU tests of the symmetric near-field pairs of the mixed path (targets =
+sources, Coulomb and regularized Coulomb): leaf pairs that list each other
+with no possible close pair are evaluated once for both sides
+(bt_sym.cu).  Against the same call with BT_SYMMETRY_OFF the potentials
+agree to FP32 rounding (the sums close in another order) and keep the mixed
+path's accuracy against the FP64 direct sum; they are the same bit for bit
+on every run, in a session and in a batch; calls the pass does not apply
+to are bit-identical to BT_SYMMETRY_OFF."""
+import numpy as np
+import pytest
+
+import barytree_b200 as B
+from conftest import uniform_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _clustered(n, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-0.6, 0.6, (4, 3))
+    pts = np.concatenate([rng.normal(c[k], 0.1, (n // 5, 3)) for k in range(4)] + [rng.uniform(-1, 1, (n // 5, 3))])
+    pts = np.clip(pts, -1, 1)
+    return pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy(), rng.uniform(-1, 1, len(pts))
+
+
+@pytest.mark.parametrize("kernel,kp,approx,sc", [(B.Kernel.COULOMB, 0.0, 1, 1.0),
+                                                 (B.Kernel.REGULARIZED_COULOMB, 1e-3, 1, 1.0),
+                                                 (B.Kernel.COULOMB, 0.0, 2, 4.0)])
+def test_symmetric_pairs_against_both_directions(kernel, kp, approx, sc):
+    x, y, z, q = _clustered(200000, 41)
+    kw = dict(kernel=kernel, kernel_param=kp, approximation=approx, theta=0.7, degree=6, max_source_leaf=500,
+              max_target_leaf=500, size_check=sc, precision=B.PRECISION_MIXED)
+    sym = B.treecode(x, y, z, x.copy(), y.copy(), z.copy(), q, **kw)
+    off = B.treecode(x, y, z, x.copy(), y.copy(), z.copy(), q, symmetry=B.SYMMETRY_OFF, **kw)
+    assert not np.array_equal(sym, off)                  # the pass ran
+    assert _rel(sym, off) < 5e-7
+    assert np.array_equal(B.treecode(x, y, z, x.copy(), y.copy(), z.copy(), q, **kw), sym)   # deterministic
+    idx = np.arange(0, len(x), 200)
+    exact = B.direct(x[idx], y[idx], z[idx], x, y, z, q, kernel=kernel, kernel_param=kp)
+    assert _rel(sym[idx], exact) <= 1.05 * _rel(off[idx], exact) + 1e-7
+
+
+def test_symmetric_pairs_with_learned_degrees_sessions_and_batches():
+    from barytree_b200 import selector
+    selector.install_default()
+    x, y, z, q = _clustered(300000, 42)
+    kw = dict(theta=0.7, degree=10, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
+              precision=B.PRECISION_MIXED, degree_policy=B.DEGREE_LEARNED, tolerance=1e-6)
+    sym = B.treecode(x, y, z, x, y, z, q, **kw)
+    off = B.treecode(x, y, z, x, y, z, q, symmetry=B.SYMMETRY_OFF, **kw)
+    assert _rel(sym, off) < 5e-7
+    idx = np.arange(0, len(x), 300)
+    assert _rel(sym[idx], B.direct(x[idx], y[idx], z[idx], x, y, z, q)) < 1e-6
+    s = B.Session([(x, y, z, x, y, z, q)], **kw)
+    assert np.array_equal(s.evaluate(q)[0], sym)
+    s.close()
+    # a batch of two systems equals the separate calls
+    x2, y2, z2, q2 = _clustered(100000, 43)
+    kb = dict(kw)
+    kb.pop("degree_policy"); kb.pop("tolerance")
+    pots = B.treecode_batch([(x, y, z, x, y, z, q), (x2, y2, z2, x2, y2, z2, q2)], **kb)
+    assert np.array_equal(pots[0], B.treecode(x, y, z, x, y, z, q, **kb))
+    assert np.array_equal(pots[1], B.treecode(x2, y2, z2, x2, y2, z2, q2, **kb))
+
+
+@pytest.mark.parametrize("case", ["targets_differ", "yukawa", "fp64"])
+def test_symmetry_does_not_apply(case):
+    tx, ty, tz, sx, sy, sz, sq = uniform_inputs(44, 80000, targets="other" if case == "targets_differ" else "same")
+    kw = dict(theta=0.7, degree=5, max_source_leaf=400, max_target_leaf=400,
+              precision=B.PRECISION_FP64 if case == "fp64" else B.PRECISION_MIXED)
+    if case == "yukawa":
+        kw.update(kernel=B.Kernel.YUKAWA, kernel_param=0.5)
+    assert np.array_equal(B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw),
+                          B.treecode(tx, ty, tz, sx, sy, sz, sq, symmetry=B.SYMMETRY_OFF, **kw))
