@@ -89,7 +89,7 @@ class Report(ctypes.Structure):
                 ("cp_ptwise", ctypes.c_longlong), ("cc_ptwise", ctypes.c_longlong),
                 ("ms_eval_kernel", ctypes.c_double), ("eval_flops", ctypes.c_longlong),
                 ("source_nodes", ctypes.c_int), ("target_nodes", ctypes.c_int), ("kernel_launches", ctypes.c_int),
-                ("selected", ctypes.c_longlong * 14)]
+                ("selected", ctypes.c_longlong * 14), ("sym_ptwise", ctypes.c_longlong)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}

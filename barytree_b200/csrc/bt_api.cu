@@ -1419,6 +1419,9 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             rep->ms_downward = d;
             rep->ms_eval_kernel = c;
             rep->kernel_launches = (int)launches;
+            long long symw = 0;
+            for (const int2 &pr : sym_pairs) symw += 2LL * S.numpar[pr.x] * S.numpar[pr.y];
+            rep->sym_ptwise = symw;
             rep->source_nodes = S.n;
             rep->target_nodes = T.n;
             double tend = now_ms();

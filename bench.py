@@ -265,6 +265,14 @@ def roofline(sfu, tflops, fma_peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_ra
         ach = evals * mufu_per_eval / (ev_ms * 1e-3) / 1e9 if ev_ms > 0 else None
         r.update(bound="sfu (MUFU rsqrt/ex2)", achieved=ach, peak=rsqrt_rate, unit="Gop/s",
                  frac=ach / rsqrt_rate if ach else None)
+        # symmetric near-field pairs: one 1/r serves two of the evaluations
+        # counted above, so the pipe itself did fewer operations
+        sym = rep.get("sym_ptwise", 0)
+        if sym and ev_ms > 0:
+            phys = (evals - sym / 2) * mufu_per_eval / (ev_ms * 1e-3) / 1e9
+            r.update(symmetric_evaluations=sym, mufu_physical=phys, frac_physical=phys / rsqrt_rate,
+                     note="achieved counts evaluations as the reference does (each direction of a near-field "
+                          "pair); mufu_physical counts the 1/r the GPU computed (one per symmetric pair)")
     else:
         r.update(bound="fp64-simt" if prec == 0 else "fp32-simt", achieved=tflops, peak=fma_peak, unit="TFLOP/s",
                  frac=tflops / fma_peak if tflops else None)

@@ -136,6 +136,8 @@ typedef struct bt_report {
     int source_nodes, target_nodes, kernel_launches;
     long long selected[14];    /* learned selection: entries per degree (index = degree),
                                   index 13 = entries evaluated directly instead */
+    long long sym_ptwise;      /* near-field evaluations (both directions counted) served
+                                  by the symmetric pass with one 1/r per pair of them   */
 } bt_report;
 
 /* Treecode evaluation with options and a report.  Same meaning of the
