@@ -20,6 +20,8 @@
 #include <climits>
 #include <cstring>
 #include <mutex>
+#include <omp.h>
+#include <sys/resource.h>
 #include <vector>
 
 #include "../../include/barytree_b200.h"
@@ -53,16 +55,32 @@ double now_ms()
 
 // Host-side phase times on stderr when the environment variable
 // BARYTREE_B200_TIMING is set (diagnostics; device phases are in bt_report).
+long minor_faults()
+{
+    struct rusage ru;
+    return getrusage(RUSAGE_SELF, &ru) == 0 ? ru.ru_minflt : 0;
+}
+
 struct PhaseTimer {
     bool on;
     double t;
-    PhaseTimer() : on(getenv("BARYTREE_B200_TIMING") != nullptr), t(now_ms()) {}
+    long flt;
+    PhaseTimer() : on(getenv("BARYTREE_B200_TIMING") != nullptr), t(now_ms()), flt(on ? minor_faults() : 0)
+    {
+        static bool said = false;
+        if (on && !said) {
+            said = true;
+            fprintf(stderr, "[barytree_b200] host threads (OpenMP) %d\n", omp_get_max_threads());
+        }
+    }
     void mark(const char *what)
     {
         if (!on) return;
         const double n = now_ms();
-        fprintf(stderr, "[barytree_b200] %-34s %9.3f ms\n", what, n - t);
+        const long f = minor_faults();
+        fprintf(stderr, "[barytree_b200] %-34s %9.3f ms %8ld page faults\n", what, n - t, f - flt);
         t = n;
+        flt = f;
     }
 };
 
@@ -556,6 +574,8 @@ struct DevPlan {
     bool sharded = false;       // this call evaluates a share of the target leaves (others get 0)
     // symmetric near-field pairs (bt_sym.cu)
     int sym_npairs = 0;
+    int sym_far_pairs = 0;      // the first pairs: boxes apart by more than the close-pair distance
+    double *d_sbox = nullptr;   // node boxes (x0 x1 y0 y1 z0 z1) for the pairs within it
     int2 *d_sym_pairs = nullptr;
     int64_t *d_sym_slot = nullptr, *d_sym_in_off = nullptr, *d_sym_in_slot = nullptr;
     float *d_sym_partial = nullptr;
@@ -782,6 +802,11 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     if (ev) CK(record(1));
     // grid-output evaluation (CP, M2L) and L2L
     if (mixed && v.queue) CK(cudaMemsetAsync(d_queue, 0, 2 * sizeof(int), st));
+    // a shard evaluates the grids of its own nodes only; the others start at 0
+    if (need_tgt_grids && nt > 0 && v.sharded) {
+        CK(cudaMemsetAsync(d_Phi, 0, sizeof(double) * (size_t)v.T_n * P * (herm ? 8 : 1), st));
+        if (v.ss) CK(cudaMemsetAsync(v.d_Phiw, 0, sizeof(double) * (size_t)v.T_n * P, st));
+    }
     if (need_tgt_grids && nt > 0 && v.ss) {
         bt::SsGridsArgs g;
         g.n = n; g.nitems = v.n_grid_items; g.items = d_griditems; g.t_grid = d_tgrid;
@@ -831,12 +856,20 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
             y.npairs = v.sym_npairs; y.pair = v.d_sym_pairs; y.slot = v.d_sym_slot;
             y.ibeg = v.d_sibeg; y.numpar = v.d_snum; y.ctr = v.d_sctr; y.pos = v.d_spos;
             y.partial = v.d_sym_partial; y.kc = (float)bt::mixed_kernel_constant(v.kernel, v.kp);
+            y.rad = v.d_srad; y.box = v.d_sbox; y.x64 = v.d_sx; y.y64 = v.d_sy; y.z64 = v.d_sz; y.q64 = v.d_sq;
+            y.kp = v.kp;
+            bt::SymArgs yc = y;
+            y.npairs = v.sym_far_pairs;
+            yc.npairs = v.sym_npairs - v.sym_far_pairs;
+            yc.pair += v.sym_far_pairs;
+            yc.slot += v.sym_far_pairs;
             bt::launch_pp_sym(v.kernel, y, st);
+            bt::launch_pp_sym_close(v.kernel, yc, st);
             bt::SymGatherArgs g;
             g.nleaves = v.T_nleaves; g.leaf_node = v.d_tleaves; g.ibeg = v.d_sibeg; g.numpar = v.d_snum;
             g.in_off = v.d_sym_in_off; g.in_slot = v.d_sym_in_slot; g.partial = v.d_sym_partial; g.pot = d_pot;
             bt::launch_sym_gather(g, st);
-            launches += 2;
+            launches += 1 + (y.npairs > 0) + (yc.npairs > 0);
         }
     } else if (nt > 0) {
         bt::EvalTargetsArgs a;
@@ -881,7 +914,12 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
     if (v.ss && nt > 0) {
         // subtraction correction (InteractionCompute_SubtractionPotentialCorrection,
         // src/interaction_compute/interaction_compute_correction.c:22-45)
-        bt::launch_ss_correction(nt, v.ss_c, v.d_tq, d_pot, st);
+        // (a shard: the targets of its own leaves, through the work items)
+        if (v.sharded)
+            bt::launch_ss_correction_items(v.n_ev_items, d_evitems, bt::ss_chunk(), d_tleaves, d_tibeg, d_tnum, v.ss_c,
+                                           v.d_tq, d_pot, st);
+        else
+            bt::launch_ss_correction(nt, v.ss_c, v.d_tq, d_pot, st);
         launches++;
     }
     CK(cudaGetLastError());
@@ -915,6 +953,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     std::vector<double> sgrid, slen, tgrid, tlen;
     fill_grids(S, n, sgrid, slen);
     fill_grids(T, n, tgrid, tlen);
+    pt.mark("plan: grids at the base degree");
     // further degrees used by a learned per-interaction selection (mixed path)
     std::vector<int> xdeg;
     std::vector<std::vector<double>> xgrid;
@@ -928,6 +967,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         std::vector<double> tmp;
         for (size_t i = 0; i < xdeg.size(); i++) fill_grids(S, xdeg[i], xgrid[i], tmp);
     }
+    pt.mark("plan: grids at the selected degrees");
     // Each extra degree needs proxies only at the source nodes some
     // interaction uses it for: its P2M and M2M run over the leaves and
     // internal nodes under those nodes (pre-order numbering: a node's
@@ -992,32 +1032,57 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     // evaluate in FP64
     const bool mixed = o.precision == BT_PRECISION_MIXED && !ssm && (!herm || o.ctype == PARTICLE_CLUSTER) &&
                        o.kernel <= REGULARIZED_COULOMB;
-    if (shape.nshards > 1) {
-        // target sharding: contiguous runs of target leaves (tree order) of
-        // about equal cost; leaf u belongs to the shard that holds the middle
-        // of its cost interval
-        double total = 0.0;
-        for (int u = 0; u < T.nleaves; u++) total += leaf_cost[u];
-        double before = 0.0;
-        for (int u = 0; u < T.nleaves; u++) {
-            const double mid = before + 0.5 * leaf_cost[u];
-            before += leaf_cost[u];
-            int k = total > 0 ? (int)(mid / total * shape.nshards) : u % shape.nshards;
-            if (k >= shape.nshards) k = shape.nshards - 1;
-            if (k != shape.shard) leaf_count[u] = 0;
-        }
-    }
-    std::vector<int2> ev_items =
-        make_items(T.nleaves, leaf_count.data(), mixed ? bt::mixed_targets_chunk() : 128, leaf_cost);
-    std::vector<int2> grid_items, l2p_items;
+    // grid-output cost per target node (CP and CC): the work-item order of
+    // the grid evaluation, and for a sharded call the share of the leaves
+    // under the node
+    std::vector<double> gcost;
     if (need_tgt_grids) {
-        std::vector<int> pcount(T.n, P);
-        std::vector<double> gcost(T.n, 0.0);
+        gcost.assign(T.n, 0.0);
         for (int i = 0; i < T.n; i++) {
             double c = (double)(pl.g_cc.off[i + 1] - pl.g_cc.off[i]) * P;
             for (int64_t k = pl.g_cp.off[i]; k < pl.g_cp.off[i + 1]; k++) c += S.numpar[pl.g_cp.idx[k]] * nq;
             gcost[i] = c;
         }
+    }
+    // target sharding: the nodes whose grid outputs this shard evaluates
+    // (the owned leaves and their ancestors)
+    std::vector<unsigned char> tnode_need;
+    if (shape.nshards > 1) {
+        // contiguous runs of target leaves (tree order) of about equal cost;
+        // leaf u belongs to the shard that holds the middle of its cost
+        // interval.  A node's grid outputs serve the leaves under it, so its
+        // cost is spread over them by particle count.
+        std::vector<double> scost(leaf_cost);
+        if (need_tgt_grids)
+            for (int u = 0; u < T.nleaves; u++) {
+                const int leaf = T.leaves[u];
+                for (int v = leaf; v >= 0; v = T.parent[v])
+                    if (T.numpar[v] > 0) scost[u] += gcost[v] * T.numpar[leaf] / T.numpar[v];
+            }
+        double total = 0.0;
+        for (int u = 0; u < T.nleaves; u++) total += scost[u];
+        double before = 0.0;
+        for (int u = 0; u < T.nleaves; u++) {
+            const double mid = before + 0.5 * scost[u];
+            before += scost[u];
+            int k = total > 0 ? (int)(mid / total * shape.nshards) : u % shape.nshards;
+            if (k >= shape.nshards) k = shape.nshards - 1;
+            if (k != shape.shard) leaf_count[u] = 0;
+        }
+        if (need_tgt_grids) {
+            tnode_need.assign(T.n, 0);
+            for (int u = 0; u < T.nleaves; u++)
+                if (leaf_count[u] > 0)
+                    for (int v = T.leaves[u]; v >= 0 && !tnode_need[v]; v = T.parent[v]) tnode_need[v] = 1;
+        }
+    }
+    std::vector<int2> ev_items =
+        make_items(T.nleaves, leaf_count.data(), mixed ? bt::mixed_targets_chunk() : ssm ? bt::ss_chunk() : 128, leaf_cost);
+    std::vector<int2> grid_items, l2p_items;
+    if (need_tgt_grids) {
+        std::vector<int> pcount(T.n, P);
+        if (!tnode_need.empty())
+            for (int i = 0; i < T.n; i++) pcount[i] = tnode_need[i] ? P : 0;
         grid_items = make_items(T.n, pcount.data(), 128, gcost);
         std::vector<double> lcost(T.nleaves, 1.0);
         l2p_items = make_items(T.nleaves, leaf_count.data(), 128, lcost);
@@ -1056,88 +1121,156 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     pt.mark("plan: work items and near-field lists");
     // Symmetric near-field pairs: with the targets being the sources and a
     // symmetric kernel, leaf pairs {A, B} (A != B) that hold each other as
-    // near-field entries with no possible close pair are evaluated once for
-    // both sides (bt_sym.cu) and leave the per-target lists.
+    // near-field entries are evaluated once for both sides (bt_sym.cu) and
+    // leave the per-target lists.  Every pass runs per unit in parallel.  The
+    // pairs whose boxes are farther apart than the close-pair distance come
+    // first, then the pairs within it (their own kernel); each group is
+    // numbered by head unit (A < B), then by partner node, so the numbering
+    // does not depend on the thread count.
     std::vector<int2> sym_pairs;
     std::vector<int64_t> sym_slot, sym_in_off, sym_in_slot;
-    int64_t sym_total = 0;
+    int64_t sym_total = 0, sym_far_pairs = 0;
     int max_leaf = 0;
     for (int u = 0; u < T.nleaves; u++) max_leaf = std::max(max_leaf, T.numpar[T.leaves[u]]);
     if (mixed && pl.same_tree && shape.sym && shape.nshards <= 1 && max_leaf <= bt::SYM_MAX_LEAF &&
-        (o.kernel == COULOMB || o.kernel == REGULARIZED_COULOMB) && T.nleaves > 1) {
+        (o.kernel == COULOMB || o.kernel == YUKAWA || o.kernel == REGULARIZED_COULOMB) && T.nleaves > 1) {
+        const int NU = T.nleaves;
         std::vector<int> unit_of(T.n, -1);
-        for (int u = 0; u < T.nleaves; u++) unit_of[T.leaves[u]] = u;
-        const int64_t ne = mx_doff[T.nleaves];
-        std::vector<unsigned char> sym(ne, 0);
-        // each unit's far partners, sorted, for the reverse look-ups
-        std::vector<int> far(ne);
-        std::vector<int64_t> far_end(T.nleaves);
+        for (int u = 0; u < NU; u++) unit_of[T.leaves[u]] = u;
+        const int64_t ne = mx_doff[NU];
+        // per unit: its partners (other leaves), sorted by node, each with the
+        // list entry it came from and whether the boxes are within the
+        // close-pair distance (the same test from both sides)
+        std::vector<int> far(ne), fent(ne);
+        std::vector<unsigned char> fnear(ne);
+        std::vector<int64_t> far_end(NU);
+#pragma omp parallel
+        {
+            std::vector<uint64_t> keys;
+#pragma omp for schedule(static)
+            for (int u = 0; u < NU; u++) {
+                const int A = T.leaves[u];
+                keys.clear();
+                for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) {
+                    const int B = mx_didx[k];
+                    if (B == A || unit_of[B] < 0) continue;
+                    keys.push_back(((uint64_t)(uint32_t)B << 32) | (uint64_t)(k - mx_doff[u]));
+                }
+                std::sort(keys.begin(), keys.end());
+                int64_t w = mx_doff[u];
+                for (uint64_t key : keys) {
+                    far[w] = (int)(key >> 32);
+                    fent[w] = (int)(key & 0xffffffffu);
+                    fnear[w] = mx_dflag[mx_doff[u] + fent[w]];
+                    w++;
+                }
+                far_end[u] = w;
+            }
+        }
+        pt.mark("plan: symmetric: sorted partners");
+        // rev[j]: where the partner's sorted list holds this unit's leaf (-1:
+        // nowhere, the entry stays one-directional)
+        std::vector<int64_t> rev(ne, -1);
+        std::vector<int64_t> poff0(NU + 1, 0), poff1(NU + 1, 0), ioff(NU + 1, 0);
 #pragma omp parallel for schedule(static)
-        for (int u = 0; u < T.nleaves; u++) {
-            int64_t w = mx_doff[u];
-            for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++)
-                if (!mx_dflag[k]) far[w++] = mx_didx[k];
-            std::sort(far.begin() + mx_doff[u], far.begin() + w);
-            far_end[u] = w;
+        for (int u = 0; u < NU; u++) {
+            const int A = T.leaves[u];
+            int64_t heads[2] = {0, 0}, all = 0;
+            for (int64_t j = mx_doff[u]; j < far_end[u]; j++) {
+                const int B = far[j], ub = unit_of[B];
+                const int *b0 = far.data() + mx_doff[ub], *b1 = far.data() + far_end[ub];
+                const int *it = std::lower_bound(b0, b1, A);
+                if (it != b1 && *it == A) {
+                    rev[j] = it - far.data();
+                    all++;
+                    heads[fnear[j]] += A < B ? 1 : 0;
+                }
+            }
+            poff0[u + 1] = heads[0];
+            poff1[u + 1] = heads[1];
+            ioff[u + 1] = all;
         }
+        for (int u = 0; u < NU; u++) {
+            poff0[u + 1] += poff0[u];
+            ioff[u + 1] += ioff[u];
+        }
+        sym_far_pairs = poff0[NU];
+        poff1[0] = sym_far_pairs;
+        for (int u = 0; u < NU; u++) poff1[u + 1] += poff1[u];
+        pt.mark("plan: symmetric: reverse look-ups");
+        const int64_t npairs = poff1[NU];
+        if (npairs > 0) {
+            // pairs headed by each unit, and the pair number of each head entry
+            sym_pairs.resize((size_t)npairs);
+            std::vector<int64_t> pid(ne, -1), usz0(NU + 1, 0), usz1(NU + 1, 0);
 #pragma omp parallel for schedule(static)
-        for (int u = 0; u < T.nleaves; u++) {
-            const int A = T.leaves[u];
-            for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) {
-                const int B = mx_didx[k];
-                if (mx_dflag[k] || B == A || unit_of[B] < 0) continue;
-                const int ub = unit_of[B];
-                sym[k] = std::binary_search(far.begin() + mx_doff[ub], far.begin() + far_end[ub], A) ? 1 : 0;
+            for (int u = 0; u < NU; u++) {
+                const int A = T.leaves[u];
+                int64_t p[2] = {poff0[u], poff1[u]}, sz[2] = {0, 0};
+                for (int64_t j = mx_doff[u]; j < far_end[u]; j++)
+                    if (rev[j] >= 0 && A < far[j]) {
+                        const int g = fnear[j];
+                        pid[j] = p[g];
+                        sym_pairs[p[g]++] = make_int2(A, far[j]);
+                        sz[g] += S.numpar[A] + S.numpar[far[j]];
+                    }
+                usz0[u + 1] = sz[0];
+                usz1[u + 1] = sz[1];
             }
-        }
-        // pairs {A, B} with A < B in unit order, then list order (leaves are
-        // of similar size, so the pairs need no cost ordering)
-        for (int u = 0; u < T.nleaves; u++) {
-            const int A = T.leaves[u];
-            for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++)
-                if (sym[k] && A < mx_didx[k]) sym_pairs.push_back(make_int2(A, mx_didx[k]));
-        }
-        if (!sym_pairs.empty()) {
-            // each pair's partial sums: A's particles, then B's; per leaf the
-            // slices addressed to it, in pair order
-            std::vector<int64_t> in_cnt(T.nleaves + 1, 0);
-            sym_slot.resize(sym_pairs.size());
-            for (size_t k = 0; k < sym_pairs.size(); k++) {
-                const int2 p = sym_pairs[k];
-                sym_slot[k] = sym_total;
-                sym_total += S.numpar[p.x] + S.numpar[p.y];
-                in_cnt[unit_of[p.x] + 1]++;
-                in_cnt[unit_of[p.y] + 1]++;
+            for (int u = 0; u < NU; u++) usz0[u + 1] += usz0[u];
+            usz1[0] = usz0[NU];
+            for (int u = 0; u < NU; u++) usz1[u + 1] += usz1[u];
+            sym_total = usz1[NU];
+            // each pair's partial sums: A's particles, then B's
+            sym_slot.resize((size_t)npairs);
+#pragma omp parallel for schedule(static)
+            for (int u = 0; u < NU; u++) {
+                const int64_t pb[2] = {poff0[u], poff1[u]}, pe[2] = {poff0[u + 1], poff1[u + 1]};
+                const int64_t sb[2] = {usz0[u], usz1[u]};
+                for (int g = 0; g < 2; g++) {
+                    int64_t s = sb[g];
+                    for (int64_t p = pb[g]; p < pe[g]; p++) {
+                        sym_slot[p] = s;
+                        s += S.numpar[sym_pairs[p].x] + S.numpar[sym_pairs[p].y];
+                    }
+                }
             }
-            for (int u = 0; u < T.nleaves; u++) in_cnt[u + 1] += in_cnt[u];
-            sym_in_off = in_cnt;
-            sym_in_slot.assign((size_t)sym_in_off[T.nleaves], 0);
-            std::vector<int64_t> fill(sym_in_off.begin(), sym_in_off.end() - 1);
-            for (size_t k = 0; k < sym_pairs.size(); k++) {
-                sym_in_slot[fill[unit_of[sym_pairs[k].x]]++] = sym_slot[k];
-                sym_in_slot[fill[unit_of[sym_pairs[k].y]]++] = sym_slot[k] + S.numpar[sym_pairs[k].x];
+            // per leaf the slices addressed to it, in partner order: its own
+            // side of the pairs it heads, the B side of the pairs headed by
+            // a partner (found through the partner's entry for this leaf)
+            sym_in_off = ioff;
+            sym_in_slot.resize((size_t)ioff[NU]);
+            std::vector<unsigned char> drop(ne, 0);
+#pragma omp parallel for schedule(static)
+            for (int u = 0; u < NU; u++) {
+                const int A = T.leaves[u];
+                int64_t w = ioff[u];
+                for (int64_t j = mx_doff[u]; j < far_end[u]; j++) {
+                    if (rev[j] < 0) continue;
+                    const int B = far[j];
+                    sym_in_slot[w++] = A < B ? sym_slot[pid[j]] : sym_slot[pid[rev[j]]] + S.numpar[B];
+                    drop[mx_doff[u] + fent[j]] = 1;
+                }
             }
+            pt.mark("plan: symmetric: pairs and slots");
             // both directions leave the per-target near-field lists
-            std::vector<int64_t> noff(T.nleaves + 1, 0);
-            for (int u = 0; u < T.nleaves; u++) {
-                int64_t c = 0;
-                for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) c += sym[k] ? 0 : 1;
-                noff[u + 1] = noff[u] + c;
-            }
-            std::vector<int> nidx((size_t)noff[T.nleaves]);
-            std::vector<unsigned char> nflag((size_t)noff[T.nleaves]);
+            std::vector<int64_t> noff(NU + 1, 0);
 #pragma omp parallel for schedule(static)
-            for (int u = 0; u < T.nleaves; u++) {
+            for (int u = 0; u < NU; u++) noff[u + 1] = (mx_doff[u + 1] - mx_doff[u]) - (ioff[u + 1] - ioff[u]);
+            for (int u = 0; u < NU; u++) noff[u + 1] += noff[u];
+            std::vector<int> nidx((size_t)noff[NU]);
+            std::vector<unsigned char> nflag((size_t)noff[NU]);
+#pragma omp parallel for schedule(static)
+            for (int u = 0; u < NU; u++) {
                 int64_t w = noff[u];
                 for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++)
-                    if (!sym[k]) { nidx[w] = mx_didx[k]; nflag[w] = mx_dflag[k]; w++; }
+                    if (!drop[k]) { nidx[w] = mx_didx[k]; nflag[w] = mx_dflag[k]; w++; }
             }
             mx_doff.swap(noff);
             mx_didx.swap(nidx);
             mx_dflag.swap(nflag);
         }
     }
-
     pt.mark("plan: symmetric near-field pairs");
     // Hermite upward pass: particle chunks of every source node
     std::vector<bt::HermChunk> hchunks;
@@ -1213,6 +1346,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     int2 *d_sym_pairs = nullptr;
     int64_t *d_sym_slot = nullptr, *d_sym_in_off = nullptr, *d_sym_in_slot = nullptr;
     float *d_sym_partial = nullptr;
+    double *d_sbox = nullptr;
     if (mixed) {
         L.add(&d_spos, ns); L.add(&d_tpos, nt);
         if (need_src_clusters) L.add(&d_Q32, (size_t)S.n * P * nq);
@@ -1221,6 +1355,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         L.add(&d_mxcpoff, mx_cpoff.size()); L.add(&d_mxcpidx, mx_cpidx.size());
         if (pl.a_deg) L.add(&d_adeg, n_approx);
         L.add(&d_srad, S.n); L.add(&d_trad, T.n);
+        if ((int64_t)sym_pairs.size() > sym_far_pairs) L.add(&d_sbox, 6 * (size_t)S.n);
         if (!sym_pairs.empty()) {
             L.add(&d_sym_pairs, sym_pairs.size()); L.add(&d_sym_slot, sym_slot.size());
             L.add(&d_sym_in_off, sym_in_off.size()); L.add(&d_sym_in_slot, sym_in_slot.size());
@@ -1290,6 +1425,15 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             UP(d_sctr, sctr.data(), sctr.size()); UP(d_tctr, tctr.data(), tctr.size());
             UP(d_mxdoff, mx_doff.data(), mx_doff.size()); UP(d_mxdidx, mx_didx.data(), mx_didx.size());
             UP(d_mxdflag, mx_dflag.data(), mx_dflag.size());
+            std::vector<double> sbox;
+            if (d_sbox) {
+                sbox.resize(6 * (size_t)S.n);
+                for (int i = 0; i < S.n; i++) {
+                    double *b = sbox.data() + 6 * (size_t)i;
+                    b[0] = S.x0[i]; b[1] = S.x1[i]; b[2] = S.y0[i]; b[3] = S.y1[i]; b[4] = S.z0[i]; b[5] = S.z1[i];
+                }
+                UP(d_sbox, sbox.data(), sbox.size());
+            }
             if (!sym_pairs.empty()) {
                 UP(d_sym_pairs, sym_pairs.data(), sym_pairs.size()); UP(d_sym_slot, sym_slot.data(), sym_slot.size());
                 UP(d_sym_in_off, sym_in_off.data(), sym_in_off.size()); UP(d_sym_in_slot, sym_in_slot.data(), sym_in_slot.size());
@@ -1313,6 +1457,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.tc_up = shape.tc_up && mixed && !herm;
         v.sharded = shape.nshards > 1;
         v.sym_npairs = (int)sym_pairs.size();
+        v.sym_far_pairs = (int)sym_far_pairs;
+        v.d_sbox = d_sbox;
         v.d_sym_pairs = d_sym_pairs; v.d_sym_slot = d_sym_slot; v.d_sym_in_off = d_sym_in_off;
         v.d_sym_in_slot = d_sym_in_slot; v.d_sym_partial = d_sym_partial;
         v.n = n; v.P = P; v.ns = ns; v.nt = nt; v.max_np1 = max_np1; v.kernel = o.kernel; v.kp = o.kp;
@@ -1684,10 +1830,6 @@ int parse_options(const bt_options *opts, bt_params &prm, bool &learned, double 
         if (opts->shard_index < 0 || opts->shard_index >= opts->shard_count) {
             set_err("shard index %d outside [0, %d)", opts->shard_index, opts->shard_count);
             return BT_ERR_PARAM;
-        }
-        if (prm.ctype != PARTICLE_CLUSTER) {
-            set_err("target sharding is provided for particle-cluster evaluations");
-            return BT_ERR_UNSUPPORTED;
         }
         shape.shard = opts->shard_index;
         shape.nshards = opts->shard_count;

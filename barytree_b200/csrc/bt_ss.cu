@@ -248,6 +248,22 @@ __global__ void k_axpy(int n, double c, const double *__restrict__ x, double *__
     if (i < n) y[i] += c * x[i];
 }
 
+// The correction over work items (unit, chunk of `chunk` targets): a
+// target-sharded call adds it to the targets of its own leaves only.  The
+// same operation as k_axpy, target by target.
+__global__ void k_axpy_items(const int2 *__restrict__ items, int chunk, const int *__restrict__ leaf_node,
+                             const int *__restrict__ ibeg, const int *__restrict__ numpar, double c,
+                             const double *__restrict__ x, double *__restrict__ y)
+{
+    const int2 it = items[blockIdx.x];
+    const int node = leaf_node[it.x];
+    const int end = min(numpar[node], (it.y + 1) * chunk);
+    for (int i = it.y * chunk + threadIdx.x; i < end; i += blockDim.x) {
+        const int t = ibeg[node] + i;
+        y[t] += c * x[t];
+    }
+}
+
 // SS direct sum over all sources (InteractionCompute_Direct with
 // singularity subtraction, src/interaction_compute/interaction_compute_direct.c:26-231):
 // one target per thread, sources staged through shared memory.
@@ -331,6 +347,12 @@ void launch_mul(int n, const double *a, const double *b, double *c, cudaStream_t
 void launch_ss_correction(int n, double c, const double *tq, double *pot, cudaStream_t st)
 {
     if (n > 0) k_axpy<<<(n + 255) / 256, 256, 0, st>>>(n, c, tq, pot);
+}
+
+void launch_ss_correction_items(int nitems, const int2 *items, int chunk, const int *leaf_node, const int *ibeg,
+                                const int *numpar, double c, const double *tq, double *pot, cudaStream_t st)
+{
+    if (nitems > 0) k_axpy_items<<<nitems, SS_THREADS, 0, st>>>(items, chunk, leaf_node, ibeg, numpar, c, tq, pot);
 }
 
 double ss_correction_constant(int kernel, double kp)

@@ -46,6 +46,9 @@ void launch_ss_direct(int kernel, int nt, int ns, const double *tx, const double
 void launch_mul(int n, const double *a, const double *b, double *c, cudaStream_t st);
 // pot[i] += c tq[i]
 void launch_ss_correction(int n, double c, const double *tq, double *pot, cudaStream_t st);
+// The same over work items (unit, chunk of `chunk` targets of the unit's leaf).
+void launch_ss_correction_items(int nitems, const int2 *items, int chunk, const int *leaf_node, const int *ibeg,
+                                const int *numpar, double c, const double *tq, double *pot, cudaStream_t st);
 double ss_correction_constant(int kernel, double kp);
 
 }  // namespace bt

@@ -1,15 +1,24 @@
 // bt_sym.cu -- symmetric near-field pairs of the mixed path.
 //
 // When the targets are the sources (same particles, same tree) and the
-// kernel is symmetric in r (Coulomb, regularized Coulomb), a pair of
+// kernel is symmetric in r (Coulomb, Yukawa, regularized Coulomb), a pair of
 // distinct leaves {A, B} that each hold the other in their near-field list
 // needs each pair distance once: 1/r_ij serves both phi_i (i in A, source j
 // in B) and phi_j (j in B, source i in A).  The reference evaluates the two
 // directions separately (src/interaction_compute/interaction_compute_pc.c,
 // direct list of each target batch); the sums are the same up to rounding.
-// Only pairs whose leaf boxes are too far apart to hold a close pair (the
-// mixed path's FP64 rule) are taken here; the rest stay in the
-// particle-output kernel.
+// Pairs of leaves whose boxes lie within the close-pair distance of each
+// other (touching leaves, mostly) can hold close pairs, which the mixed path
+// evaluates in FP64 from the FP64 particles.  Their kernel (CLAMP) raises
+// every FP32 r^2 to at least the close-pair distance squared, so a close
+// pair adds a bounded, known term (the kernel at that distance) to both
+// sides; before the main loop the block finds the particles of each leaf
+// that lie within that distance of the other leaf's box (a few per cent of
+// them, found in FP64), recomputes the FP32 r^2 of every pair among those
+// candidates with the main loop's own instructions, and for each pair
+// below the distance writes the FP64 kernel minus the clamped term into
+// both sides' slices.  The main loop's sums are added to these at the end.
+// Self pairs (A with A) stay in the particle-output kernel.
 //
 // Work: one block per pair.  The block's threads hold A's targets, four per
 // thread in two packed FP32 pairs, in chunks of 512; B's particles stream
@@ -25,7 +34,11 @@
 
 #include <cstdint>
 
+#include <cfloat>
+
 #include "bt_f2.cuh"
+#include "bt_kernels.cuh"
+#include "bt_mixed.h"
 #include "bt_sym.h"
 
 namespace bt {
@@ -55,12 +68,76 @@ __device__ __forceinline__ void rs_stage(float *v, int lane)
     }
 }
 
+// The kernel value of a packed pair of r^2 (the particle-output kernel's
+// arithmetic): Coulomb 1/r; regularised Coulomb 1/sqrt(r^2 + eps^2);
+// Yukawa with one Newton step on 1/r, then exp(-kappa r) by ex2.
 template <int KT>
+__device__ __forceinline__ f2_t sym_kval(f2_t r2, f2_t kc2)
+{
+    if (KT == 3) r2 = f2_fma(f2_make(1.0f, 1.0f), kc2, r2);
+    float ra, rb;
+    f2_split(r2, ra, rb);
+    f2_t k = f2_make(rsqrt_apx(ra), rsqrt_apx(rb));
+    if (KT == 2) {
+        const f2_t h = f2_mul(r2, k);
+        const f2_t t = f2_fma(f2_mul(h, f2_make(-0.5f, -0.5f)), k, f2_make(1.5f, 1.5f));
+        float e0, e1;
+        f2_split(f2_mul(kc2, f2_mul(h, t)), e0, e1);
+        k = f2_mul(f2_mul(k, t), f2_make(ex2_apx(e0), ex2_apx(e1)));
+    }
+    return k;
+}
+
+// The main loop's FP32 r^2 of one pair, with its instructions: x, y, z the
+// target in the source leaf's frame, p the source.
+__device__ __forceinline__ float sym_r2(float x, float y, float z, float4 p)
+{
+    const f2_t dx = f2_sub(f2_make(x, x), f2_make(p.x, p.x)), dy = f2_sub(f2_make(y, y), f2_make(p.y, p.y)),
+               dz = f2_sub(f2_make(z, z), f2_make(p.z, p.z));
+    float r2, unused;
+    f2_split(f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz))), r2, unused);
+    return r2;
+}
+
+// Indices i < n of the particles (FP64, from `base`) within distance d of
+// the box b (x0 x1 y0 y1 z0 z1), in index order, into out; returns how many.
+__device__ int near_box(int *out, int n, int base, const double *__restrict__ x, const double *__restrict__ y,
+                        const double *__restrict__ z, const double *b, double d, int *wcnt)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int total = 0;
+    for (int c0 = 0; c0 < n; c0 += SY_THREADS) {
+        const int i = c0 + threadIdx.x;
+        bool f = false;
+        if (i < n) {
+            const double px = x[base + i], py = y[base + i], pz = z[base + i];
+            const double gx = fmax(0.0, fmax(b[0] - px, px - b[1])), gy = fmax(0.0, fmax(b[2] - py, py - b[3])),
+                         gz = fmax(0.0, fmax(b[4] - pz, pz - b[5]));
+            f = gx * gx + gy * gy + gz * gz <= d * d;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wcnt[warp] = __popc(bal);
+        __syncthreads();
+        int off = total, all = 0;
+#pragma unroll
+        for (int w = 0; w < SY_WARPS; w++) {
+            off += w < warp ? wcnt[w] : 0;
+            all += wcnt[w];
+        }
+        if (f) out[off + __popc(bal & ((1u << lane) - 1u))] = i;
+        __syncthreads();
+        total += all;
+    }
+    return total;
+}
+
+template <int KT, bool CLAMP>
 __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
 {
     __shared__ __align__(16) f2_t tile[SY_TILE][4];     // {x, x}, {y, y}, {z, z}, {q, q}
     __shared__ float red[SY_WARPS][SY_TILE];
     __shared__ float accB[SYM_MAX_LEAF];
+    __shared__ double accA[SY_TPT][SY_THREADS];          // A side: each tile's FP32 sums, added in FP64
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int2 pr = a.pair[blockIdx.x];
     const int A = pr.x, B = pr.y;
@@ -70,7 +147,49 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
     // A's targets in B's frame: positions relative to A's centre minus the offset of B's
     const float ox = (float)(a.ctr[3 * B] - a.ctr[3 * A]), oy = (float)(a.ctr[3 * B + 1] - a.ctr[3 * A + 1]),
                 oz = (float)(a.ctr[3 * B + 2] - a.ctr[3 * A + 2]);
-    const f2_t kc2 = f2_make(a.kc, a.kc), one = f2_make(1.0f, 1.0f);
+    const f2_t kc2 = f2_make(a.kc, a.kc);
+    // the close-pair distance squared, as the particle-output kernel has it
+    float thr2 = 0.0f;
+    if (CLAMP) {
+        const double rr = MX_CLOSE_FRAC * (a.rad[A] + a.rad[B]);
+        thr2 = fmaxf((float)(rr * rr), FLT_MIN);
+        __shared__ int wcnt[SY_WARPS];
+        int *candA = reinterpret_cast<int *>(&tile[0][0]), *candB = candA + SYM_MAX_LEAF;
+        for (int i = threadIdx.x; i < na; i += SY_THREADS) outA[i] = 0.0f;
+        for (int j = threadIdx.x; j < nb; j += SY_THREADS) outB[j] = 0.0f;
+        // every pair with FP32 r^2 below thr2 lies within 1.01 thr of both boxes
+        const double d = 1.01 * sqrt((double)thr2);
+        const int nca = near_box(candA, na, ia, a.x64, a.y64, a.z64, a.box + 6 * B, d, wcnt);
+        const int ncb = near_box(candB, nb, ib, a.x64, a.y64, a.z64, a.box + 6 * A, d, wcnt);
+        if (nca > 0 && ncb > 0) {
+            float kcl, unused;
+            f2_split(sym_kval<KT>(f2_make(thr2, thr2), kc2), kcl, unused);   // the clamped term's kernel value
+            const double kcd = (double)kcl;
+            for (int k = threadIdx.x; k < nca + ncb; k += SY_THREADS) {
+                // thread k: candidate k of A (its sum over B's candidates), then of B
+                const bool sideA = k < nca;
+                const int i = sideA ? candA[k] : candB[k - nca];
+                const int gi = (sideA ? ia : ib) + i;
+                const float4 pi = a.pos[gi];
+                double c = 0.0;
+                for (int m = 0; m < (sideA ? ncb : nca); m++) {
+                    const int j = sideA ? candB[m] : candA[m];
+                    const int gj = (sideA ? ib : ia) + j;
+                    const float4 pj = a.pos[gj];
+                    // the pair's r^2 as the main loop forms it: A's target in B's frame
+                    const float r2 = sideA ? sym_r2(pi.x - ox, pi.y - oy, pi.z - oz, pj)
+                                           : sym_r2(pj.x - ox, pj.y - oy, pj.z - oz, pi);
+                    if (r2 < thr2) {
+                        const double ex = a.x64[gi] - a.x64[gj], ey = a.y64[gi] - a.y64[gj],
+                                     ez = a.z64[gi] - a.z64[gj];
+                        c += k_pp<KT>(ex * ex + ey * ey + ez * ez, a.q64[gj], a.kp) - (double)pj.w * kcd;
+                    }
+                }
+                (sideA ? outA[i] : outB[i]) = (float)c;
+            }
+        }
+        __syncthreads();                                  // the candidate lists live in the tile
+    }
     for (int j = threadIdx.x; j < nb; j += SY_THREADS) accB[j] = 0.0f;
     for (int c0 = 0; c0 < na; c0 += SY_CHUNK) {
         // targets c0 + threadIdx.x + k * SY_THREADS, k = 0..3, packed as (0, 1), (2, 3)
@@ -88,6 +207,8 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
             QT[p] = f2_make(act[2 * p] ? p0.w : 0.0f, act[2 * p + 1] ? p1.w : 0.0f);   // absent targets add nothing
             S[p] = f2_make(0.0f, 0.0f);
         }
+#pragma unroll
+        for (int k = 0; k < SY_TPT; k++) accA[k][threadIdx.x] = 0.0;
         for (int s0 = 0; s0 < nb; s0 += SY_TILE) {
             const int cm = min(SY_TILE, nb - s0), cmb = (cm + SY_SB - 1) & ~(SY_SB - 1);
             __syncthreads();                              // the previous tile is done with
@@ -110,10 +231,12 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
                     for (int p = 0; p < 2; p++) {
                         const f2_t dx = f2_sub(X[p], xy.x), dy = f2_sub(Y[p], xy.y), dz = f2_sub(Z[p], zq.x);
                         f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
-                        if (KT == 3) r2 = f2_fma(one, kc2, r2);
-                        float ra, rb;
-                        f2_split(r2, ra, rb);
-                        rinv[p] = f2_make(rsqrt_apx(ra), rsqrt_apx(rb));
+                        if (CLAMP) {
+                            float ra, rb;
+                            f2_split(r2, ra, rb);
+                            r2 = f2_make(fmaxf(ra, thr2), fmaxf(rb, thr2));
+                        }
+                        rinv[p] = sym_kval<KT>(r2, kc2);      // serves both sides
                         S[p] = f2_fma(zq.y, rinv[p], S[p]);
                     }
                     // B side: the four targets' charges over r, folded into one value
@@ -129,6 +252,15 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
                 v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
                 if ((lane & 1) == 0) red[warp][sb + (lane >> 1)] = v[0];
             }
+            // the tile's A-side sums into FP64 (FP32 chains of at most one tile)
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                float lo, hi;
+                f2_split(S[p], lo, hi);
+                accA[2 * p][threadIdx.x] += (double)lo;
+                accA[2 * p + 1][threadIdx.x] += (double)hi;
+                S[p] = f2_make(0.0f, 0.0f);
+            }
             __syncthreads();
             // the block's B-side sum per source, warps in a fixed order
             for (int j = threadIdx.x; j < cm; j += SY_THREADS) {
@@ -139,16 +271,13 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
             }
         }
 #pragma unroll
-        for (int p = 0; p < 2; p++) {
-            float lo, hi;
-            f2_split(S[p], lo, hi);
-            const int t0 = c0 + threadIdx.x + (2 * p) * SY_THREADS, t1 = t0 + SY_THREADS;
-            if (act[2 * p]) outA[t0] = lo;
-            if (act[2 * p + 1]) outA[t1] = hi;
+        for (int k = 0; k < SY_TPT; k++) {
+            const int t = c0 + threadIdx.x + k * SY_THREADS;
+            if (act[k]) outA[t] = (float)(CLAMP ? accA[k][threadIdx.x] + (double)outA[t] : accA[k][threadIdx.x]);
         }
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < nb; j += SY_THREADS) outB[j] = accB[j];
+    for (int j = threadIdx.x; j < nb; j += SY_THREADS) outB[j] = CLAMP ? accB[j] + outB[j] : accB[j];
 }
 
 __global__ void k_sym_gather(SymGatherArgs a)
@@ -170,8 +299,17 @@ __global__ void k_sym_gather(SymGatherArgs a)
 void launch_pp_sym(int kernel, const SymArgs &a, cudaStream_t st)
 {
     if (a.npairs <= 0) return;
-    if (kernel == 3) k_pp_sym<3><<<a.npairs, SY_THREADS, 0, st>>>(a);
-    else k_pp_sym<1><<<a.npairs, SY_THREADS, 0, st>>>(a);
+    if (kernel == 3) k_pp_sym<3, false><<<a.npairs, SY_THREADS, 0, st>>>(a);
+    else if (kernel == 2) k_pp_sym<2, false><<<a.npairs, SY_THREADS, 0, st>>>(a);
+    else k_pp_sym<1, false><<<a.npairs, SY_THREADS, 0, st>>>(a);
+}
+
+void launch_pp_sym_close(int kernel, const SymArgs &a, cudaStream_t st)
+{
+    if (a.npairs <= 0) return;
+    if (kernel == 3) k_pp_sym<3, true><<<a.npairs, SY_THREADS, 0, st>>>(a);
+    else if (kernel == 2) k_pp_sym<2, true><<<a.npairs, SY_THREADS, 0, st>>>(a);
+    else k_pp_sym<1, true><<<a.npairs, SY_THREADS, 0, st>>>(a);
 }
 
 void launch_sym_gather(const SymGatherArgs &a, cudaStream_t st)

@@ -18,6 +18,11 @@ struct SymArgs {
     const float4 *pos;            // particles relative to their leaf centre, with charge
     float *partial;               // per pair, per particle of A then of B: the pair's potential there
     float kc;                     // mixed_kernel_constant()
+    // pairs of leaves within the close-pair distance of each other (launch_pp_sym_close)
+    const double *rad;            // node radii
+    const double *box;            // node boxes, x0 x1 y0 y1 z0 z1 per node
+    const double *x64, *y64, *z64, *q64;   // FP64 particles in tree order
+    double kp;                    // kernel parameter (FP64 close pairs)
 };
 
 struct SymGatherArgs {
@@ -30,7 +35,12 @@ struct SymGatherArgs {
     double *pot;                  // += the sum of the partial vectors, FP64, in that order
 };
 
+// Pairs whose leaf boxes are farther apart than the close-pair distance.
 void launch_pp_sym(int kernel, const SymArgs &a, cudaStream_t st);
+// Pairs whose boxes lie within it: FP32 distances below the close-pair
+// distance are clamped to it, and each clamped pair's two terms are replaced
+// by FP64 ones (from the FP64 particles) before the slices are written.
+void launch_pp_sym_close(int kernel, const SymArgs &a, cudaStream_t st);
 void launch_sym_gather(const SymGatherArgs &a, cudaStream_t st);
 
 }  // namespace bt

@@ -102,16 +102,19 @@ typedef struct bt_options {
     int upward;           /* mixed Lagrange upward pass: BT_UPWARD_AUTO (default: leaf
                              P2M on the tensor cores in 3xTF32 where (n+1)^2 <= 128)
                              or BT_UPWARD_FP64 (FP64 SIMT, as the FP64 path)         */
-    /* Target sharding (particle-cluster): with shard_count > 1 the call
-     * evaluates shard_index's share of the target leaves (contiguous in tree
-     * order, equal estimated cost) and leaves the other potentials 0; the sum
-     * of the outputs of all shards is the unsharded result with
-     * BT_SYMMETRY_OFF, bit for bit (shards do not pair leaves across shards).
-     * Trees, lists and proxies are built in full by every shard.            */
+    /* Target sharding: with shard_count > 1 the call evaluates shard_index's
+     * share of the target leaves (contiguous in tree order, equal estimated
+     * cost) and leaves the other potentials 0; the sum of the outputs of all
+     * shards is the unsharded result with BT_SYMMETRY_OFF, bit for bit
+     * (shards do not pair leaves across shards).  Trees, lists and proxies
+     * are built in full by every shard; with target grids (cluster-particle,
+     * cluster-cluster) a shard evaluates the grids of its leaves and their
+     * ancestors only, so the grids of shared ancestors are evaluated by
+     * every shard that holds a leaf under them.                            */
     int shard_index;
     int shard_count;
     int symmetry;         /* mixed path, targets = sources (all of a batch's systems),
-                             Coulomb or regularized Coulomb, leaves of at most 2048
+                             Coulomb, Yukawa or regularized Coulomb, leaves of at most 2048
                              particles, not sharded: BT_SYMMETRY_AUTO (default)
                              evaluates each pair of near-field leaves that list each
                              other (and can hold no close pair) once for both sides;

@@ -1,11 +1,11 @@
 """GPU tests of target sharding (bt_options.shard_index / shard_count), the
-multi-GPU decomposition of one particle-cluster system: every shard builds
-the trees, lists and proxies, evaluates a contiguous run of target leaves of
-about equal cost and leaves the other potentials 0, so one all-reduce (sum)
-over the shards gives the result.  Here the shards run one after another on
-one GPU: their sum must equal the unsharded potentials bit for bit, every
-target must come from exactly one shard, and the shards' costs must be
-balanced."""
+multi-GPU decomposition of one system: every shard builds the trees, lists
+and proxies, evaluates a contiguous run of target leaves of about equal cost
+(with target grids, the grids of those leaves and their ancestors) and
+leaves the other potentials 0, so one all-reduce (sum) over the shards gives
+the result.  Here the shards run one after another on one GPU: their sum
+must equal the unsharded potentials bit for bit, every target must come from
+exactly one shard, and the shards' costs must be balanced."""
 import numpy as np
 import pytest
 
@@ -62,3 +62,45 @@ def test_one_shard_is_the_unsharded_call():
     assert np.array_equal(B.treecode(tx, ty, tz, sx, sy, sz, sq, shard=(0, 1), **kw),
                           B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw))
     # one shard of one is no sharding: the symmetric pass stays on
+    x, y, z, q = _clustered(40000, 34)
+    assert np.array_equal(B.treecode(x, y, z, x, y, z, q, shard=(0, 1), **kw),
+                          B.treecode(x, y, z, x, y, z, q, **kw))
+
+
+# cluster-particle and cluster-cluster: target grids split by subtree; with
+# singularity subtraction the correction term belongs to the shard's targets
+GRID_CASES = [
+    dict(compute_type=B.ComputeType.CLUSTER_CLUSTER, kernel=B.Kernel.YUKAWA, kernel_param=[0.5],
+         precision=B.PRECISION_FP64, nshards=2),
+    dict(compute_type=B.ComputeType.CLUSTER_CLUSTER, kernel=B.Kernel.COULOMB, kernel_param=[],
+         precision=B.PRECISION_MIXED, nshards=3),
+    dict(compute_type=B.ComputeType.CLUSTER_PARTICLE, kernel=B.Kernel.COULOMB, kernel_param=[],
+         approximation=B.Approximation.HERMITE, precision=B.PRECISION_FP64, nshards=2),
+    dict(compute_type=B.ComputeType.CLUSTER_PARTICLE, kernel=B.Kernel.YUKAWA, kernel_param=[0.5],
+         precision=B.PRECISION_MIXED, nshards=4),
+    dict(compute_type=B.ComputeType.CLUSTER_CLUSTER, kernel=B.Kernel.COULOMB, kernel_param=[0.5],
+         singularity=B.Singularity.SUBTRACTION, precision=B.PRECISION_FP64, nshards=2),
+    dict(compute_type=B.ComputeType.PARTICLE_CLUSTER, kernel=B.Kernel.YUKAWA, kernel_param=[0.5],
+         singularity=B.Singularity.SUBTRACTION, precision=B.PRECISION_FP64, nshards=3),
+]
+
+
+@pytest.mark.parametrize("case", GRID_CASES, ids=["cc-yukawa-fp64", "cc-coulomb-mixed", "cp-hermite-fp64",
+                                                  "cp-yukawa-mixed", "cc-subtraction-fp64",
+                                                  "pc-subtraction-fp64"])
+def test_sum_of_grid_and_subtraction_shards_is_the_unsharded_result(case):
+    case = dict(case)
+    nshards = case.pop("nshards")
+    x, y, z, q = _clustered(150000, 35)
+    rng = np.random.default_rng(36)
+    kw = dict(theta=0.8, degree=6, max_source_leaf=600, max_target_leaf=600, size_check=1.0, **case)
+    if case.get("singularity") == B.Singularity.SUBTRACTION:
+        kw.update(target_q=q.copy(), source_w=rng.uniform(0.5, 1.5, len(q)))
+    tx, ty, tz = x + 1e-3, y.copy(), z.copy()          # targets apart from the sources
+    full = B.treecode(tx, ty, tz, x, y, z, q, **kw)
+    parts = [B.treecode(tx, ty, tz, x, y, z, q, shard=(k, nshards), **kw) for k in range(nshards)]
+    assert np.array_equal(np.sum(parts, axis=0), full)
+    nonzero = np.array([p != 0 for p in parts])
+    assert np.all(nonzero.sum(axis=0) == 1)
+    counts = nonzero.sum(axis=1)
+    assert counts.min() > 0.3 * len(tx) / nshards

@@ -76,5 +76,8 @@ def test_shard_arguments_are_checked_before_any_device_use():
         B.treecode(x, y, z, x, y, z, q, precision=B.PRECISION_MIXED, shard=(3, 3))
     assert e.value.code == B.BT_ERR_PARAM
     with pytest.raises(B.BaryTreeError) as e:
-        B.treecode(x, y, z, x, y, z, q, compute_type=B.ComputeType.CLUSTER_CLUSTER, shard=(0, 2))
-    assert e.value.code == B.BT_ERR_UNSUPPORTED
+        B.treecode(x, y, z, x, y, z, q, compute_type=B.ComputeType.CLUSTER_CLUSTER, shard=(-1, 2))
+    assert e.value.code == B.BT_ERR_PARAM and "shard index" in B.last_error()
+    with pytest.raises(B.BaryTreeError) as e:
+        B.treecode(x, y, z, x, y, z, q, compute_type=B.ComputeType.CLUSTER_PARTICLE, shard=(0, -2))
+    assert e.value.code == B.BT_ERR_PARAM and "shard count" in B.last_error()
