@@ -22,6 +22,8 @@
 #include <mutex>
 #include <omp.h>
 #include <sys/resource.h>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/barytree_b200.h"
@@ -84,6 +86,32 @@ struct PhaseTimer {
     }
 };
 
+// Host vectors whose elements are left uninitialised on construction and
+// resize (trivial types): the planning passes write every element they read,
+// in parallel, instead of a serial zero fill of tens of MB per call.
+template <typename T>
+struct NoInit : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInit<U>;
+    };
+    NoInit() = default;
+    template <typename U>
+    NoInit(const NoInit<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value)
+    {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U *p, Args &&...args)
+    {
+        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <typename T>
+using hvec = std::vector<T, NoInit<T>>;
+
 // Grow-only device arena per device, reused across calls so steady-state
 // calls do not touch cudaMalloc.
 struct Arena {
@@ -109,9 +137,17 @@ struct Arena {
     }
 };
 
+// A second stream and its fork / join events: work that is independent of
+// the main stream's next kernels runs beside them.
+struct Fork {
+    cudaStream_t side = nullptr, side2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
+};
+
 struct DeviceCtx {
     int device = -1;
     cudaStream_t stream = nullptr;
+    Fork fk;
     Arena arena;
     Arena tree_arena;       // particles in tree order (GPU tree build), kept through the call
     cudaEvent_t ev[8] = {};
@@ -180,6 +216,14 @@ int get_ctx(int device, DeviceCtx **out)
             return BT_ERR_CUDA;
         }
         for (auto &e : c.ev) cudaEventCreate(&e);
+        if (cudaStreamCreateWithFlags(&c.fk.side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&c.fk.side2, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c.fk.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c.fk.join, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c.fk.join2, cudaEventDisableTiming) != cudaSuccess) {
+            set_err("stream creation failed");
+            return BT_ERR_CUDA;
+        }
         c.device = device;
     }
     *out = &c;
@@ -317,15 +361,20 @@ void fill_grids(const bt_tree &t, int n, std::vector<double> &grid, std::vector<
 // starts the longest work first.
 std::vector<int2> make_items(int units, const int *count_of_unit, int chunk, const std::vector<double> &cost)
 {
-    std::vector<std::pair<double, int2>> v;
-    for (int u = 0; u < units; u++) {
-        int m = count_of_unit[u];
-        int nch = (m + chunk - 1) / chunk;
-        for (int c = 0; c < nch; c++) v.push_back({cost[u], make_int2(u, c)});
-    }
-    std::stable_sort(v.begin(), v.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
-    std::vector<int2> out(v.size());
-    for (size_t i = 0; i < v.size(); i++) out[i] = v[i].second;
+    // the items of a unit share its cost: a stable sort of the units, each
+    // then expanded into its chunks in order, is the stable sort of the items
+    std::vector<int> ord;
+    size_t n = 0;
+    for (int u = 0; u < units; u++)
+        if (count_of_unit[u] > 0) {
+            ord.push_back(u);
+            n += (size_t)((count_of_unit[u] + chunk - 1) / chunk);
+        }
+    std::stable_sort(ord.begin(), ord.end(), [&cost](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<int2> out;
+    out.reserve(n);
+    for (int u : ord)
+        for (int c = 0; c < (count_of_unit[u] + chunk - 1) / chunk; c++) out.push_back(make_int2(u, c));
     return out;
 }
 
@@ -400,7 +449,7 @@ void leaf_ranges(const bt_tree &t, std::vector<int> &first, std::vector<int> &co
 
 // Replace every node entry of a CSR by the leaves under it, in DFS order.
 void expand_to_leaves(const bt_csr &in, const bt_tree &t, const std::vector<int> &first,
-                      const std::vector<int> &count, std::vector<int64_t> &off, std::vector<int> &idx)
+                      const std::vector<int> &count, std::vector<int64_t> &off, hvec<int> &idx)
 {
     off.assign(in.rows + 1, 0);
 #pragma omp parallel for schedule(static)
@@ -654,7 +703,7 @@ bt::MixedTargetsArgs mixed_targets_args(const DevPlan &v)
 // pass, and the scatter of the potentials into caller order at scatter_out.
 // ev: 5 events bracketing the phases, or nullptr.
 int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatter_out, long long &launches,
-               bool capturing = false)
+               bool capturing = false, const Fork *fk = nullptr)
 {
     // inside a stream capture an event becomes a record node of the graph
     // only when recorded as external
@@ -849,8 +898,18 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         launches++;
     } else if (nt > 0 && mixed) {
         const bt::MixedTargetsArgs a = mixed_targets_args(v);
-        bt::launch_eval_targets_mixed(v.kernel, a, st);
-        launches++;
+        // the symmetric pairs write only their own partial sums: their two
+        // kernels run beside the particle-output kernel on two more streams,
+        // joined before the gather adds them into the potentials
+        const bool fork = v.sym_npairs > 0 && fk && fk->side && fk->side2;
+        cudaStream_t sst = st, sst2 = st;
+        if (fork) {
+            CK(cudaEventRecord(fk->fork, st));
+            CK(cudaStreamWaitEvent(fk->side, fk->fork, 0));
+            CK(cudaStreamWaitEvent(fk->side2, fk->fork, 0));
+            sst = fk->side;
+            sst2 = fk->side2;
+        }
         if (v.sym_npairs > 0) {
             bt::SymArgs y;
             y.npairs = v.sym_npairs; y.pair = v.d_sym_pairs; y.slot = v.d_sym_slot;
@@ -863,13 +922,25 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
             yc.npairs = v.sym_npairs - v.sym_far_pairs;
             yc.pair += v.sym_far_pairs;
             yc.slot += v.sym_far_pairs;
-            bt::launch_pp_sym(v.kernel, y, st);
-            bt::launch_pp_sym_close(v.kernel, yc, st);
+            bt::launch_pp_sym(v.kernel, y, sst);
+            bt::launch_pp_sym_close(v.kernel, yc, sst2);
+            launches += (y.npairs > 0) + (yc.npairs > 0);
+        }
+        bt::launch_eval_targets_mixed(v.kernel, a, st);
+        launches++;
+        if (fork) {
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(fk->join, sst));
+            CK(cudaEventRecord(fk->join2, sst2));
+            CK(cudaStreamWaitEvent(st, fk->join, 0));
+            CK(cudaStreamWaitEvent(st, fk->join2, 0));
+        }
+        if (v.sym_npairs > 0) {
             bt::SymGatherArgs g;
             g.nleaves = v.T_nleaves; g.leaf_node = v.d_tleaves; g.ibeg = v.d_sibeg; g.numpar = v.d_snum;
             g.in_off = v.d_sym_in_off; g.in_slot = v.d_sym_in_slot; g.partial = v.d_sym_partial; g.pot = d_pot;
             bt::launch_sym_gather(g, st);
-            launches += 1 + (y.npairs > 0) + (yc.npairs > 0);
+            launches++;
         }
     } else if (nt > 0) {
         bt::EvalTargetsArgs a;
@@ -1093,8 +1164,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     // then can a pair be close, or a target coincide with a source)
     std::vector<double> sctr, tctr;
     std::vector<int64_t> mx_doff, mx_cpoff;
-    std::vector<int> mx_didx, mx_cpidx;
-    std::vector<unsigned char> mx_dflag;
+    hvec<int> mx_didx, mx_cpidx;
+    hvec<unsigned char> mx_dflag;
     if (mixed) {
         sctr.resize(3 * (size_t)S.n);
         tctr.resize(3 * (size_t)T.n);
@@ -1127,8 +1198,9 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     // first, then the pairs within it (their own kernel); each group is
     // numbered by head unit (A < B), then by partner node, so the numbering
     // does not depend on the thread count.
-    std::vector<int2> sym_pairs;
-    std::vector<int64_t> sym_slot, sym_in_off, sym_in_slot;
+    hvec<int2> sym_pairs;
+    hvec<int64_t> sym_slot, sym_in_slot;
+    std::vector<int64_t> sym_in_off;
     int64_t sym_total = 0, sym_far_pairs = 0;
     int max_leaf = 0;
     for (int u = 0; u < T.nleaves; u++) max_leaf = std::max(max_leaf, T.numpar[T.leaves[u]]);
@@ -1141,8 +1213,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         // per unit: its partners (other leaves), sorted by node, each with the
         // list entry it came from and whether the boxes are within the
         // close-pair distance (the same test from both sides)
-        std::vector<int> far(ne), fent(ne);
-        std::vector<unsigned char> fnear(ne);
+        hvec<int> far(ne), fent(ne);
+        hvec<unsigned char> fnear(ne);
         std::vector<int64_t> far_end(NU);
 #pragma omp parallel
         {
@@ -1170,7 +1242,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         pt.mark("plan: symmetric: sorted partners");
         // rev[j]: where the partner's sorted list holds this unit's leaf (-1:
         // nowhere, the entry stays one-directional)
-        std::vector<int64_t> rev(ne, -1);
+        hvec<int64_t> rev(ne);
         std::vector<int64_t> poff0(NU + 1, 0), poff1(NU + 1, 0), ioff(NU + 1, 0);
 #pragma omp parallel for schedule(static)
         for (int u = 0; u < NU; u++) {
@@ -1180,6 +1252,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
                 const int B = far[j], ub = unit_of[B];
                 const int *b0 = far.data() + mx_doff[ub], *b1 = far.data() + far_end[ub];
                 const int *it = std::lower_bound(b0, b1, A);
+                rev[j] = -1;
                 if (it != b1 && *it == A) {
                     rev[j] = it - far.data();
                     all++;
@@ -1202,7 +1275,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         if (npairs > 0) {
             // pairs headed by each unit, and the pair number of each head entry
             sym_pairs.resize((size_t)npairs);
-            std::vector<int64_t> pid(ne, -1), usz0(NU + 1, 0), usz1(NU + 1, 0);
+            hvec<int64_t> pid(ne);
+            std::vector<int64_t> usz0(NU + 1, 0), usz1(NU + 1, 0);
 #pragma omp parallel for schedule(static)
             for (int u = 0; u < NU; u++) {
                 const int A = T.leaves[u];
@@ -1240,11 +1314,12 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             // a partner (found through the partner's entry for this leaf)
             sym_in_off = ioff;
             sym_in_slot.resize((size_t)ioff[NU]);
-            std::vector<unsigned char> drop(ne, 0);
+            hvec<unsigned char> drop(ne);
 #pragma omp parallel for schedule(static)
             for (int u = 0; u < NU; u++) {
                 const int A = T.leaves[u];
                 int64_t w = ioff[u];
+                std::fill(drop.begin() + mx_doff[u], drop.begin() + mx_doff[u + 1], (unsigned char)0);
                 for (int64_t j = mx_doff[u]; j < far_end[u]; j++) {
                     if (rev[j] < 0) continue;
                     const int B = far[j];
@@ -1258,8 +1333,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
 #pragma omp parallel for schedule(static)
             for (int u = 0; u < NU; u++) noff[u + 1] = (mx_doff[u + 1] - mx_doff[u]) - (ioff[u + 1] - ioff[u]);
             for (int u = 0; u < NU; u++) noff[u + 1] += noff[u];
-            std::vector<int> nidx((size_t)noff[NU]);
-            std::vector<unsigned char> nflag((size_t)noff[NU]);
+            hvec<int> nidx((size_t)noff[NU]);
+            hvec<unsigned char> nflag((size_t)noff[NU]);
 #pragma omp parallel for schedule(static)
             for (int u = 0; u < NU; u++) {
                 int64_t w = noff[u];
@@ -1544,7 +1619,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
             goto done;
         }
         pt.mark("plan: device arrays and uploads");
-        rc = issue_plan(v, st, ev, out_on_device ? out : d_out, launches);
+        rc = issue_plan(v, st, ev, out_on_device ? out : d_out, launches, false, &ctx->fk);
         if (rc != BT_OK) goto done;
         if (!out_on_device && nt > 0)
             CK(cudaMemcpyAsync(out, d_out, sizeof(double) * nt, cudaMemcpyDeviceToHost, st));
@@ -1695,8 +1770,10 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             aoff[u + 1] += aoff[u];
             doff[u + 1] += doff[u];
         }
-        std::vector<int> aidx((size_t)aoff[rows]), didx((size_t)doff[rows]);
-        std::vector<unsigned char> adeg((size_t)aoff[rows]);
+        // the new lists, filled in parallel straight into their final arrays
+        int *aidx = (int *)malloc(sizeof(int) * ((size_t)aoff[rows] + 1));
+        int *didx = (int *)malloc(sizeof(int) * ((size_t)doff[rows] + 1));
+        unsigned char *adeg = (unsigned char *)malloc((size_t)aoff[rows] + 1);
         long long hist[14] = {};
 #pragma omp parallel
         {
@@ -1720,13 +1797,10 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         pl.t_approx.rows = pl.t_direct.rows = rows;
         pl.t_approx.off = aoff;
         pl.t_direct.off = doff;
-        pl.t_approx.idx = (int *)malloc(sizeof(int) * (aidx.size() + 1));
-        pl.t_direct.idx = (int *)malloc(sizeof(int) * (didx.size() + 1));
-        memcpy(pl.t_approx.idx, aidx.data(), sizeof(int) * aidx.size());
-        memcpy(pl.t_direct.idx, didx.data(), sizeof(int) * didx.size());
+        pl.t_approx.idx = aidx;
+        pl.t_direct.idx = didx;
         free(pl.a_deg);
-        pl.a_deg = (unsigned char *)malloc(adeg.size() + 1);
-        memcpy(pl.a_deg, adeg.data(), adeg.size());
+        pl.a_deg = adeg;
     }
     pt.mark("selection: list rewrite (host)");
 done:
@@ -2656,7 +2730,7 @@ int bt_session_create(int numSystems, const long long *targetOffsets, const long
         if (e == cudaSuccess) {
             bt::launch_gather(ns, sorder, S->d_qin, (double *)S->v.d_sq, st);
             long long launches = 1;
-            int rc2 = issue_plan(S->v, st, S->ev, S->v.d_out, launches, true);
+            int rc2 = issue_plan(S->v, st, S->ev, S->v.d_out, launches, true, &ctx->fk);
             e = cudaStreamEndCapture(st, &S->graph);
             if (rc2 != BT_OK) rc = rc2;
             S->graph_kernels = launches;
