@@ -378,15 +378,24 @@ class Session:
         _check(rc)
         self._h = h
 
-    def evaluate(self, charges, return_report=False):
-        """Potentials per system for new source charges (one array per system, or concatenated)."""
+    def evaluate(self, charges, return_report=False, out=None):
+        """Potentials per system for new source charges (one array per system, or concatenated).
+
+        out: optional float64 array of all systems' targets (concatenated),
+        reused across calls by an iterative solver; the potentials are
+        written there and the per-system results are views of it.  Without
+        it each call returns fresh arrays."""
         q = _c(np.concatenate(charges) if isinstance(charges, (list, tuple)) else charges)
         if len(q) != self.soff[-1]:
             raise BaryTreeError(BT_ERR_PARAM, f"expected {self.soff[-1]} charges, got {len(q)}")
-        out = np.zeros(int(self.toff[-1]))
+        nt = int(self.toff[-1])
+        if out is not None and (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (nt,)
+                                or not out.flags.c_contiguous):
+            raise BaryTreeError(BT_ERR_PARAM, f"out must be a contiguous float64 array of {nt} values")
+        buf = out if out is not None else np.empty(nt)
         rep = Report()
-        _check(lib().bt_session_eval(self._h, _p(q), _p(out), ctypes.byref(rep)))
-        pots = [out[self.toff[k]:self.toff[k + 1]].copy() for k in range(len(self.toff) - 1)]
+        _check(lib().bt_session_eval(self._h, _p(q), _p(buf), ctypes.byref(rep)))
+        pots = [buf[self.toff[k]:self.toff[k + 1]] for k in range(len(self.toff) - 1)]
         return (pots, rep.as_dict()) if return_report else pots
 
     def close(self):

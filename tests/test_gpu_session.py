@@ -59,3 +59,27 @@ def test_session_rejects_wrong_charge_count():
     s = B.Session([(tx, ty, tz, sx, sy, sz, sq)], degree=4, max_source_leaf=100, max_target_leaf=100)
     with pytest.raises(B.BaryTreeError):
         s.evaluate(sq[:-1])
+
+
+def test_session_writes_into_a_reused_output_array():
+    rng = np.random.default_rng(9)
+    systems = []
+    for n in (5000, 12000):
+        x, y, z = (rng.uniform(-1, 1, n) for _ in range(3))
+        systems.append((x, y, z, x.copy(), y.copy(), z.copy(), rng.uniform(-1, 1, n)))
+    kw = dict(degree=6, max_source_leaf=400, max_target_leaf=400, precision=B.PRECISION_MIXED)
+    s = B.Session(systems, **kw)
+    out = np.full(17000, np.nan)
+    for _ in range(2):
+        q2 = [rng.uniform(-1, 1, len(t[6])) for t in systems]
+        got = s.evaluate(q2, out=out)
+        fresh = s.evaluate(q2)
+        for g, f in zip(got, fresh):
+            assert np.array_equal(g, f)
+            assert np.shares_memory(g, out)
+        assert np.array_equal(np.concatenate(got), out)
+    with pytest.raises(B.BaryTreeError):
+        s.evaluate(q2, out=np.empty(16999))
+    with pytest.raises(B.BaryTreeError):
+        s.evaluate(q2, out=np.empty(17000, dtype=np.float32))
+    s.close()
