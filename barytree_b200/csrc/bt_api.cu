@@ -339,7 +339,7 @@ void hermite_ww(int n, double *ww)
 // Chebyshev grids of every node: x0 + (cos(i pi / n) + 1) / 2 (x1 - x0) per
 // axis, the same operations as bt_cheb_nodes (src/clusters/clusters.c:857-862)
 // with the n+1 factors (cos + 1) / 2 computed once per call.
-void fill_grids(const bt_tree &t, int n, std::vector<double> &grid, std::vector<double> &len)
+void fill_grids(const bt_tree &t, int n, hvec<double> &grid, hvec<double> &len)
 {
     const int np1 = n + 1;
     double h[BT_MAX_DEGREE + 1];
@@ -1021,21 +1021,28 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     PhaseTimer pt;
     long long launches = 0;
 
-    std::vector<double> sgrid, slen, tgrid, tlen;
+    hvec<double> sgrid, slen, tgrid, tlen;
     fill_grids(S, n, sgrid, slen);
     fill_grids(T, n, tgrid, tlen);
     pt.mark("plan: grids at the base degree");
     // further degrees used by a learned per-interaction selection (mixed path)
     std::vector<int> xdeg;
-    std::vector<std::vector<double>> xgrid;
+    std::vector<hvec<double>> xgrid;
     int64_t n_approx = pl.t_approx.off[pl.t_approx.rows];
     if (pl.a_deg) {
         bool used[BT_MAX_DEGREE + 1] = {};
-        for (int64_t k = 0; k < n_approx; k++) used[pl.a_deg[k]] = true;
+#pragma omp parallel
+        {
+            bool u[BT_MAX_DEGREE + 1] = {};
+#pragma omp for schedule(static)
+            for (int64_t k = 0; k < n_approx; k++) u[pl.a_deg[k]] = true;
+#pragma omp critical
+            for (int d = 0; d <= BT_MAX_DEGREE; d++) used[d] = used[d] || u[d];
+        }
         for (int d = 1; d <= BT_MAX_DEGREE; d++)
             if (used[d] && d != n) xdeg.push_back(d);
         xgrid.resize(xdeg.size());
-        std::vector<double> tmp;
+        hvec<double> tmp;
         for (size_t i = 0; i < xdeg.size(); i++) fill_grids(S, xdeg[i], xgrid[i], tmp);
     }
     pt.mark("plan: grids at the selected degrees");
@@ -1050,9 +1057,10 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         for (int d = 0; d <= BT_MAX_DEGREE; d++) slot[d] = -1;
         for (size_t i = 0; i < X; i++) slot[xdeg[i]] = (int)i;
         std::vector<unsigned char> need((size_t)S.n * X, 0);
+#pragma omp parallel for schedule(static)
         for (int64_t k = 0; k < n_approx; k++) {
             const int sl = slot[pl.a_deg[k]];
-            if (sl >= 0) need[(size_t)pl.t_approx.idx[k] * X + sl] = 1;
+            if (sl >= 0) __atomic_store_n(&need[(size_t)pl.t_approx.idx[k] * X + sl], (unsigned char)1, __ATOMIC_RELAXED);
         }
         for (int v = 0; v < S.n; v++)
             for (int c = 0; c < S.nchild[v]; c++) {
@@ -2375,8 +2383,8 @@ long bt_selector_training_data(int n, const double *x, const double *y, const do
     std::vector<double> sctr, srad, tctr, trad;
     node_geometry(S, sctr, srad);
     node_geometry(T, tctr, trad);
-    std::vector<std::vector<double>> grids(bt::MLP_DMAX + 1);
-    std::vector<double> slen;
+    std::vector<hvec<double>> grids(bt::MLP_DMAX + 1);
+    hvec<double> slen;
     for (int d = bt::MLP_DMIN; d <= bt::MLP_DMAX; d++) fill_grids(S, d, grids[d], slen);
     double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx, *d_ty, *d_tz, *d_mom, *d_sctr, *d_tctr, *d_srad, *d_trad, *d_slen;
     int *d_sibeg, *d_snum, *d_tibeg, *d_tnum, *d_snch, *d_sch, *d_sleaves, *d_slvl, *d_tn, *d_sn;
