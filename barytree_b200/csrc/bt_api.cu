@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <climits>
 #include <cstring>
+#include <future>
 #include <mutex>
 #include <omp.h>
 #include <sys/resource.h>
@@ -552,9 +553,13 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
     const int nt = (int)sys.toff[sys.n], ns = (int)sys.soff[sys.n];
     long long launches = 0;
     bool same = sys.toff == sys.soff && o.maxs == o.maxt;
+    // host arrays: the comparison runs on another host thread while the
+    // source tree is built (its inputs go to the device meanwhile)
+    std::future<bool> same_fut;
     if (same && !inputs_on_device)
-        same = same_host(tx, sx, (size_t)nt) && same_host(ty, sy, (size_t)nt) && same_host(tz, sz, (size_t)nt);
-    pt.mark("setup: compare target/source arrays");
+        same_fut = std::async(std::launch::async, [=] {
+            return same_host(tx, sx, (size_t)nt) && same_host(ty, sy, (size_t)nt) && same_host(tz, sz, (size_t)nt);
+        });
     const bool check_on_device = same && inputs_on_device && !(tx == sx && ty == sy && tz == sz);
     double *d_sx, *d_sy, *d_sz, *d_sq, *d_tx = nullptr, *d_ty = nullptr, *d_tz = nullptr;
     int *d_sord, *d_tord = nullptr;
@@ -585,6 +590,10 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
                                  &launches);
     const char *which = "source";
     pt.mark("setup: source tree (GPU)");
+    if (same_fut.valid()) {
+        same = same_fut.get();
+        pt.mark("setup: compare target/source arrays");
+    }
     if (!e && !same) {
         bt::GtArrays ta{d_tx, d_ty, d_tz, nullptr, d_tord};
         which = "target";
