@@ -37,6 +37,21 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def host_threads_per_rank():
+    """torchrun starts every rank with OMP_NUM_THREADS=1.  The library plans
+    each call on the host with OpenMP (interaction lists, the degree
+    selection's list rewrite, the symmetric pairs), so each rank gets an
+    equal share of the host's cores instead.  Runs at import, before the
+    library and its OpenMP runtime are loaded; an explicit setting other
+    than 1 is kept."""
+    local = int(os.environ.get("LOCAL_WORLD_SIZE", "1") or 1)
+    if local > 1 and os.environ.get("OMP_NUM_THREADS") == "1":
+        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 1) // local))
+
+
+host_threads_per_rank()
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
