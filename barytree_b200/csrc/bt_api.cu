@@ -1262,20 +1262,34 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         hvec<int64_t> rev(ne);
         std::vector<int64_t> poff0(NU + 1, 0), poff1(NU + 1, 0), ioff(NU + 1, 0);
 #pragma omp parallel for schedule(static)
+        for (int u = 0; u < NU; u++)
+            for (int64_t j = mx_doff[u]; j < far_end[u]; j++) rev[j] = -1;
+        // the head of each pair (A < B) looks itself up in B's list and links
+        // both entries; every entry is written by one head at most
+#pragma omp parallel for schedule(static)
+        for (int u = 0; u < NU; u++) {
+            const int A = T.leaves[u];
+            for (int64_t j = mx_doff[u]; j < far_end[u]; j++) {
+                const int B = far[j], ub = unit_of[B];
+                if (B < A) continue;
+                const int *b0 = far.data() + mx_doff[ub], *b1 = far.data() + far_end[ub];
+                const int *it = std::lower_bound(b0, b1, A);
+                if (it != b1 && *it == A) {
+                    const int64_t q = it - far.data();
+                    rev[j] = q;
+                    rev[q] = j;
+                }
+            }
+        }
+#pragma omp parallel for schedule(static)
         for (int u = 0; u < NU; u++) {
             const int A = T.leaves[u];
             int64_t heads[2] = {0, 0}, all = 0;
-            for (int64_t j = mx_doff[u]; j < far_end[u]; j++) {
-                const int B = far[j], ub = unit_of[B];
-                const int *b0 = far.data() + mx_doff[ub], *b1 = far.data() + far_end[ub];
-                const int *it = std::lower_bound(b0, b1, A);
-                rev[j] = -1;
-                if (it != b1 && *it == A) {
-                    rev[j] = it - far.data();
+            for (int64_t j = mx_doff[u]; j < far_end[u]; j++)
+                if (rev[j] >= 0) {
                     all++;
-                    heads[fnear[j]] += A < B ? 1 : 0;
+                    heads[fnear[j]] += A < far[j] ? 1 : 0;
                 }
-            }
             poff0[u + 1] = heads[0];
             poff1[u + 1] = heads[1];
             ioff[u + 1] = all;
