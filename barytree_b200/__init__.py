@@ -123,7 +123,7 @@ _BTI_ARGS = (
 )
 
 # every exported symbol of include/barytree_b200.h
-EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists",
+EXPORTED_SYMBOLS = ("BaryTreeInterface", "BaryTreeInterface_ex", "bt_eval", "bt_direct", "bt_lists", "bt_lists_ex",
                     "bt_tree_dump", "bt_tree_dump_ex", "bt_eval_batch", "bt_direct_ex", "bt_session_create", "bt_session_eval", "bt_session_destroy", "bt_measure_peaks", "bt_last_error", "bt_kernel_launch_count",
                     "bt_selector_nweights", "bt_selector_set", "bt_selector_training_data", "bt_selector_train",
                     "bt_mlp_loss_grad", "bt_mlp_predict", "bt_eval_ex", "bt_direct_full", "bt_eval_noalloc",
@@ -157,6 +157,11 @@ def lib():
                            ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                            ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip, _ip, _ip, ctypes.c_long)
     L.bt_lists.restype = ctypes.c_long
+    L.bt_lists_ex.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp,
+                              ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                              ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                              _ip, _ip, _ip, ctypes.c_long)
+    L.bt_lists_ex.restype = ctypes.c_long
     L.bt_tree_dump.argtypes = (ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, ctypes.c_int)
     L.bt_tree_dump.restype = ctypes.c_int
     L.bt_eval_batch.argtypes = (ctypes.c_int, _llp, _llp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
@@ -517,20 +522,28 @@ def direct(tx, ty, tz, sx, sy, sz, sq, kernel=Kernel.COULOMB, kernel_param=0.0, 
 
 
 def interaction_lists(tx, ty, tz, sx, sy, sz, compute_type, approximation, theta, degree,
-                      max_source_leaf, max_target_leaf, size_check):
-    """(units, nodes, entries[k,3]) in the canonical (unit, kind, node) form."""
+                      max_source_leaf, max_target_leaf, size_check, tree_build=None, device=0):
+    """(units, nodes, entries[k,3]) in the canonical (unit, kind, node) form.
+    tree_build=TREE_GPU plans as the evaluation path does (trees built on the
+    GPU); the default builds the trees on the host."""
     tx, ty, tz, sx, sy, sz = map(_c, (tx, ty, tz, sx, sy, sz))
     units, nodes = ctypes.c_int(0), ctypes.c_int(0)
     cap = 1 << 16
     while True:
         ent = np.zeros(3 * cap, dtype=np.int32)
-        n = lib().bt_lists(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), int(compute_type),
-                           int(approximation), float(theta), int(degree), int(max_source_leaf),
-                           int(max_target_leaf), float(size_check), ctypes.byref(units), ctypes.byref(nodes),
-                           ent.ctypes.data_as(_ip), cap)
+        args = (len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), int(compute_type),
+                int(approximation), float(theta), int(degree), int(max_source_leaf), int(max_target_leaf),
+                float(size_check))
+        if tree_build is None:
+            n = lib().bt_lists(*args, ctypes.byref(units), ctypes.byref(nodes), ent.ctypes.data_as(_ip), cap)
+        else:
+            n = lib().bt_lists_ex(*args, int(tree_build), int(device), ctypes.byref(units), ctypes.byref(nodes),
+                                  ent.ctypes.data_as(_ip), cap)
+        if n == -2:
+            _check(BT_ERR_CUDA)
         if n >= 0:
             return units.value, nodes.value, ent[: 3 * n].reshape(-1, 3)
-        cap *= 4
+        cap = max(cap * 4, 1 << 20)
 
 
 def tree_summary(x, y, z, maxparnode, tree_build=TREE_HOST, device=0, return_order=False):

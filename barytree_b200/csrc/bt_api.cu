@@ -2325,11 +2325,45 @@ long bt_lists(int numTargets, int numSources, const double *targetX, const doubl
               int approximation, double theta, int interpOrder, int maxPerSourceLeaf, int maxPerTargetLeaf,
               double sizeCheck, int *units, int *nodes, int *entries, long cap)
 {
+    return bt_lists_ex(numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, compute_type,
+                       approximation, theta, interpOrder, maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, BT_TREE_HOST,
+                       0, units, nodes, entries, cap);
+}
+
+long bt_lists_ex(int numTargets, int numSources, const double *targetX, const double *targetY,
+                 const double *targetZ, const double *sourceX, const double *sourceY, const double *sourceZ,
+                 int compute_type, int approximation, double theta, int interpOrder, int maxPerSourceLeaf,
+                 int maxPerTargetLeaf, double sizeCheck, int tree_build, int device, int *units, int *nodes,
+                 int *entries, long cap)
+{
+    g_err[0] = 0;
+    if (tree_build != BT_TREE_GPU && tree_build != BT_TREE_HOST) {
+        set_err("invalid tree_build %d", tree_build);
+        return -2;
+    }
     bt_plan pl;
     memset(&pl, 0, sizeof pl);
     bt_params_setup(&pl.prm, COULOMB, 0, nullptr, SKIPPING, approximation, compute_type, theta, interpOrder,
                     maxPerSourceLeaf, maxPerTargetLeaf, sizeCheck, -1.0, 0);
-    build_plan(pl, numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, nullptr);
+    if (tree_build == BT_TREE_HOST) {
+        build_plan(pl, numTargets, numSources, targetX, targetY, targetZ, sourceX, sourceY, sourceZ, nullptr);
+    } else {
+        // the evaluation path's own planning: trees built on the GPU, then the lists
+        DeviceCtx *ctx = nullptr;
+        if (get_ctx(device, &ctx) != BT_OK) return -2;
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        DevParts dp;
+        int e = build_plan_gpu(ctx, ctx->tree_arena, pl, Systems(numTargets, numSources), targetX, targetY, targetZ,
+                               sourceX, sourceY, sourceZ, nullptr, false, dp);
+        if (e == BT_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            set_err("CUDA error after the tree build");
+            e = BT_ERR_CUDA;
+        }
+        if (e != BT_OK) {
+            bt_plan_free(&pl);
+            return -2;
+        }
+    }
     *units = pl.pp.rows;
     *nodes = compute_type == CLUSTER_PARTICLE ? pl.tt.n : pl.st.n;
     long cnt = 0;

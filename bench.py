@@ -166,8 +166,78 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# Configurations whose reference measurement runs the reference on the full
+# system (particle-cluster, oracle/ref_sampled.c); the others (cluster-cluster,
+# the batch of systems) time the reference on smaller independent samples.
+FULL_SYSTEM_REFERENCE = (1, 3, 5)
+
+
+def reference_full_system(cfg, threads, warmup, steps, step_seconds):
+    """The reference's own CPU code (oracle/_ref, built from its sources) on
+    the configuration's full system, the same seed-0 inputs the GPU arm's rank
+    0 evaluates.
+
+    The reference's setup (source tree, target batches, source proxies,
+    interaction lists: its own serial routines) runs once and is timed.  Each
+    step then evaluates a strided sample of the target batches with the
+    reference's InteractionCompute_PC on `threads` host threads (a different
+    offset every step); the batches of a step are sized to take about
+    `step_seconds`.  The whole-system time on `threads` cores is the setup
+    plus the full evaluation, extrapolated from the sampled batches by the
+    pointwise interaction counts (the reference's own count):
+        t = t_setup + W_total / (r_core * threads),
+    with r_core = sampled interactions / the sampled batches' summed thread
+    seconds.  Returns None if the reference build is absent."""
+    from oracle import oracle as O
+    if not O.ref_available() or not os.path.exists(os.path.join(O.REF_DIR, "libBaryTree_refsample.so")):
+        return None
+    x, y, z, q, _ = make_inputs(cfg, 0)
+    n = len(x)
+    R = O.RefSampled(x, y, z, x.copy(), y.copy(), z.copy(), q, cfg["kernel"], [cfg["kp"]], cfg["approx"],
+                     cfg["theta"], cfg["degree"], cfg["leaf"], cfg["leaf"], cfg["sc"])
+    t_setup = sum(R.setup_seconds.values())
+    nb, w_total = R.nbatches, int(R.work.sum())
+    out = np.zeros(n)
+    # warm-up steps: one batch per thread each, which also calibrates the rate
+    cpu = work = 0.0
+    for s in range(max(1, warmup)):
+        sel = np.arange(s * threads, (s + 1) * threads) * 7919 % nb
+        _, _, per = R.evaluate(sel, threads, out=out, batch_seconds=True)
+        cpu += per.sum()
+        work += R.work[sel].sum()
+    stride = max(1, int(np.ceil(w_total / ((work / cpu) * threads * step_seconds))))
+    rates, walls, nsel, ntgt, wsum, csum = [], [], 0, 0, 0, 0.0
+    for s in range(steps):
+        sel = np.arange((s * 104729 + 1) % stride, nb, stride)
+        _, wall, per = R.evaluate(sel, threads, out=out, batch_seconds=True)
+        rates.append(R.work[sel].sum() / per.sum())
+        walls.append(wall)
+        nsel += len(sel)
+        ntgt += int(R.sizes[sel].sum())
+        wsum += int(R.work[sel].sum())
+        csum += float(per.sum())
+    R.close()
+    r_core = wsum / csum
+    t_eval = w_total / (r_core * threads)
+    per_step = [n / (t_setup + w_total / (r * threads)) for r in rates]
+    return {"value": n / (t_setup + t_eval), "per_step": per_step, "n": n, "threads": threads,
+            "setup_s": t_setup, "setup_phases_s": R.setup_seconds, "eval_s_extrapolated": t_eval,
+            "whole_system_s": t_setup + t_eval, "rate_per_core": r_core, "interactions_total": w_total,
+            "batches": nb, "batches_per_step": nsel / max(1, steps), "stride": stride,
+            "sample_fraction": wsum / (w_total * max(1, steps)), "targets_sampled": ntgt,
+            "ms_per_sample_step": 1e3 * statistics.mean(walls) if walls else None,
+            "sample": (f"reference BaryTree CPU build (gcc -O3, its own routines) on the full N={n:,} system, seed 0: "
+                       f"setup (source tree, target batches, degree-{cfg['degree']} proxies, lists; serial, as in "
+                       f"the reference) timed once = {t_setup:.1f} s; per step every {stride}-th of {nb} target "
+                       f"batches evaluated by InteractionCompute_PC on {threads} host threads "
+                       f"({100 * wsum / (w_total * max(1, steps)):.2f} % of the pointwise interactions per step); "
+                       f"whole-system time on {threads} cores = setup + evaluation extrapolated by the interaction "
+                       f"count = {t_setup + t_eval:.0f} s")}
+
+
 def reference_sample_worker(args):
-    """One bounded sample of the workload through the reference CPU build."""
+    """One bounded sample of the workload through the reference CPU build:
+    smaller independent systems with the configuration's distribution."""
     cfg, seed, n = args
     from oracle import oracle as O
     c = dict(cfg)
@@ -190,8 +260,9 @@ def reference_sample_worker(args):
     return int(off[-1]), time.perf_counter() - t0, len(off) - 1
 
 
-def cpu_baseline(cfg, cores=1):
-    """The reference (oracle/_ref) on `cores` independent samples, one core each."""
+def reference_samples(cfg, cores):
+    """The reference on `cores` independent smaller systems, one core each
+    (configurations without a full-system reference measurement)."""
     from oracle import oracle as O
     if not O.ref_available():
         return None
@@ -210,29 +281,54 @@ def cpu_baseline(cfg, cores=1):
         value = sum(r[0] for r in res) / secs
         nsys = res[0][2]
         n = res[0][0]
-    return {"value": value, "unit": "targets/s", "cores": cores, "kind": "reference",
-            "sample": f"reference BaryTree CPU build (gcc -O3, serial) on {cores} independent sample(s) of "
-                      f"N={n} particles" + (f" in {nsys} systems" if cfg["dist"] == "batch" else "") +
-                      f" with this configuration's distribution and parameters; {secs:.1f} s wall"}
+    return {"value": value, "n": n, "sample": f"reference BaryTree CPU build (gcc -O3, serial) on {cores} independent "
+                                              f"system(s) of N={n} particles" +
+                                              (f" in {nsys} systems" if cfg["dist"] == "batch" else "") +
+                                              f" with this configuration's distribution and parameters (not the full "
+                                              f"configuration); {secs:.1f} s wall"}
 
 
-PROFILE_FOR_CONFIG = {5: "eval_targets_mixed_blobs2M.md"}
-
-
-def traffic_from_profiles(config_id):
-    """DRAM bytes per launch of the evaluation kernel, from the committed ncu summary."""
-    if config_id not in PROFILE_FOR_CONFIG:
+def cpu_baseline(cfg, config_id, cores):
+    """The reference on this host: the full system where the split harness
+    covers the configuration (one short sampled step), else independent
+    smaller systems."""
+    if config_id in FULL_SYSTEM_REFERENCE and "n_override" not in cfg:
+        r = reference_full_system(cfg, cores, 1, 1, 10.0)
+        if r is None:
+            return None
+        return {"value": r["value"], "unit": "targets/s", "cores": cores, "kind": "reference",
+                "sample": r["sample"], "whole_system_s": r["whole_system_s"], "setup_s": r["setup_s"]}
+    r = reference_samples(cfg, cores)
+    if r is None:
         return None
-    path = os.path.join(ROOT, "profiles", PROFILE_FOR_CONFIG[config_id])
+    return {"value": r["value"], "unit": "targets/s", "cores": cores, "kind": "reference", "sample": r["sample"]}
+
+
+# committed ncu summaries that carry a DRAM traffic figure for a configuration,
+# and what that figure is
+PROFILE_FOR_CONFIG = {5: ("eval_targets_mixed_blobs2M.md",
+                          "estimate: ncu captures of the three evaluation kernels on the 2M reduction of this "
+                          "configuration (815.5 MB), scaled x8 by the particle count to N = 16M; not a capture "
+                          "of the 16M launch")}
+
+
+def traffic_from_profiles(config_id, n_override=None):
+    """DRAM bytes per launch of the evaluation kernels from the committed ncu
+    summary, and where the figure comes from; (None, None) where no summary
+    covers the run (a reduced --n is not what the figure describes)."""
+    if config_id not in PROFILE_FOR_CONFIG or n_override:
+        return None, None
+    name, source = PROFILE_FOR_CONFIG[config_id]
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
-        return None
+        return None, None
     for line in open(path):
         if line.startswith("traffic_bytes_per_launch:"):
             try:
-                return float(line.split(":", 1)[1])
+                return float(line.split(":", 1)[1]), f"{source} (profiles/{name})"
             except ValueError:
-                return None
-    return None
+                return None, None
+    return None, None
 
 
 def max_over_ranks(ms, world, device):
@@ -262,7 +358,7 @@ def job_throughput(n_per_rank, world, ms_per_step):
     return world * n_per_rank / (ms_per_step * 1e-3)
 
 
-def roofline(sfu, tflops, fma_peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_rate, traffic):
+def roofline(sfu, tflops, fma_peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_rate, traffic, traffic_source):
     """Roofline of the particle-output evaluation (PC + PP onto targets): the
     particle-output kernel and, when the targets are the sources, the
     symmetric near-field pair kernels beside it and their gather.
@@ -275,6 +371,7 @@ def roofline(sfu, tflops, fma_peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_ra
     evals = rep["eval_flops"] / w
     r = {"kernel": "evaluation: k_eval_targets(_mixed) + k_pp_sym + k_sym_gather (PC + PP)", "ms_per_launch": ev_ms,
          "evaluations_per_launch": evals, "flops_per_launch": rep["eval_flops"], "traffic": traffic,
+         "traffic_source": traffic_source,
          "simt_tflops": tflops, "simt_peak_tflops": fma_peak,
          "simt_frac": tflops / fma_peak if tflops else None,
          "peak_source": "measured by bt_measure_peaks on this GPU (rsqrt probe; FMA = 2 FLOP)"}
@@ -297,25 +394,46 @@ def roofline(sfu, tflops, fma_peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_ra
 
 
 def run_reference_arm(args, cfg, rank, world):
+    """The reference's CPU implementation on this host's cores (rank 0 only):
+    for configurations 1, 3 and 5 on the full system (reference_full_system),
+    else on independent smaller systems (labelled as such)."""
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    vals = []
-    for _ in range(args.warmup):
-        cpu_baseline(cfg, cores)
-    for _ in range(args.steps):
-        b = cpu_baseline(cfg, cores)
-        if b is None:
+    full = args.config in FULL_SYSTEM_REFERENCE and "n_override" not in cfg
+    if full:
+        r = reference_full_system(cfg, cores, args.warmup, args.steps, args.ref_step_seconds)
+        if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
             return
-        vals.append(b["value"])
-    v = statistics.mean(vals)
+        v = statistics.mean(r["per_step"])
+        workload = cfg["workload"]
+        extra = {k: r[k] for k in ("whole_system_s", "setup_s", "setup_phases_s", "eval_s_extrapolated",
+                                   "rate_per_core", "interactions_total", "batches", "batches_per_step",
+                                   "sample_fraction", "ms_per_sample_step")}
+        sample = r["sample"]
+    else:
+        vals = []
+        for _ in range(args.warmup):
+            reference_samples(cfg, cores)
+        for _ in range(args.steps):
+            b = reference_samples(cfg, cores)
+            if b is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
+                return
+            vals.append(b["value"])
+        v = statistics.mean(vals)
+        workload = f"{cfg['workload']} [reference: {b['sample']}]"
+        extra = {}
+        sample = b["sample"]
     line = {"metric": "targets/s", "value": v, "unit": "targets/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "config_id": args.config},
-            "cpu_baseline": {"value": v, "unit": "targets/s", "cores": cores, "kind": "reference",
-                             "sample": b["sample"]},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy PCG64 with the configuration's "
+                                                         "distribution, seed 0 as the GPU arm's rank 0)",
+            "config": {"workload": workload, "config_id": args.config, "precision": "fp64",
+                       "degree_policy": "fixed", "degree": cfg["degree"], "full_system": full},
+            "cpu_baseline": dict({"value": v, "unit": "targets/s", "cores": cores, "kind": "reference",
+                                  "sample": sample}, **extra),
             "e2e": {"value": v, "unit": "targets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -333,6 +451,8 @@ def make_parser():
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--no-fp64-plain", action="store_true", help="skip the FP64 fixed-degree comparison step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-step-seconds", type=float, default=4.0,
+                    help="reference arm: host seconds of sampled evaluation per step")
     ap.add_argument("--no-graph", action="store_true", help="skip the session (graph replay) measurement")
     ap.add_argument("--dispatch", choices=["auto", "queue", "grid"], default="auto",
                     help="mixed evaluation kernels: persistent blocks on a device work queue, or one block per item")
@@ -586,7 +706,9 @@ def main():
             "e2e": {"value": e2e, "unit": "targets/s", "h2d_bytes_per_step": 4 * 8 * n,
                     "d2h_bytes_per_step": 8 * n, "ms_per_step": ms_e2e / args.steps},
             "roofline": roofline(sfu, achieved, peak, B.PRECISION_FP64 if fp64_kernels else prec, rep, ev_ms, w,
-                                 mufu_per_eval, rsqrt_rate, traffic_from_profiles(args.config)),
+                                 mufu_per_eval, rsqrt_rate,
+                                 *(traffic_from_profiles(args.config, args.n) if sfu and policy == "learned"
+                                   else (None, None))),
             "phases_ms": {k: rep[k] for k in ("ms_setup", "ms_upward", "ms_compute", "ms_downward", "ms_transfer")},
             "interactions": {k: rep[k] for k in ("pp_ptwise", "pc_ptwise", "cp_ptwise", "cc_ptwise")},
             "clocks": clock_info,
@@ -599,7 +721,7 @@ def main():
             line["speedup_vs_fp64_plain"] = {"value": value / fp64_plain["value"],
                                              "e2e": e2e / fp64_plain["value"]}
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(cfg, 1)
+            line["cpu_baseline"] = cpu_baseline(cfg, args.config, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

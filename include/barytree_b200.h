@@ -268,7 +268,12 @@ int bt_tuning_get(int device, int kernel, int approximation, bt_tuning *tuning, 
  * with a message giving both sizes (roughly up to 5e5 particles at degree 8).
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress with that device current); make that first call
- * before any stream capture.  Every call on a device shares the one array
+ * before any stream capture.  Under CUDA's default lazy module loading the
+ * array's memory is taken when the library's module is first used on a
+ * device (at the latest by that first call), not when the library is
+ * loaded: a caller that reserves all of a device's free memory for itself
+ * must make its first call of this function (or of any other library
+ * function on that device) before doing so.  Every call on a device shares the one array
  * and leaves the previous call's contents in it; all kernels write their
  * scratch before reading it, so nothing needs to start at zero.  Calls
  * through this library are serialised per device by a lock; work that the
@@ -328,6 +333,19 @@ long bt_lists(int numTargets, int numSources,
               int compute_type, int approximation, double theta, int interpOrder,
               int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck,
               int *units, int *nodes, int *entries, long cap);
+
+/* bt_lists with the tree build the lists come from: BT_TREE_HOST, or
+ * BT_TREE_GPU on `device` (the evaluation path's own planning: trees built
+ * on the GPU, then the MAC traversal).  Returns the number of triples, -1 if
+ * `cap` is too small, -2 on other errors (bt_last_error).  No counterpart
+ * in the reference beyond InteractionLists_Make itself: it lets the parity
+ * tests check the lists the evaluation path uses. */
+long bt_lists_ex(int numTargets, int numSources,
+                 const double *targetX, const double *targetY, const double *targetZ,
+                 const double *sourceX, const double *sourceY, const double *sourceZ,
+                 int compute_type, int approximation, double theta, int interpOrder,
+                 int maxPerSourceLeaf, int maxPerTargetLeaf, double sizeCheck,
+                 int tree_build, int device, int *units, int *nodes, int *entries, long cap);
 
 /* Tree summary, as bto_tree in the oracle: per node (ibeg 1-based, iend,
  * num_children, level) and (x_min,x_max,y_min,y_max,z_min,z_max,radius).

@@ -197,3 +197,70 @@ def ref_tree_order(x, y, z, maxpar):
     order = np.zeros(max(1, len(x)), dtype=np.int32)
     L.refl_tree_order(len(x), _p(x), _p(y), _p(z), int(maxpar), order.ctypes.data_as(_ip))
     return order[: len(x)]
+
+
+_refsample = None
+
+
+def refsample_lib():
+    global _refsample
+    if _refsample is None:
+        lib = ctypes.CDLL(os.path.join(REF_DIR, "libBaryTree_refsample.so"))
+        lib.refs_setup.argtypes = (ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                   ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp)
+        lib.refs_setup.restype = ctypes.c_void_p
+        lib.refs_num_batches.argtypes = (ctypes.c_void_p,)
+        lib.refs_num_batches.restype = ctypes.c_int
+        lib.refs_batch_work.argtypes = (ctypes.c_void_p, ctypes.c_int)
+        lib.refs_batch_work.restype = ctypes.c_longlong
+        lib.refs_batch_size.argtypes = (ctypes.c_void_p, ctypes.c_int)
+        lib.refs_batch_size.restype = ctypes.c_int
+        lib.refs_eval.argtypes = (ctypes.c_void_p, ctypes.c_int, _ip, ctypes.c_int, _dp, _dp)
+        lib.refs_eval.restype = ctypes.c_double
+        lib.refs_free.argtypes = (ctypes.c_void_p,)
+        lib.refs_free.restype = None
+        _refsample = lib
+    return _refsample
+
+
+class RefSampled:
+    """The reference's particle-cluster treecode (built from its own sources)
+    with setup and per-batch evaluation split (oracle/ref_sampled.c): full-size
+    systems are set up once, then any subset of the target batches is
+    evaluated with exactly the values a full call gives those targets."""
+
+    def __init__(self, tx, ty, tz, sx, sy, sz, sq, kernel, kparams, approximation, theta, degree, max_source_leaf,
+                 max_target_leaf, size_check):
+        tx, ty, tz, sx, sy, sz, sq = map(_c, (tx, ty, tz, sx, sy, sz, sq))
+        kp = _c(np.atleast_1d(kparams if kparams is not None else [0.0]))
+        self.lib = refsample_lib()
+        self.nt = len(tx)
+        phases = np.zeros(4)
+        self.h = self.lib.refs_setup(len(tx), len(sx), _p(tx), _p(ty), _p(tz), _p(sx), _p(sy), _p(sz), _p(sq),
+                                     int(kernel), len(kp), _p(kp), int(approximation), float(theta), int(degree),
+                                     int(max_source_leaf), int(max_target_leaf), float(size_check), _p(phases))
+        self.setup_seconds = dict(zip(("source_tree", "target_batches", "source_proxies", "lists"),
+                                      map(float, phases)))
+        self.nbatches = self.lib.refs_num_batches(self.h)
+        self.work = np.array([self.lib.refs_batch_work(self.h, b) for b in range(self.nbatches)], dtype=np.int64)
+        self.sizes = np.array([self.lib.refs_batch_size(self.h, b) for b in range(self.nbatches)], dtype=np.int64)
+
+    def evaluate(self, batches, threads=1, out=None, batch_seconds=False):
+        """Potentials of the given batches' targets, written into `out`
+        (caller order; NaN elsewhere if `out` is None).  Returns (out, wall
+        seconds), and with batch_seconds=True also each batch's own seconds."""
+        sel = np.ascontiguousarray(batches, dtype=np.int32)
+        if out is None:
+            out = np.full(self.nt, np.nan)
+        per = np.zeros(len(sel))
+        secs = self.lib.refs_eval(self.h, len(sel), sel.ctypes.data_as(_ip), int(threads), _p(out), _p(per))
+        return (out, secs, per) if batch_seconds else (out, secs)
+
+    def close(self):
+        if self.h:
+            self.lib.refs_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -112,3 +112,42 @@ def test_close_pairs_across_touching_leaves(kernel, kp):
     assert err_sym.max() < 1e-6 and err_off.max() < 1e-6, (err_sym.max(), err_off.max())
     assert _rel(sym, off) < 5e-7
     assert np.array_equal(B.treecode(x, y, z, x.copy(), y.copy(), z.copy(), q, **kw), sym)
+
+
+_THREADS_SCRIPT = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[2])
+import barytree_b200 as B
+rng = np.random.default_rng(43)
+c = rng.uniform(-0.6, 0.6, (4, 3))
+pts = np.clip(np.concatenate([rng.normal(c[k], 0.1, (40000, 3)) for k in range(4)] +
+                             [rng.uniform(-1, 1, (40000, 3))]), -1, 1)
+x, y, z = pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy()
+q = rng.uniform(-1, 1, len(x))
+pot, rep = B.treecode(x, y, z, x.copy(), y.copy(), z.copy(), q, theta=0.7, degree=6, max_source_leaf=500,
+                      max_target_leaf=500, precision=B.PRECISION_MIXED, return_report=True)
+np.savez(sys.argv[1], pot=pot, sym=rep["sym_ptwise"], pp=rep["pp_ptwise"])
+"""
+
+
+@pytest.mark.parametrize("threads", [[1, 16], [3, 8]])
+def test_symmetric_pass_independent_of_host_threads(tmp_path, threads):
+    """The host builds the symmetric pairs in parallel (OpenMP) and numbers
+    them per head unit and partner node, so the pair list, the slices and
+    therefore the potentials do not depend on the number of host threads:
+    the same evaluation in fresh processes with different OMP_NUM_THREADS
+    gives the same bits and the same count of symmetric evaluations."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    res = []
+    for t in threads:
+        path = str(tmp_path / f"pot_{t}.npz")
+        env = dict(os.environ, OMP_NUM_THREADS=str(t))
+        subprocess.run([sys.executable, "-c", _THREADS_SCRIPT, path, ROOT], env=env, check=True, timeout=600)
+        res.append(np.load(path))
+    assert res[0]["sym"] > 0
+    assert res[0]["sym"] == res[1]["sym"] and res[0]["pp"] == res[1]["pp"]
+    assert np.array_equal(res[0]["pot"], res[1]["pot"])

@@ -172,3 +172,21 @@ def test_no_device_status():
     rc, out = _bti()
     assert rc == B.BT_ERR_NO_DEVICE
     assert np.all(out[:100] == 0.0)
+
+
+@pytest.mark.parametrize("cid", [1, 2, 3])
+def test_lists_match_reference_benchmark_configs(cid):
+    """The interaction lists of the benchmark configurations at their full
+    sizes (100k particle-cluster; 1M cluster-cluster, theta 0.8; 4M Gaussian
+    Hermite with size check 4 and leaf 1000), from the seed-0 inputs of
+    bench.py, against the reference's own InteractionLists_Make: bit for bit."""
+    if not O.ref_available():
+        pytest.skip("reference build oracle/_ref not present")
+    import refjobs
+    cfg, x, y, z, _ = refjobs.inputs(cid)
+    args = (x, y, z, x.copy(), y.copy(), z.copy(), cfg["ctype"], cfg["approx"], cfg["theta"], cfg["degree"],
+            cfg["leaf"], cfg["leaf"], cfg["sc"])
+    a = B.interaction_lists(*args)
+    b = O.ref_lists(*args)
+    assert a[0] == b[0] and a[1] == b[1]
+    assert a[2].shape == b[2].shape and np.array_equal(a[2], b[2])
