@@ -567,3 +567,45 @@ def tree_summary(x, y, z, maxparnode, tree_build=TREE_HOST, device=0, return_ord
 
 def kernel_launch_count() -> int:
     return int(lib().bt_kernel_launch_count())
+
+
+# Leaf size of the reference's GPU build on its beta path: with OpenACC on,
+# RunParams_Setup sets 3000 particles per source and target leaf
+# (src/run_params/run_params.c:101-103); its CPU build uses 50/5 and 5/50.
+BETA_GPU_LEAF = 3000
+
+
+class _RunParams(ctypes.Structure):
+    """struct RunParams of include/barytree_compat.h (the reference's
+    src/run_params/struct_run_params.h:7-31)."""
+    _fields_ = [("kernel", ctypes.c_int), ("num_kernel_params", ctypes.c_int), ("kernel_params", _dp),
+                ("approximation", ctypes.c_int), ("singularity", ctypes.c_int), ("compute_type", ctypes.c_int),
+                ("theta", ctypes.c_double), ("size_check_factor", ctypes.c_double),
+                ("interp_degree", ctypes.c_int), ("interp_pts_per_cluster", ctypes.c_int),
+                ("interp_charges_per_cluster", ctypes.c_int), ("interp_weights_per_cluster", ctypes.c_int),
+                ("max_per_source_leaf", ctypes.c_int), ("max_per_target_leaf", ctypes.c_int),
+                ("beta", ctypes.c_double), ("verbosity", ctypes.c_int)]
+
+
+def beta_parameters(beta, compute_type=ComputeType.PARTICLE_CLUSTER, approximation=Approximation.LAGRANGE):
+    """theta, degree and size check that the reference's accuracy knob beta
+    in [0, 1] stands for (run_params.c:51-95), from the library's
+    RunParams_Setup; the leaf sizes returned are the reference GPU build's
+    (BETA_GPU_LEAF).  Larger beta: smaller theta, higher degree."""
+    L = lib()
+    rp = ctypes.POINTER(_RunParams)
+    L.RunParams_Setup.argtypes = (ctypes.POINTER(rp), ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int)
+    L.RunParams_Setup.restype = None
+    L.RunParams_Free.argtypes = (ctypes.POINTER(rp),)
+    L.RunParams_Free.restype = None
+    p = rp()
+    kp = np.zeros(1)
+    L.RunParams_Setup(ctypes.byref(p), int(Kernel.COULOMB), 1, _p(kp), int(approximation), int(Singularity.SKIPPING),
+                      int(compute_type), 0.0, 0, 1, 1, 0.0, float(beta), 0)
+    s = p.contents
+    out = {"beta": float(beta), "theta": s.theta, "degree": s.interp_degree, "size_check": s.size_check_factor,
+           "max_source_leaf": BETA_GPU_LEAF, "max_target_leaf": BETA_GPU_LEAF}
+    L.RunParams_Free(ctypes.byref(p))
+    return out

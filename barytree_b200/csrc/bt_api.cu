@@ -32,6 +32,7 @@
 #include "bt_mixed.h"
 #include "bt_learned.h"
 #include "bt_gputree.h"
+#include "bt_gpulists.h"
 #include "bt_ss.h"
 #include "bt_tc.h"
 #include "bt_sym.h"
@@ -617,8 +618,30 @@ int build_plan_gpu(DeviceCtx *ctx, Arena &tarena, bt_plan &pl, const Systems &sy
         dp.tx = d_tx; dp.ty = d_ty; dp.tz = d_tz; dp.order = d_tord;
     }
     pt.mark("setup: target tree");
-    bt_plan_lists(&pl);
-    pt.mark("setup: interaction lists (host)");
+    // particle-cluster and cluster-particle lists: traversed on the GPU in the
+    // tree build's work memory (free again now); cluster-cluster's dual
+    // traversal, and a traversal that does not fit, run on the host
+    int lrc = -1;
+    if ((o.ctype == PARTICLE_CLUSTER || o.ctype == CLUSTER_PARTICLE) && !getenv("BARYTREE_B200_HOST_LISTS")) {
+        const bt_tree *trav = o.ctype == PARTICLE_CLUSTER ? &pl.st : &pl.tt;
+        const bt_tree *bat = o.ctype == PARTICLE_CLUSTER ? &pl.tt : &pl.st;
+        long long gl = 0;
+        lrc = bt::gpu_pc_lists(trav, bat, &o, d_work, wbytes, &pl.ap, &pl.pp, st, &gl);
+        g_launches += gl;
+        if (lrc > 0) {
+            set_err("CUDA error %s in the interaction-list traversal", cudaGetErrorString((cudaError_t)lrc));
+            return BT_ERR_CUDA;
+        }
+    }
+    if (lrc == 0) {
+        bt_csr_empty(&pl.pc, pl.ap.rows);
+        bt_csr_empty(&pl.cp, pl.ap.rows);
+        bt_plan_work_lists(&pl);
+        pt.mark("setup: interaction lists (GPU traversal)");
+    } else {
+        bt_plan_lists(&pl);
+        pt.mark("setup: interaction lists (host)");
+    }
     return BT_OK;
 }
 
@@ -974,8 +997,13 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
                 }
             }
         }
-        bt::launch_l2p(n, herm, v.n_l2p_items, d_l2pitems, d_tleaves, d_tpar, d_tibeg, d_tnum, d_tgrid,
-                       d_tlen, d_ww, d_Phi, d_tx, d_ty, d_tz, d_pot, st);
+        if (v.tc_up && !herm && !v.ss && bt::p2m_tc_supported(n))
+            // mixed Lagrange: the leaf interpolation as a GEMM on the tensor cores
+            bt::launch_l2p_tc(n, v.n_l2p_items, d_l2pitems, d_tleaves, d_tibeg, d_tnum, d_tgrid, d_Phi, d_tx, d_ty,
+                              d_tz, d_pot, v.d_err, st);
+        else
+            bt::launch_l2p(n, herm, v.n_l2p_items, d_l2pitems, d_tleaves, d_tpar, d_tibeg, d_tnum, d_tgrid,
+                           d_tlen, d_ww, d_Phi, d_tx, d_ty, d_tz, d_pot, st);
         launches++;
         if (v.ss) {
             // the weight field, interpolated and multiplied by -tq per target
@@ -1165,7 +1193,8 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         }
     }
     std::vector<int2> ev_items =
-        make_items(T.nleaves, leaf_count.data(), mixed ? bt::mixed_targets_chunk() : ssm ? bt::ss_chunk() : 128, leaf_cost);
+        make_items(T.nleaves, leaf_count.data(),
+                   mixed ? bt::mixed_targets_chunk() : ssm ? bt::ss_chunk() : bt::fp64_targets_chunk(), leaf_cost);
     std::vector<int2> grid_items, l2p_items;
     if (need_tgt_grids) {
         std::vector<int> pcount(T.n, P);
@@ -1693,6 +1722,15 @@ std::vector<float> g_selector;      // installed MLP weights (bt_selector_set), 
 std::mutex g_selector_mu;
 constexpr double SELECT_MARGIN_DECADES = 0.5;   // predicted error must sit this far below the budget
 
+// The constant c of the per-batch budget selection (bt::launch_select_budget);
+// 0 selects the per-interaction rule (predicted error SELECT_MARGIN_DECADES
+// below the tolerance).  BARYTREE_B200_SELECT_SHARE overrides it (calibration).
+double select_share_constant()
+{
+    const char *e = getenv("BARYTREE_B200_SELECT_SHARE");
+    return e ? atof(e) : 0.0;
+}
+
 void node_geometry(const bt_tree &t, std::vector<double> &ctr, std::vector<double> &rad)
 {
     ctr.resize(3 * (size_t)t.n);
@@ -1720,6 +1758,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
     const bt_tree &S = pl.st, &T = pl.tt;
     PhaseTimer pt;
     const int64_t ne = pl.t_approx.off[pl.t_approx.rows];
+    const double share_c = select_share_constant();
     std::vector<unsigned char> choice(ne > 0 ? ne : 1);
     cudaStream_t st = ctx->stream;
     int rc = BT_OK;
@@ -1743,6 +1782,14 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
         L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size());
         L.add(&d_pred, (size_t)ne * bt::MLP_OUT); L.add(&d_choice, ne);
+        // per-batch budget: the near-field lists and one share per batch
+        const int64_t nd = pl.t_direct.off[pl.t_direct.rows];
+        int64_t *d_doff = nullptr;
+        int *d_didx = nullptr;
+        float *d_share = nullptr;
+        if (share_c > 0) {
+            L.add(&d_doff, pl.t_direct.rows + 1); L.add(&d_didx, nd > 0 ? nd : 1); L.add(&d_share, pl.t_approx.rows);
+        }
         if (!arena.reserve(L.total())) {
             set_err(arena.fixed ? "degree selection needs more scratch than the static array holds"
                                 : "device allocation failed");
@@ -1760,6 +1807,7 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             UP(d_idx, pl.t_approx.idx, ne); UP(d_unit, T.leaves, T.nleaves);
             UP(d_off, pl.t_approx.off, pl.t_approx.rows + 1); UP(d_w, w.data(), w.size());
 #undef UP
+#define UP2(dst, src, cnt) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
             bt::MomentTree mt{S.n, S.nleaves, S.max_depth, d_sleaves, d_sibeg, d_snum, d_snch, d_sch, d_slvl, S.lvl_off};
             long long launches = bt::launch_node_moments(mt, d_sq, d_mom, st);
             bt::FeatureArgs fa;
@@ -1770,9 +1818,17 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             launches++;
             bt::mlp_infer(d_w, ne, d_feat, d_pred, st);
             launches++;
-            bt::launch_select(ne, d_pred, d_feat, (float)(log10(tol) - SELECT_MARGIN_DECADES), d_choice, st);
-            launches++;
+            if (share_c > 0) {
+                UP2(d_doff, pl.t_direct.off, pl.t_direct.rows + 1);
+                if (nd > 0) UP2(d_didx, pl.t_direct.idx, nd);
+                bt::launch_select_budget(fa, d_doff, d_didx, share_c * tol, ne, d_pred, d_feat, d_share, d_choice, st);
+                launches += 2;
+            } else {
+                bt::launch_select(ne, d_pred, d_feat, (float)(log10(tol) - SELECT_MARGIN_DECADES), d_choice, st);
+                launches++;
+            }
             CK(cudaGetLastError());
+#undef UP2
             CK(cudaMemcpyAsync(choice.data(), d_choice, ne, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             g_launches += launches;
@@ -2487,6 +2543,7 @@ long bt_selector_training_data(int n, const double *x, const double *y, const do
             }
         }
         {
+#define UP2(dst, src, cnt) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
             bt::MomentTree mt{S.n, S.nleaves, S.max_depth, d_sleaves, d_sibeg, d_snum, d_snch, d_sch, d_slvl, S.lvl_off};
             launches += bt::launch_node_moments(mt, d_sq, d_mom, st);
         }

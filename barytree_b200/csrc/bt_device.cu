@@ -525,10 +525,14 @@ void launch_p2m_hermite(int n, int nchunks, const HermChunk *chunks, int nred, c
 
 // ---------------------------------------------------------------------------
 // Particle-output evaluation: PC (clusters) + PP (particles) per target leaf.
-// One CTA per work item (target leaf, chunk of EV_THREADS targets), one thread
-// per target, FP64 accumulation in a register; exactly one writer per target.
+// One CTA per work item (target leaf, chunk of EV_TB * EV_THREADS targets),
+// EV_TB targets per thread (ti and ti + EV_THREADS, ...) so that every grid
+// point or source read from shared memory serves EV_TB evaluations; FP64
+// accumulation in registers in each target's own order (the same order as
+// one target per thread); exactly one writer per target.
 // ---------------------------------------------------------------------------
 constexpr int EV_THREADS = 128;
+constexpr int EV_TB = 2;
 constexpr int PP_TILE = 512;
 
 template <int KT, bool HERM>
@@ -548,11 +552,18 @@ k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ le
     const int u = it.x;
     const int tnode = leaf_node[u];
     const int tb = t_ibeg[tnode], tn = t_numpar[tnode];
-    const int ti = it.y * EV_THREADS + threadIdx.x;
-    const bool active = ti < tn;
-    const int t = tb + (active ? ti : 0);
-    const double x = tx[t], y = ty[t], z = tz[t];
-    double acc = 0.0;
+    bool active[EV_TB];
+    int t[EV_TB];
+    double x[EV_TB], y[EV_TB], z[EV_TB], acc[EV_TB];
+#pragma unroll
+    for (int b = 0; b < EV_TB; b++) {
+        const int ti = it.y * (EV_TB * EV_THREADS) + b * EV_THREADS + threadIdx.x;
+        active[b] = ti < tn;
+        t[b] = tb + (active[b] ? ti : 0);
+        x[b] = tx[t[b]]; y[b] = ty[t[b]]; z[b] = tz[t[b]];
+        acc[b] = 0.0;
+    }
+    const bool any = active[0];     // target b > 0 is active only if target 0 is
     const int np1 = n + 1, P = np1 * np1 * np1;
 
     // far field: source clusters
@@ -565,24 +576,38 @@ k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ le
         for (int i = threadIdx.x; i < 3 * np1; i += blockDim.x) g[i] = s_grid[(size_t)s * 3 * np1 + i];
         for (int i = threadIdx.x; i < nq; i += blockDim.x) q[i] = Qs[i];
         __syncthreads();
-        if (active) {
+        if (any) {
             int j = 0;
             for (int k3 = 0; k3 < np1; k3++) {
-                double dz = z - g[2 * np1 + k3];
+                const double gz = g[2 * np1 + k3];
                 for (int k2 = 0; k2 < np1; k2++) {
-                    double dy = y - g[np1 + k2];
+                    const double gy = g[np1 + k2];
                     if (!HERM && KT <= K_REGCOULOMB) {
-                        double dyz = dy * dy + dz * dz;
+                        double dyz[EV_TB];
+#pragma unroll
+                        for (int b = 0; b < EV_TB; b++) {
+                            const double dz = z[b] - gz, dy = y[b] - gy;
+                            dyz[b] = dy * dy + dz * dz;
+                        }
                         for (int k1 = 0; k1 < np1; k1++, j++) {
-                            double dx = x - g[k1];
-                            acc += k_far<KT>(fma(dx, dx, dyz), q[j], kp);
+                            const double gx = g[k1], qj = q[j];
+#pragma unroll
+                            for (int b = 0; b < EV_TB; b++) {
+                                const double dx = x[b] - gx;
+                                acc[b] += k_far<KT>(fma(dx, dx, dyz[b]), qj, kp);
+                            }
                         }
                     } else if (!HERM) {
-                        for (int k1 = 0; k1 < np1; k1++, j++) acc += k_any<KT, false>(x - g[k1], dy, dz, q[j], kp, kp2);
+                        for (int k1 = 0; k1 < np1; k1++, j++) {
+#pragma unroll
+                            for (int b = 0; b < EV_TB; b++)
+                                acc[b] += k_any<KT, false>(x[b] - g[k1], y[b] - gy, z[b] - gz, q[j], kp, kp2);
+                        }
                     } else {
                         for (int k1 = 0; k1 < np1; k1++, j++) {
-                            double dx = x - g[k1];
-                            acc += k_pc_herm<KT>(dx, dy, dz, q + j, P, kp);
+#pragma unroll
+                            for (int b = 0; b < EV_TB; b++)
+                                acc[b] += k_pc_herm<KT>(x[b] - g[k1], y[b] - gy, z[b] - gz, q + j, P, kp);
                         }
                     }
                 }
@@ -600,18 +625,23 @@ k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ le
             for (int i = threadIdx.x; i < cm; i += blockDim.x)
                 tile[i] = make_double4(sx[sb + c0 + i], sy[sb + c0 + i], sz[sb + c0 + i], sq[sb + c0 + i]);
             __syncthreads();
-            if (active) {
+            if (any) {
                 for (int i = 0; i < cm; i++) {
-                    double4 p = tile[i];
-                    double dx = x - p.x, dy = y - p.y, dz = z - p.z;
-                    acc += k_any<KT, true>(dx, dy, dz, p.w, kp, kp2);
+                    const double4 p = tile[i];
+#pragma unroll
+                    for (int b = 0; b < EV_TB; b++)
+                        acc[b] += k_any<KT, true>(x[b] - p.x, y[b] - p.y, z[b] - p.z, p.w, kp, kp2);
                 }
             }
             __syncthreads();
         }
     }
-    if (active) pot[t] = acc;
+#pragma unroll
+    for (int b = 0; b < EV_TB; b++)
+        if (active[b]) pot[t[b]] = acc[b];
 }
+
+int fp64_targets_chunk() { return EV_TB * EV_THREADS; }
 
 // ---------------------------------------------------------------------------
 // Grid-output evaluation: M2L (source clusters, CC) + CP (source particles)

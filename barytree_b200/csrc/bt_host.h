@@ -97,7 +97,9 @@ void bt_tree_set_roots(bt_tree *t, int nsys);
 
 /* bt_lists.c */
 void bt_csr_free(bt_csr *c);
+void bt_csr_empty(bt_csr *c, int rows);   /* rows empty rows */
 void bt_plan_lists(bt_plan *pl);        /* reference-shaped lists and device work lists */
+void bt_plan_work_lists(bt_plan *pl);   /* device work lists from pl->ap, pp, pc, cp       */
 void bt_plan_free(bt_plan *pl);
 
 /* Chebyshev-2 node placement for one node, in FP64 with the host libm,

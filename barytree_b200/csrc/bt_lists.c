@@ -106,6 +106,11 @@ static void empty_csr(bt_csr *c, int rows)
     csr_from_vecs(c, vecs(rows), rows);
 }
 
+void bt_csr_empty(bt_csr *c, int rows)
+{
+    empty_csr(c, rows);
+}
+
 /* Invert a CSR (rows = units, idx = columns in [0, ncols)) to rows = columns,
  * keeping row order, and optionally mapping each column through colmap. */
 static void csr_invert(const bt_csr *a, int ncols, const int *colmap, int nrows_out, bt_csr *out)
@@ -166,7 +171,14 @@ void bt_plan_lists(bt_plan *pl)
         csr_from_vecs(&pl->cp, L.cp, nt);
     }
 
-    /* device work lists */
+    bt_plan_work_lists(pl);
+}
+
+/* Device-shaped work lists from the reference-shaped lists (pl->ap, pp, pc,
+ * cp), whichever traversal made them. */
+void bt_plan_work_lists(bt_plan *pl)
+{
+    const bt_params *o = &pl->prm;
     const bt_tree *T = &pl->tt;
     pl->n_units_t = T->nleaves;
     int *leaf_of = malloc(sizeof(int) * (size_t)(T->n > 0 ? T->n : 1));

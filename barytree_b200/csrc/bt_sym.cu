@@ -47,6 +47,7 @@ namespace {
 
 constexpr int SY_THREADS = 128;
 constexpr int SY_TPT = 4;                      // targets of A per thread: two packed pairs
+constexpr int SY_NP = SY_TPT / 2;
 constexpr int SY_CHUNK = SY_TPT * SY_THREADS;  // targets of A per pass
 constexpr int SY_TILE = 512;                   // sources of B per shared-memory tile
 constexpr int SY_SB = 16;                      // sources per warp reduction
@@ -192,11 +193,11 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
     }
     for (int j = threadIdx.x; j < nb; j += SY_THREADS) accB[j] = 0.0f;
     for (int c0 = 0; c0 < na; c0 += SY_CHUNK) {
-        // targets c0 + threadIdx.x + k * SY_THREADS, k = 0..3, packed as (0, 1), (2, 3)
-        f2_t X[2], Y[2], Z[2], QT[2], S[2];
+        // targets c0 + threadIdx.x + k * SY_THREADS, k = 0..SY_TPT-1, packed as (0, 1), (2, 3), ...
+        f2_t X[SY_NP], Y[SY_NP], Z[SY_NP], QT[SY_NP], S[SY_NP];
         bool act[SY_TPT];
 #pragma unroll
-        for (int p = 0; p < 2; p++) {
+        for (int p = 0; p < SY_NP; p++) {
             const int t0 = c0 + threadIdx.x + (2 * p) * SY_THREADS, t1 = t0 + SY_THREADS;
             act[2 * p] = t0 < na;
             act[2 * p + 1] = t1 < na;
@@ -226,9 +227,9 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
                 for (int s = 0; s < SY_SB; s++) {
                     const ulonglong2 xy = *reinterpret_cast<const ulonglong2 *>(&tile[sb + s][0]);
                     const ulonglong2 zq = *reinterpret_cast<const ulonglong2 *>(&tile[sb + s][2]);
-                    f2_t rinv[2];
+                    f2_t cb = f2_make(0.0f, 0.0f);
 #pragma unroll
-                    for (int p = 0; p < 2; p++) {
+                    for (int p = 0; p < SY_NP; p++) {
                         const f2_t dx = f2_sub(X[p], xy.x), dy = f2_sub(Y[p], xy.y), dz = f2_sub(Z[p], zq.x);
                         f2_t r2 = f2_fma(dx, dx, f2_fma(dy, dy, f2_mul(dz, dz)));
                         if (CLAMP) {
@@ -236,12 +237,13 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
                             f2_split(r2, ra, rb);
                             r2 = f2_make(fmaxf(ra, thr2), fmaxf(rb, thr2));
                         }
-                        rinv[p] = sym_kval<KT>(r2, kc2);      // serves both sides
-                        S[p] = f2_fma(zq.y, rinv[p], S[p]);
+                        const f2_t rinv = sym_kval<KT>(r2, kc2);      // serves both sides
+                        S[p] = f2_fma(zq.y, rinv, S[p]);
+                        // B side: the targets' charges over r, folded into one pair
+                        cb = p == 0 ? f2_mul(QT[0], rinv) : f2_fma(QT[p], rinv, cb);
                     }
-                    // B side: the four targets' charges over r, folded into one value
                     float c0v, c1v;
-                    f2_split(f2_fma(QT[0], rinv[0], f2_mul(QT[1], rinv[1])), c0v, c1v);
+                    f2_split(cb, c0v, c1v);
                     v[s] = c0v + c1v;
                 }
                 // reduce-scatter over the warp: lanes 2i and 2i+1 end with source i
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
             }
             // the tile's A-side sums into FP64 (FP32 chains of at most one tile)
 #pragma unroll
-            for (int p = 0; p < 2; p++) {
+            for (int p = 0; p < SY_NP; p++) {
                 float lo, hi;
                 f2_split(S[p], lo, hi);
                 accA[2 * p][threadIdx.x] += (double)lo;

@@ -30,6 +30,7 @@
 // its tensor memory and returns without writing.
 #include <cuda_runtime.h>
 
+#include <cfloat>
 #include <cstdint>
 #include <cstdlib>
 
@@ -50,15 +51,17 @@ constexpr uint32_t TC_TMEM_COLS = 32;      // accumulators: hi*hi in columns 0-1
 constexpr long long TC_WAIT_LIMIT = 1LL << 22;
 constexpr long long TC_TEST_WAIT_LIMIT = 1LL << 10;   // the failure-path test's wait
 
-// Shared-memory layout (bytes).  A tile: 128 rows x 32 tf32; B tile: 16 x 32.
+// Shared-memory layout (bytes).  A tile: 128 rows x 32 tf32; B tile: 16 x 32;
+// bases: float [axis][k][particle], rows padded to LSTR floats (16-byte rows
+// whose bank groups differ for consecutive k).
+constexpr int LSTR = 36;
 constexpr uint32_t A_BYTES = TC_M * TC_KC * 4;                  // 16 KB
 constexpr uint32_t B_BYTES = TC_N * TC_KC * 4;                  // 2 KB
 constexpr uint32_t OFF_A = 0;                                   // [hi, lo]
 constexpr uint32_t OFF_B = OFF_A + 2 * A_BYTES;                 // [hi, lo]
-constexpr uint32_t OFF_L = OFF_B + 2 * B_BYTES;                 // float [3][TC_KC][TC_MAXNP1]
-constexpr uint32_t OFF_Q = OFF_L + 3 * TC_KC * TC_MAXNP1 * 4;   // float [TC_KC]
-constexpr uint32_t OFF_NODES = OFF_Q + TC_KC * 4;               // double [3][TC_MAXNP1]
-constexpr uint32_t OFF_BAR = (OFF_NODES + 3 * TC_MAXNP1 * 8 + 15) / 16 * 16;   // uint64
+constexpr uint32_t OFF_L = OFF_B + 2 * B_BYTES;                 // float [3][TC_MAXNP1][LSTR]
+constexpr uint32_t OFF_NODES = OFF_L + 3 * TC_MAXNP1 * LSTR * 4;  // float [3][TC_MAXNP1], relative to the centre
+constexpr uint32_t OFF_BAR = (OFF_NODES + 3 * TC_MAXNP1 * 4 + 15) / 16 * 16;   // uint64
 constexpr uint32_t OFF_MISC = OFF_BAR + 16;                     // tmem address, status
 constexpr uint32_t TC_SMEM = OFF_MISC + 16;
 
@@ -70,19 +73,15 @@ __device__ __forceinline__ uint32_t kmajor_off(int rows, int row, int k)
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ uint32_t tf32_rna(float x)
-{
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
+constexpr uint32_t TF32_MASK = 0xFFFFE000u;     // sign, exponent and the 10 stored mantissa bits of a TF32
 
-// a*b = hi + lo in two TF32 values: hi the product rounded to TF32, lo the
-// rest (exact in FP32 by the fused multiply-add) rounded to TF32
-__device__ __forceinline__ void split_tf32(float a, float b, uint32_t &hi, uint32_t &lo)
+// p = hi + lo with hi = p truncated to TF32 and lo the exact FP32 rest, also
+// truncated to TF32: both are valid TF32 bit patterns, and hi + lo carries p
+// to about 2^-21 relative (the 3xTF32 products hi*hi + hi*lo + lo*hi)
+__device__ __forceinline__ void split_tf32(float p, uint32_t &hi, uint32_t &lo)
 {
-    hi = tf32_rna(a * b);
-    lo = tf32_rna(fmaf(a, b, -__uint_as_float(hi)));
+    hi = __float_as_uint(p) & TF32_MASK;
+    lo = __float_as_uint(p - __uint_as_float(hi)) & TF32_MASK;
 }
 
 // Shared-memory matrix descriptor: no swizzle, K-major; LBO = distance of the
@@ -146,13 +145,12 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
 {
     constexpr int n = NP1 - 1, ROWS = NP1 * NP1, P = ROWS * NP1;
     extern __shared__ __align__(1024) unsigned char sm[];
-    float *Lb = reinterpret_cast<float *>(sm + OFF_L);          // [axis][particle][k]
-    float *qs = reinterpret_cast<float *>(sm + OFF_Q);
-    double *nodes = reinterpret_cast<double *>(sm + OFF_NODES);
+    float *Lb = reinterpret_cast<float *>(sm + OFF_L);          // [axis][k][particle], rows of LSTR
+    float *nodes = reinterpret_cast<float *>(sm + OFF_NODES);   // [axis][k], relative to the grid's centre
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
     uint32_t *misc = reinterpret_cast<uint32_t *>(sm + OFF_MISC);  // [0] tmem address, [1] status
     unsigned char *Ah = sm + OFF_A, *Al = Ah + A_BYTES, *Bh = sm + OFF_B, *Bl = Bh + B_BYTES;
-    const int t = threadIdx.x, warp = t >> 5;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int node = leaves[blockIdx.x];
 
     if (warp == 0) {
@@ -165,8 +163,15 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         misc[1] = 1;
     }
-    for (int i = t; i < 3 * NP1; i += TC_THREADS) nodes[i] = grid[(size_t)node * 3 * NP1 + i];
-    // padding rows of the operand tiles stay zero
+    // each axis's grid relative to its centre, in FP32: the bases are
+    // evaluated at FP32 relative coordinates (FP64 difference, rounded once)
+    const double *g = grid + (size_t)node * 3 * NP1;
+    const double cx = 0.5 * (g[0] + g[n]), cy = 0.5 * (g[NP1] + g[NP1 + n]), cz = 0.5 * (g[2 * NP1] + g[2 * NP1 + n]);
+    if (t < 3 * NP1) {
+        const int ax = t / NP1;
+        nodes[t] = (float)(g[t] - (ax == 0 ? cx : ax == 1 ? cy : cz));
+    }
+    // operand tiles start zero: padding rows and columns are never written
     for (uint32_t o = t * 16; o < OFF_L; o += TC_THREADS * 16) *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -181,7 +186,6 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
     for (int k = 0; k < NP1; k++) acc[k] = 0.0;
     bool ok = true;
     const uint32_t bar_a = smem_addr(bar);
-    uint32_t wpar = 0;                         // parity of the last wait (repeated once if it expired)
     if (expire_test) {
         // failure-path test: wait, before any MMA is issued, on a phase that
         // nothing completes; the bounded wait expires and the kernel takes
@@ -190,36 +194,107 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
         __syncthreads();
         ok = misc[1] != 0;
     }
-    // chunk c: products hi*hi into accumulator columns 0-15 and the two
-    // cross products into columns 16-31, from zero (short FP32 sums on the
-    // tensor core); once its MMAs have completed the threads fold the chunk
-    // into FP64 registers.  The bases of chunk c+1 are evaluated while the
-    // tensor core works on chunk c.
-    for (int c = 0; c <= nch && ok; c++) {
-        if (c < nch) {
-            const int cm = min(TC_KC, m - c * TC_KC);
-            if (t < 3 * TC_KC) {
-                const int i = t / 3, ax = t % 3;
-                double L[NP1];
-                if (i < cm) {
-                    const double *src = ax == 0 ? sx : ax == 1 ? sy : sz;
-                    lagrange_basis(n, nodes + ax * NP1, src[b0 + c * TC_KC + i], L);
-                    if (ax == 0) qs[i] = (float)sq[b0 + c * TC_KC + i];
-                } else {
+
+    // Bases of one chunk: warp a < 3 evaluates axis a for the chunk's 32
+    // particles (lane = particle), barycentric form in FP32 with the
+    // exact-node rule on the FP32 relative coordinate; the x bases carry the
+    // charge.  Particles past the leaf's end get zero bases.
+    auto bases = [&](int c) {
+        if (warp >= 3) return;
+        const int i = c * TC_KC + lane;
+        float L[NP1];
+        if (i < m) {
+            const double *src = warp == 0 ? sx : warp == 1 ? sy : sz;
+            const float xr = (float)(src[b0 + i] - (warp == 0 ? cx : warp == 1 ? cy : cz));
+            const float *nd = nodes + warp * NP1;
+            float sum = 0.0f;
+            int ex = -1;
 #pragma unroll
-                    for (int k = 0; k < NP1; k++) L[k] = 0.0;
-                    if (ax == 0) qs[i] = 0.0f;
-                }
+            for (int k = 0; k < NP1; k++) {
+                const float d = xr - nd[k];
+                if (fabsf(d) < FLT_MIN) ex = k;
+                const float w = ((k & 1) ? -1.0f : 1.0f) * ((k == 0 || k == n) ? 0.5f : 1.0f);
+                L[k] = w * __frcp_rn(d);
+                sum += L[k];
+            }
+            float scale = __frcp_rn(sum);
+            if (warp == 0) scale *= (float)sq[b0 + i];
+            if (ex >= 0) {
+                const float qv = warp == 0 ? (float)sq[b0 + i] : 1.0f;
 #pragma unroll
-                for (int k = 0; k < NP1; k++) Lb[(ax * TC_KC + i) * TC_MAXNP1 + k] = (float)L[k];
+                for (int k = 0; k < NP1; k++) L[k] = k == ex ? qv : 0.0f;
+            } else {
+#pragma unroll
+                for (int k = 0; k < NP1; k++) L[k] *= scale;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < NP1; k++) L[k] = 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < NP1; k++) Lb[(warp * TC_MAXNP1 + k) * LSTR + lane] = L[k];
+    };
+
+    // chunk c: hi*hi into accumulator columns 0-15 and the two cross
+    // products into columns 16-31, from zero (short FP32 sums on the tensor
+    // core), folded into FP64 registers once its MMAs have completed.  The
+    // next chunk's bases are evaluated while the tensor core works.
+    if (ok) bases(0);
+    __syncthreads();
+    for (int c = 0; c < nch && ok; c++) {
+        // A rows (k2, k3): Ly[k2] * Lz[k3] for the chunk's particles
+        if (t < ROWS) {
+            const float *ly = Lb + (1 * TC_MAXNP1 + k2) * LSTR, *lz = Lb + (2 * TC_MAXNP1 + k3) * LSTR;
+#pragma unroll
+            for (int k4 = 0; k4 < TC_KC; k4 += 4) {
+                const float4 a = *reinterpret_cast<const float4 *>(ly + k4);
+                const float4 b = *reinterpret_cast<const float4 *>(lz + k4);
+                uint4 h, l;
+                split_tf32(a.x * b.x, h.x, l.x);
+                split_tf32(a.y * b.y, h.y, l.y);
+                split_tf32(a.z * b.z, h.z, l.z);
+                split_tf32(a.w * b.w, h.w, l.w);
+                const uint32_t o = kmajor_off(TC_M, t, k4);
+                *reinterpret_cast<uint4 *>(Ah + o) = h;
+                *reinterpret_cast<uint4 *>(Al + o) = l;
             }
         }
-        if (c >= 1) {
-            // chunk c-1: wait for its MMAs, then fold its accumulators
-            wpar = (uint32_t)((c - 1) & 1);
-            if (t == 0) misc[1] = bar_wait(bar_a, wpar) ? 1u : 0u;
-            __syncthreads();
-            if (misc[1] == 0) { ok = false; break; }
+        {
+            // B rows k1: q * Lx[k1]; thread t covers row t / 8, particles 4 (t % 8) .. +3
+            const int k1 = t >> 3, k4 = (t & 7) * 4;
+            if (k1 < NP1) {
+                const float4 a = *reinterpret_cast<const float4 *>(Lb + k1 * LSTR + k4);
+                uint4 h, l;
+                split_tf32(a.x, h.x, l.x);
+                split_tf32(a.y, h.y, l.y);
+                split_tf32(a.z, h.z, l.z);
+                split_tf32(a.w, h.w, l.w);
+                const uint32_t o = kmajor_off(TC_N, k1, k4);
+                *reinterpret_cast<uint4 *>(Bh + o) = h;
+                *reinterpret_cast<uint4 *>(Bl + o) = l;
+            }
+        }
+        // make the operands visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t ah = smem_addr(Ah), al = smem_addr(Al), bh = smem_addr(Bh), bl = smem_addr(Bl);
+#pragma unroll
+            for (int s = 0; s < TC_KSTEPS; s++) {
+                const uint32_t oa = s * TC_M * 32, ob = s * TC_N * 32;
+                mma_tf32(tmem, smem_desc(ah + oa), smem_desc(bh + ob), s > 0 ? 1u : 0u);
+                mma_tf32(tmem + 16, smem_desc(ah + oa), smem_desc(bl + ob), s > 0 ? 1u : 0u);
+                mma_tf32(tmem + 16, smem_desc(al + oa), smem_desc(bh + ob), 1u);
+            }
+            mma_commit(bar_a);
+        }
+        // the next chunk's bases (the operands of this chunk are formed)
+        if (c + 1 < nch) bases(c + 1);
+        // this chunk's accumulators, once its MMAs have completed
+        const bool done = bar_wait(bar_a, (uint32_t)(c & 1));
+        if (done) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             uint32_t r[32];
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
@@ -237,54 +312,14 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
 #pragma unroll
             for (int k = 0; k < NP1; k++)
                 acc[k] += (double)__uint_as_float(r[k]) + (double)__uint_as_float(r[16 + k]);
-        } else {
-            __syncthreads();
         }
-        if (c == nch) break;
-        // operands of chunk c (the tensor core has finished reading chunk c-1's)
-        if (t < ROWS) {
-#pragma unroll
-            for (int k4 = 0; k4 < TC_KC; k4 += 4) {
-                uint32_t h[4], l[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int i = k4 + j;
-                    split_tf32(Lb[(TC_KC + i) * TC_MAXNP1 + k2], Lb[(2 * TC_KC + i) * TC_MAXNP1 + k3], h[j], l[j]);
-                }
-                const uint32_t o = kmajor_off(TC_M, t, k4);
-                *reinterpret_cast<uint4 *>(Ah + o) = make_uint4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<uint4 *>(Al + o) = make_uint4(l[0], l[1], l[2], l[3]);
-            }
-        }
-        {
-            // B rows: thread t covers row k1 = t / 8, particles 4 (t % 8) .. +3
-            const int k1 = t >> 3, k4 = (t & 7) * 4;
-            uint32_t h[4] = {0, 0, 0, 0}, l[4] = {0, 0, 0, 0};
-            if (k1 < NP1) {
-#pragma unroll
-                for (int j = 0; j < 4; j++) split_tf32(qs[k4 + j], Lb[(k4 + j) * TC_MAXNP1 + k1], h[j], l[j]);
-            }
-            const uint32_t o = kmajor_off(TC_N, k1, k4);
-            *reinterpret_cast<uint4 *>(Bh + o) = make_uint4(h[0], h[1], h[2], h[3]);
-            *reinterpret_cast<uint4 *>(Bl + o) = make_uint4(l[0], l[1], l[2], l[3]);
-        }
-        // make the operands visible to the tensor core (async proxy); the
-        // barrier also orders the accumulator loads above before the MMAs
-        // that overwrite those columns
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        // orders the accumulator loads before the next MMAs and the new bases
+        // before the next operands; a wait that expired anywhere ends the loop
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (t == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t ah = smem_addr(Ah), al = smem_addr(Al), bh = smem_addr(Bh), bl = smem_addr(Bl);
-#pragma unroll
-            for (int s = 0; s < TC_KSTEPS; s++) {
-                const uint32_t oa = s * TC_M * 32, ob = s * TC_N * 32;
-                mma_tf32(tmem, smem_desc(ah + oa), smem_desc(bh + ob), s > 0 ? 1u : 0u);
-                mma_tf32(tmem + 16, smem_desc(ah + oa), smem_desc(bl + ob), s > 0 ? 1u : 0u);
-                mma_tf32(tmem + 16, smem_desc(al + oa), smem_desc(bh + ob), 1u);
-            }
-            mma_commit(bar_a);
+        ok = !__syncthreads_or(done ? 0 : 1);
+        if (!ok && t == 0) {
+            // one more bounded wait for the MMAs in flight before the memory is released
+            bar_wait(bar_a, (uint32_t)(c & 1));
         }
     }
     if (ok) {
@@ -294,8 +329,6 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
         }
     } else if (t == 0) {
         atomicExch(err, 1);
-        // one more bounded wait for the MMAs in flight before the memory is released
-        if (!expire_test) bar_wait(bar_a, wpar);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -318,6 +351,218 @@ void p2m_tc_t(int nleaves, const int *leaves, const int *ibeg, const int *numpar
                                                           expire_now);
 }
 
+// ---------------------------------------------------------------------------
+// L2P on the tensor cores (cp_comp_pot, src/interaction_compute/
+// interaction_compute_downpass.c:326-497): the potential of target i from its
+// leaf's grid values Phi[k1, k2, k3] is
+//   phi_i = sum_{k2,k3} Ly_i[k2] Lz_i[k3] G[i, (k2, k3)],
+//   G[i, (k2, k3)] = sum_k1 Lx_i[k1] Phi[k1, (k2, k3)],
+// G a GEMM with the item's 128 targets as M, the (k2, k3) pairs as N (padded
+// to 128) and k1 as K (padded to 16): 2 K steps x 3 products (3xTF32) into
+// 128 TMEM columns.  Each thread (= TMEM lane = target) then reads its row
+// and finishes the (n+1)^2-term contraction in FP32 registers, so the
+// (n+1)^3 multiply-adds per target run on the tensor core.
+// ---------------------------------------------------------------------------
+
+constexpr int L2_M = 128, L2_N = 128, L2_K = 16;
+constexpr uint32_t L2_TMEM_COLS = 128;
+constexpr uint32_t L2_A_BYTES = L2_M * L2_K * 4;        // 8 KB
+constexpr uint32_t L2_B_BYTES = L2_N * L2_K * 4;        // 8 KB
+constexpr uint32_t L2_OFF_A = 0;                        // [hi, lo]
+constexpr uint32_t L2_OFF_B = L2_OFF_A + 2 * L2_A_BYTES;  // [hi, lo]
+constexpr uint32_t L2_OFF_NODES = L2_OFF_B + 2 * L2_B_BYTES;   // float [3][TC_MAXNP1]
+constexpr uint32_t L2_OFF_BAR = (L2_OFF_NODES + 3 * TC_MAXNP1 * 4 + 15) / 16 * 16;
+constexpr uint32_t L2_OFF_MISC = L2_OFF_BAR + 16;
+constexpr uint32_t L2_SMEM = L2_OFF_MISC + 16;
+constexpr uint32_t L2_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(L2_N >> 3) << 17) |
+                              ((uint32_t)(L2_M >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32_l2(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(L2_IDESC), "r"(accumulate));
+}
+
+// Barycentric Lagrange basis in FP32 at a coordinate relative to the grid's
+// centre, with the exact-node rule (the FP32 difference is zero).
+template <int NP1>
+__device__ __forceinline__ void basis_f32(float xr, const float *nd, float *L)
+{
+    constexpr int n = NP1 - 1;
+    float sum = 0.0f;
+    int ex = -1;
+#pragma unroll
+    for (int k = 0; k < NP1; k++) {
+        const float d = xr - nd[k];
+        if (fabsf(d) < FLT_MIN) ex = k;
+        const float w = ((k & 1) ? -1.0f : 1.0f) * ((k == 0 || k == n) ? 0.5f : 1.0f);
+        L[k] = w * __frcp_rn(d);
+        sum += L[k];
+    }
+    if (ex >= 0) {
+#pragma unroll
+        for (int k = 0; k < NP1; k++) L[k] = k == ex ? 1.0f : 0.0f;
+    } else {
+        const float inv = __frcp_rn(sum);
+#pragma unroll
+        for (int k = 0; k < NP1; k++) L[k] *= inv;
+    }
+}
+
+template <int NP1>
+__global__ void __launch_bounds__(TC_THREADS)
+k_l2p_tc(const int2 *__restrict__ items, const int *__restrict__ leaf_node, const int *__restrict__ t_ibeg,
+         const int *__restrict__ t_numpar, const double *__restrict__ t_grid, const double *__restrict__ Phi,
+         const double *__restrict__ tx, const double *__restrict__ ty, const double *__restrict__ tz,
+         double *__restrict__ pot, int *err)
+{
+    constexpr int n = NP1 - 1, ROWS = NP1 * NP1, P = ROWS * NP1;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    float *nodes = reinterpret_cast<float *>(sm + L2_OFF_NODES);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L2_OFF_BAR);
+    uint32_t *misc = reinterpret_cast<uint32_t *>(sm + L2_OFF_MISC);
+    unsigned char *Ah = sm + L2_OFF_A, *Al = Ah + L2_A_BYTES, *Bh = sm + L2_OFF_B, *Bl = Bh + L2_B_BYTES;
+    const int t = threadIdx.x, warp = t >> 5;
+    const int2 it = items[blockIdx.x];
+    const int node = leaf_node[it.x];
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(misc)),
+                     "r"(L2_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const double *g = t_grid + (size_t)node * 3 * NP1;
+    const double cx = 0.5 * (g[0] + g[n]), cy = 0.5 * (g[NP1] + g[NP1 + n]), cz = 0.5 * (g[2 * NP1] + g[2 * NP1 + n]);
+    if (t < 3 * NP1) {
+        const int ax = t / NP1;
+        nodes[t] = (float)(g[t] - (ax == 0 ? cx : ax == 1 ? cy : cz));
+    }
+    // B rows (k2, k3): the grid values over k1, split into TF32 pairs; rows
+    // and columns past the grid stay zero
+    {
+        uint32_t h[L2_K], l[L2_K];
+#pragma unroll
+        for (int k = 0; k < L2_K; k++) h[k] = l[k] = 0u;
+        if (t < ROWS) {
+#pragma unroll
+            for (int k1 = 0; k1 < NP1; k1++) split_tf32((float)Phi[(size_t)node * P + k1 + NP1 * t], h[k1], l[k1]);
+        }
+#pragma unroll
+        for (int k4 = 0; k4 < L2_K; k4 += 4) {
+            const uint32_t o = kmajor_off(L2_N, t, k4);
+            *reinterpret_cast<uint4 *>(Bh + o) = make_uint4(h[k4], h[k4 + 1], h[k4 + 2], h[k4 + 3]);
+            *reinterpret_cast<uint4 *>(Bl + o) = make_uint4(l[k4], l[k4 + 1], l[k4 + 2], l[k4 + 3]);
+        }
+    }
+    __syncthreads();
+    // A row t: this target's Lx, split; its Ly and Lz stay in registers
+    const int ti = it.y * TC_THREADS + t;
+    const bool active = ti < t_numpar[node];
+    const int gi = t_ibeg[node] + (active ? ti : 0);
+    float Ly[NP1], Lz[NP1];
+    {
+        float Lx[NP1];
+        if (active) {
+            basis_f32<NP1>((float)(tx[gi] - cx), nodes, Lx);
+            basis_f32<NP1>((float)(ty[gi] - cy), nodes + NP1, Ly);
+            basis_f32<NP1>((float)(tz[gi] - cz), nodes + 2 * NP1, Lz);
+        } else {
+#pragma unroll
+            for (int k = 0; k < NP1; k++) Lx[k] = Ly[k] = Lz[k] = 0.0f;
+        }
+        uint32_t h[L2_K], l[L2_K];
+#pragma unroll
+        for (int k = 0; k < L2_K; k++) h[k] = l[k] = 0u;
+#pragma unroll
+        for (int k1 = 0; k1 < NP1; k1++) split_tf32(Lx[k1], h[k1], l[k1]);
+#pragma unroll
+        for (int k4 = 0; k4 < L2_K; k4 += 4) {
+            const uint32_t o = kmajor_off(L2_M, t, k4);
+            *reinterpret_cast<uint4 *>(Ah + o) = make_uint4(h[k4], h[k4 + 1], h[k4 + 2], h[k4 + 3]);
+            *reinterpret_cast<uint4 *>(Al + o) = make_uint4(l[k4], l[k4 + 1], l[k4 + 2], l[k4 + 3]);
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    const uint32_t tmem = misc[0];
+    const uint32_t bar_a = smem_addr(bar);
+    if (t == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t ah = smem_addr(Ah), al = smem_addr(Al), bh = smem_addr(Bh), bl = smem_addr(Bl);
+        constexpr int KSTEPS = (NP1 + 7) / 8;
+#pragma unroll
+        for (int s = 0; s < KSTEPS; s++) {
+            const uint32_t oa = s * L2_M * 32, ob = s * L2_N * 32;
+            mma_tf32_l2(tmem, smem_desc(ah + oa), smem_desc(bh + ob), s > 0 ? 1u : 0u);
+            mma_tf32_l2(tmem, smem_desc(ah + oa), smem_desc(bl + ob), 1u);
+            mma_tf32_l2(tmem, smem_desc(al + oa), smem_desc(bh + ob), 1u);
+        }
+        mma_commit(bar_a);
+    }
+    const bool done = bar_wait(bar_a, 0u);
+    const bool ok = !__syncthreads_or(done ? 0 : 1);
+    if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float s3[NP1];
+#pragma unroll
+        for (int k = 0; k < NP1; k++) s3[k] = 0.0f;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int c0 = 0; c0 < ROWS; c0 += 32) {
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                "[%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                const int c = c0 + j;
+                if (c < ROWS) s3[c / NP1] = fmaf(Ly[c % NP1], __uint_as_float(r[j]), s3[c / NP1]);
+            }
+        }
+        float phi = 0.0f;
+#pragma unroll
+        for (int k3 = 0; k3 < NP1; k3++) phi = fmaf(Lz[k3], s3[k3], phi);
+        if (active) pot[gi] += (double)phi;
+    } else if (t == 0) {
+        atomicExch(err, 1);
+        bar_wait(bar_a, 0u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L2_TMEM_COLS));
+    }
+}
+
+template <int NP1>
+void l2p_tc_t(int nitems, const int2 *items, const int *leaf_node, const int *t_ibeg, const int *t_numpar,
+              const double *t_grid, const double *Phi, const double *tx, const double *ty, const double *tz,
+              double *pot, int *err, cudaStream_t st)
+{
+    cudaFuncSetAttribute(k_l2p_tc<NP1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L2_SMEM);
+    k_l2p_tc<NP1><<<nitems, TC_THREADS, L2_SMEM, st>>>(items, leaf_node, t_ibeg, t_numpar, t_grid, Phi, tx, ty, tz,
+                                                         pot, err);
+}
+
 }  // namespace
 
 bool p2m_tc_supported(int n) { return n >= 1 && n + 1 <= TC_MAXNP1; }
@@ -331,6 +576,18 @@ void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const
 #define BT_TC(N) case N: p2m_tc_t<N>(nleaves, leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err, st); return;
         BT_TC(2) BT_TC(3) BT_TC(4) BT_TC(5) BT_TC(6) BT_TC(7) BT_TC(8) BT_TC(9) BT_TC(10) BT_TC(11)
 #undef BT_TC
+    }
+}
+
+void launch_l2p_tc(int n, int nitems, const int2 *items, const int *leaf_node, const int *t_ibeg,
+                   const int *t_numpar, const double *t_grid, const double *Phi, const double *tx, const double *ty,
+                   const double *tz, double *pot, int *err, cudaStream_t st)
+{
+    if (nitems <= 0) return;
+    switch (n + 1) {
+#define BT_L2(N) case N: l2p_tc_t<N>(nitems, items, leaf_node, t_ibeg, t_numpar, t_grid, Phi, tx, ty, tz, pot, err, st); return;
+        BT_L2(2) BT_L2(3) BT_L2(4) BT_L2(5) BT_L2(6) BT_L2(7) BT_L2(8) BT_L2(9) BT_L2(10) BT_L2(11)
+#undef BT_L2
     }
 }
 

@@ -14,4 +14,12 @@ void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const
                    const double *sx, const double *sy, const double *sz, const double *sq, double *Q, int *err,
                    cudaStream_t st);
 
+// L2P (Lagrange) at the target leaves on the tensor cores: each item (leaf,
+// chunk of 128 targets) adds its targets' interpolated grid values to pot
+// (3xTF32, FP32 accumulation); same items and layout as launch_l2p, degrees
+// with (n+1)^2 <= 128.  *err as for launch_p2m_tc.
+void launch_l2p_tc(int n, int nitems, const int2 *items, const int *leaf_node, const int *t_ibeg,
+                   const int *t_numpar, const double *t_grid, const double *Phi, const double *tx, const double *ty,
+                   const double *tz, double *pot, int *err, cudaStream_t st);
+
 }  // namespace bt

@@ -450,6 +450,10 @@ def make_parser():
                     help="auto: learned for the 16M clustered configuration, fixed otherwise")
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--no-fp64-plain", action="store_true", help="skip the FP64 fixed-degree comparison step")
+    ap.add_argument("--fp64-steps", type=int, default=3, help="timed steps of the FP64 fixed-degree comparison")
+    ap.add_argument("--no-baselines", action="store_true",
+                    help="skip the learned selection's baselines (lowest fixed degree meeting the tolerance in "
+                         "mixed and FP64, the reference's beta path, and the split of the speed-up)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-step-seconds", type=float, default=4.0,
                     help="reference arm: host seconds of sampled evaluation per step")
@@ -643,13 +647,82 @@ def main():
                 combine_shards(d_out, world)
             return rep
         step_plain()
-        ms_plain, preps = timed(step_plain, 1)
-        (ms_plain,) = max_over_ranks([ms_plain], world, dev)
+        k_plain = max(1, args.fp64_steps)
+        ms_plain, preps = timed(step_plain, k_plain)
+        (ms_plain,) = max_over_ranks([ms_plain / k_plain], world, dev)
         fp64_plain = {"value": ranks_n / (ms_plain * 1e-3), "unit": "targets/s", "ms_per_step": ms_plain,
-                      "steps": 1, "degree": cfg["degree"],
+                      "steps": k_plain, "degree": cfg["degree"],
                       "rel_l2_vs_fp64_direct": accuracy(d_out.cpu().numpy())[0],
                       "ms_eval_kernel": preps[-1]["ms_eval_kernel"],
                       "interactions": preps[-1]["pp_ptwise"] + preps[-1]["pc_ptwise"]}
+
+    # what the learned selection gains over the method without it: the lowest
+    # fixed degree that meets the tolerance (mixed and FP64), the reference's
+    # beta knob at the lowest beta that meets it, and the headline speed-up
+    # split into its factors (precision, symmetric pass, degree selection)
+    baselines = None
+    if (not args.no_baselines and not shard and not batch and prec == B.PRECISION_MIXED and policy == "learned"
+            and world == 1):
+        def variant(k, **over):
+            kw = dict(common)
+            kw.update(degree_policy=B.DEGREE_FIXED, **over)
+
+            def st():
+                return call([t.data_ptr() for t in d_in[3:6] + d_in[:3] + d_in[6:]], d_out.data_ptr(), True, **kw)
+            st()
+            ms, vreps = timed(st, k)
+            r = vreps[-1]
+            return {"targets_per_s": n / (ms / k * 1e-3), "ms_per_step": ms / k, "steps": k,
+                    "ms_eval_kernel": r["ms_eval_kernel"], "evaluations": r["pp_ptwise"] + r["pc_ptwise"],
+                    "rel_l2_vs_fp64_direct": accuracy(d_out.cpu().numpy())[0],
+                    "precision": "fp64" if kw["precision"] == B.PRECISION_FP64 else "mixed",
+                    "theta": kw["theta"], "degree": kw["degree"], "leaf": kw["max_source_leaf"],
+                    "symmetry": "off" if kw["symmetry"] == B.SYMMETRY_OFF else "auto"}
+
+        def lowest_passing(runs):
+            ok = [r for r in runs if r["rel_l2_vs_fp64_direct"] <= args.tolerance]
+            return min(ok, key=lambda r: r["ms_per_step"]) if ok else None
+
+        # mixed, fixed degree, from the configuration's degree down until the
+        # tolerance is missed (lower degree: fewer far-field terms per pair)
+        mixed_sweep = []
+        for d in range(cfg["degree"], 1, -1):
+            mixed_sweep.append(variant(2, degree=d))
+            if mixed_sweep[-1]["rel_l2_vs_fp64_direct"] > args.tolerance:
+                break
+        mixed_best = lowest_passing(mixed_sweep)
+        # FP64, fixed degree, from the mixed path's best degree down
+        fp64_sweep = []
+        d0 = mixed_best["degree"] if mixed_best else cfg["degree"]
+        for d in range(d0, 1, -1):
+            fp64_sweep.append(variant(1, degree=d, precision=B.PRECISION_FP64, dispatch=B.DISPATCH_AUTO))
+            if fp64_sweep[-1]["rel_l2_vs_fp64_direct"] > args.tolerance:
+                break
+        # the reference's beta knob (theta and degree from beta, the reference
+        # GPU build's leaf size), mixed precision, from beta 0.5 down by 0.1
+        beta_sweep = []
+        for b10 in range(5, 0, -1):
+            bp = B.beta_parameters(b10 / 10, cfg["ctype"], cfg["approx"])
+            r = variant(2, theta=bp["theta"], degree=bp["degree"], size_check=bp["size_check"],
+                        max_source_leaf=bp["max_source_leaf"], max_target_leaf=bp["max_target_leaf"])
+            r["beta"] = bp["beta"]
+            beta_sweep.append(r)
+            if r["rel_l2_vs_fp64_direct"] > args.tolerance:
+                break
+        # the speed-up's factors at the configuration's degree: precision
+        # (FP64 -> mixed, symmetric pass off), the symmetric pass, the selection
+        mixed_nosym = variant(2, degree=cfg["degree"], symmetry=B.SYMMETRY_OFF)
+        mixed_sym = mixed_sweep[0]
+        baselines = {
+            "mixed_fixed_best": mixed_best, "fp64_fixed_best": lowest_passing(fp64_sweep),
+            "beta_auto": lowest_passing(beta_sweep),
+            "sweeps": {"mixed_fixed": mixed_sweep, "fp64_fixed": fp64_sweep, "beta": beta_sweep,
+                       "mixed_fixed_symmetry_off": mixed_nosym},
+            "what": ("device-resident steps like value; each variant one untimed step, then timed steps; rel-L2 "
+                     "against the FP64 direct sum on the same strided targets; *_best = the fastest run of the "
+                     "sweep that meets the tolerance; beta runs use the reference's theta/degree for beta and "
+                     f"its GPU build's leaf size {B.BETA_GPU_LEAF}"),
+        }
 
     # the same evaluation through a session: trees, lists and degree selection
     # built once, then per evaluation the charges go host->device, one CUDA
@@ -720,6 +793,20 @@ def main():
             line["fp64_plain"] = fp64_plain
             line["speedup_vs_fp64_plain"] = {"value": value / fp64_plain["value"],
                                              "e2e": e2e / fp64_plain["value"]}
+        if baselines is not None:
+            line["baselines"] = baselines
+            ratio = {k: (value / baselines[k]["targets_per_s"] if baselines[k] else None)
+                     for k in ("mixed_fixed_best", "fp64_fixed_best", "beta_auto")}
+            line["speedup_vs_baselines"] = ratio
+            if fp64_plain is not None:
+                nosym = baselines["sweeps"]["mixed_fixed_symmetry_off"]["targets_per_s"]
+                sym = baselines["sweeps"]["mixed_fixed"][0]["targets_per_s"]
+                line["speedup_vs_fp64_plain"]["factors"] = {
+                    "precision": nosym / fp64_plain["value"], "symmetric_pass": sym / nosym,
+                    "degree_selection": value / sym,
+                    "what": (f"at the configuration's degree {cfg['degree']}: FP64 -> mixed (symmetric pass off), "
+                             "then the symmetric near-field pass, then the learned selection; their product is "
+                             "the speed-up up to run-to-run noise")}
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(cfg, args.config, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)

@@ -5,10 +5,11 @@
   relative (FP32 accumulation over the batch);
 * labels made by the treecode fall with the degree, and training on them
   with the library's Adam kernels lowers the loss;
-* A/B against the fixed-degree method (degree 10, mixed precision) on a
-  clustered system: with the selector the relative L2 error against the FP64
-  direct sum stays within the 1e-6 tolerance while the number of kernel
-  evaluations drops.
+* A/B against the fixed-degree method (mixed precision) on a clustered
+  system: with the selector the relative L2 error against the FP64 direct sum
+  stays within the 1e-6 tolerance, with fewer kernel evaluations and less
+  kernel time than at degree 10 and than at the lowest fixed degree that
+  meets the tolerance.
 """
 import os
 
@@ -74,19 +75,35 @@ def _selector_weights():
 
 
 def test_learned_vs_fixed_degree_ab():
+    """A/B on a 1M clustered system: the learned selection against fixed
+    degree 10 and against the lowest fixed degree that meets the tolerance
+    (the method without the network, tuned by hand for this system), both in
+    mixed precision with the same theta and leaves."""
     S.install(_selector_weights())
     x, y, z, q = S.blobs(1_000_000, seed=77)
     common = dict(theta=0.7, max_source_leaf=2000, max_target_leaf=2000, precision=B.PRECISION_MIXED,
                   return_report=True)
-    fixed, rf = B.treecode(x, y, z, x, y, z, q, degree=10, **common)
-    learned, rl = B.treecode(x, y, z, x, y, z, q, degree=10, degree_policy=B.DEGREE_LEARNED, tolerance=1e-6, **common)
     idx = np.arange(0, len(x), 97)
     d = B.direct(x[idx], y[idx], z[idx], x, y, z, q)
-    err_fixed = np.linalg.norm(fixed[idx] - d) / np.linalg.norm(d)
-    err_learned = np.linalg.norm(learned[idx] - d) / np.linalg.norm(d)
-    evals_fixed = rf["pp_ptwise"] + rf["pc_ptwise"]
-    evals_learned = rl["pp_ptwise"] + rl["pc_ptwise"]
-    print(f"fixed n=10: rel-L2 {err_fixed:.2e}, {evals_fixed:.3e} evals, kernel {rf['ms_eval_kernel']:.1f} ms; "
-          f"learned: rel-L2 {err_learned:.2e}, {evals_learned:.3e} evals, kernel {rl['ms_eval_kernel']:.1f} ms")
+
+    def run(**kw):
+        pot, r = B.treecode(x, y, z, x, y, z, q, **common, **kw)
+        pot, r = B.treecode(x, y, z, x, y, z, q, **common, **kw)     # second call: warm kernel timing
+        return np.linalg.norm(pot[idx] - d) / np.linalg.norm(d), r["pp_ptwise"] + r["pc_ptwise"], r
+
+    err_learned, evals_learned, rl = run(degree=10, degree_policy=B.DEGREE_LEARNED, tolerance=1e-6)
+    sweep = []
+    for deg in range(10, 1, -1):
+        err, ev, r = run(degree=deg)
+        sweep.append((deg, err, ev, r["ms_eval_kernel"]))
+        print(f"fixed n={deg}: rel-L2 {err:.2e}, {ev:.3e} evals, kernel {r['ms_eval_kernel']:.2f} ms")
+        if err > 1e-6:
+            break
+    print(f"learned: rel-L2 {err_learned:.2e}, {evals_learned:.3e} evals, kernel {rl['ms_eval_kernel']:.2f} ms")
+    passing = [s for s in sweep if s[1] <= 1e-6]
+    assert passing, "no fixed degree meets the tolerance"
+    best = passing[-1]
     assert err_learned <= 1e-6
-    assert evals_learned < 0.8 * evals_fixed
+    assert evals_learned < 0.8 * sweep[0][2]                  # against fixed degree 10
+    assert evals_learned < best[2], f"best fixed degree {best[0]}: {best[2]:.3e} evaluations"
+    assert rl["ms_eval_kernel"] < best[3], f"best fixed degree {best[0]}: {best[3]:.2f} ms"

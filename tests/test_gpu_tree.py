@@ -103,3 +103,27 @@ def test_gpu_tree_eval_matches_host_tree():
         a = B.treecode(tx, ty, tz, sx, sy, sz, sq, tree_build=B.TREE_GPU, **kw)
         b = B.treecode(tx, ty, tz, sx, sy, sz, sq, tree_build=B.TREE_HOST, **kw)
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("ctype,theta,degree,leaf,sc", [(1, 0.7, 8, 50, 1.0), (2, 0.5, 3, 20, 4.0),
+                                                        (1, 0.9, 2, 7, 1.0), (2, 0.8, 6, 300, 1.0)])
+def test_gpu_traversal_lists_match_host_traversal(ctype, theta, degree, leaf, sc):
+    """Particle-cluster and cluster-particle lists traversed on the GPU
+    (bt_gpulists.cu) equal the host traversal's on the same GPU-built trees
+    (BARYTREE_B200_HOST_LISTS selects the host traversal) and the host-built
+    plan's, entry for entry and in order: clustered and duplicate points,
+    deep trees (small leaves), distinct targets."""
+    import os
+    x, y, z = _clustered(4, 12000)
+    tx, ty, tz = _duplicates(5, 9000)
+    args = (tx, ty, tz, x, y, z, ctype, 1, theta, degree, leaf, leaf, sc)
+    gpu = B.interaction_lists(*args, tree_build=B.TREE_GPU)
+    os.environ["BARYTREE_B200_HOST_LISTS"] = "1"
+    try:
+        host = B.interaction_lists(*args, tree_build=B.TREE_GPU)
+    finally:
+        del os.environ["BARYTREE_B200_HOST_LISTS"]
+    ref = B.interaction_lists(*args)
+    assert gpu[0] == host[0] == ref[0] and gpu[1] == host[1] == ref[1]
+    assert len(gpu[2]) > 0
+    assert np.array_equal(gpu[2], host[2]) and np.array_equal(gpu[2], ref[2])
