@@ -1250,11 +1250,17 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
     int64_t sym_total = 0, sym_far_pairs = 0;
     int max_leaf = 0;
     for (int u = 0; u < T.nleaves; u++) max_leaf = std::max(max_leaf, T.numpar[T.leaves[u]]);
-    if (mixed && pl.same_tree && shape.sym && shape.nshards <= 1 && max_leaf <= bt::SYM_MAX_LEAF &&
+    if (mixed && pl.same_tree && shape.sym && max_leaf <= bt::SYM_MAX_LEAF &&
         (o.kernel == COULOMB || o.kernel == YUKAWA || o.kernel == REGULARIZED_COULOMB) && T.nleaves > 1) {
         const int NU = T.nleaves;
         std::vector<int> unit_of(T.n, -1);
         for (int u = 0; u < NU; u++) unit_of[T.leaves[u]] = u;
+        // a pair belongs to the shard that owns its head (the lower leaf):
+        // that shard evaluates it and gathers both sides, the partner's side
+        // into targets another shard owns (the combining sum adds them)
+        std::vector<unsigned char> owned(NU, 1);
+        if (shape.nshards > 1)
+            for (int u = 0; u < NU; u++) owned[u] = leaf_count[u] > 0;
         const int64_t ne = mx_doff[NU];
         // per unit: its partners (other leaves), sorted by node, each with the
         // list entry it came from and whether the boxes are within the
@@ -1310,14 +1316,17 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
                 }
             }
         }
-#pragma omp parallel for schedule(static)
+        int64_t npaired = 0;       // entries in a pair, whichever shard evaluates it
+#pragma omp parallel for schedule(static) reduction(+ : npaired)
         for (int u = 0; u < NU; u++) {
             const int A = T.leaves[u];
             int64_t heads[2] = {0, 0}, all = 0;
             for (int64_t j = mx_doff[u]; j < far_end[u]; j++)
                 if (rev[j] >= 0) {
-                    all++;
-                    heads[fnear[j]] += A < far[j] ? 1 : 0;
+                    npaired++;
+                    const bool head = A < far[j];
+                    if (head ? owned[u] : owned[unit_of[far[j]]]) all++;
+                    heads[fnear[j]] += head && owned[u] ? 1 : 0;
                 }
             poff0[u + 1] = heads[0];
             poff1[u + 1] = heads[1];
@@ -1332,7 +1341,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         for (int u = 0; u < NU; u++) poff1[u + 1] += poff1[u];
         pt.mark("plan: symmetric: reverse look-ups");
         const int64_t npairs = poff1[NU];
-        if (npairs > 0) {
+        if (npaired > 0) {
             // pairs headed by each unit, and the pair number of each head entry
             sym_pairs.resize((size_t)npairs);
             hvec<int64_t> pid(ne);
@@ -1342,7 +1351,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
                 const int A = T.leaves[u];
                 int64_t p[2] = {poff0[u], poff1[u]}, sz[2] = {0, 0};
                 for (int64_t j = mx_doff[u]; j < far_end[u]; j++)
-                    if (rev[j] >= 0 && A < far[j]) {
+                    if (rev[j] >= 0 && A < far[j] && owned[u]) {
                         const int g = fnear[j];
                         pid[j] = p[g];
                         sym_pairs[p[g]++] = make_int2(A, far[j]);
@@ -1383,15 +1392,21 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
                 for (int64_t j = mx_doff[u]; j < far_end[u]; j++) {
                     if (rev[j] < 0) continue;
                     const int B = far[j];
-                    sym_in_slot[w++] = A < B ? sym_slot[pid[j]] : sym_slot[pid[rev[j]]] + S.numpar[B];
+                    // both directions leave the lists; only this shard's pairs are gathered
                     drop[mx_doff[u] + fent[j]] = 1;
+                    if (!(A < B ? owned[u] : owned[unit_of[B]])) continue;
+                    sym_in_slot[w++] = A < B ? sym_slot[pid[j]] : sym_slot[pid[rev[j]]] + S.numpar[B];
                 }
             }
             pt.mark("plan: symmetric: pairs and slots");
             // both directions leave the per-target near-field lists
             std::vector<int64_t> noff(NU + 1, 0);
 #pragma omp parallel for schedule(static)
-            for (int u = 0; u < NU; u++) noff[u + 1] = (mx_doff[u + 1] - mx_doff[u]) - (ioff[u + 1] - ioff[u]);
+            for (int u = 0; u < NU; u++) {
+                int64_t kept = 0;
+                for (int64_t k = mx_doff[u]; k < mx_doff[u + 1]; k++) kept += !drop[k];
+                noff[u + 1] = kept;
+            }
             for (int u = 0; u < NU; u++) noff[u + 1] += noff[u];
             hvec<int> nidx((size_t)noff[NU]);
             hvec<unsigned char> nflag((size_t)noff[NU]);
@@ -1722,15 +1737,6 @@ std::vector<float> g_selector;      // installed MLP weights (bt_selector_set), 
 std::mutex g_selector_mu;
 constexpr double SELECT_MARGIN_DECADES = 0.5;   // predicted error must sit this far below the budget
 
-// The constant c of the per-batch budget selection (bt::launch_select_budget);
-// 0 selects the per-interaction rule (predicted error SELECT_MARGIN_DECADES
-// below the tolerance).  BARYTREE_B200_SELECT_SHARE overrides it (calibration).
-double select_share_constant()
-{
-    const char *e = getenv("BARYTREE_B200_SELECT_SHARE");
-    return e ? atof(e) : 0.0;
-}
-
 void node_geometry(const bt_tree &t, std::vector<double> &ctr, std::vector<double> &rad)
 {
     ctr.resize(3 * (size_t)t.n);
@@ -1758,7 +1764,6 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
     const bt_tree &S = pl.st, &T = pl.tt;
     PhaseTimer pt;
     const int64_t ne = pl.t_approx.off[pl.t_approx.rows];
-    const double share_c = select_share_constant();
     std::vector<unsigned char> choice(ne > 0 ? ne : 1);
     cudaStream_t st = ctx->stream;
     int rc = BT_OK;
@@ -1782,14 +1787,6 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
         L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size());
         L.add(&d_pred, (size_t)ne * bt::MLP_OUT); L.add(&d_choice, ne);
-        // per-batch budget: the near-field lists and one share per batch
-        const int64_t nd = pl.t_direct.off[pl.t_direct.rows];
-        int64_t *d_doff = nullptr;
-        int *d_didx = nullptr;
-        float *d_share = nullptr;
-        if (share_c > 0) {
-            L.add(&d_doff, pl.t_direct.rows + 1); L.add(&d_didx, nd > 0 ? nd : 1); L.add(&d_share, pl.t_approx.rows);
-        }
         if (!arena.reserve(L.total())) {
             set_err(arena.fixed ? "degree selection needs more scratch than the static array holds"
                                 : "device allocation failed");
@@ -1807,7 +1804,6 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             UP(d_idx, pl.t_approx.idx, ne); UP(d_unit, T.leaves, T.nleaves);
             UP(d_off, pl.t_approx.off, pl.t_approx.rows + 1); UP(d_w, w.data(), w.size());
 #undef UP
-#define UP2(dst, src, cnt) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
             bt::MomentTree mt{S.n, S.nleaves, S.max_depth, d_sleaves, d_sibeg, d_snum, d_snch, d_sch, d_slvl, S.lvl_off};
             long long launches = bt::launch_node_moments(mt, d_sq, d_mom, st);
             bt::FeatureArgs fa;
@@ -1818,17 +1814,9 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             launches++;
             bt::mlp_infer(d_w, ne, d_feat, d_pred, st);
             launches++;
-            if (share_c > 0) {
-                UP2(d_doff, pl.t_direct.off, pl.t_direct.rows + 1);
-                if (nd > 0) UP2(d_didx, pl.t_direct.idx, nd);
-                bt::launch_select_budget(fa, d_doff, d_didx, share_c * tol, ne, d_pred, d_feat, d_share, d_choice, st);
-                launches += 2;
-            } else {
-                bt::launch_select(ne, d_pred, d_feat, (float)(log10(tol) - SELECT_MARGIN_DECADES), d_choice, st);
-                launches++;
-            }
+            bt::launch_select(ne, d_pred, d_feat, (float)(log10(tol) - SELECT_MARGIN_DECADES), d_choice, st);
+            launches++;
             CK(cudaGetLastError());
-#undef UP2
             CK(cudaMemcpyAsync(choice.data(), d_choice, ne, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             g_launches += launches;
@@ -2543,7 +2531,6 @@ long bt_selector_training_data(int n, const double *x, const double *y, const do
             }
         }
         {
-#define UP2(dst, src, cnt) CK(cudaMemcpyAsync(dst, src, sizeof(*(src)) * (size_t)(cnt), cudaMemcpyHostToDevice, st))
             bt::MomentTree mt{S.n, S.nleaves, S.max_depth, d_sleaves, d_sibeg, d_snum, d_snch, d_sch, d_slvl, S.lvl_off};
             launches += bt::launch_node_moments(mt, d_sq, d_mom, st);
         }

@@ -453,86 +453,6 @@ void launch_labels(const LabelArgs &a, int nsamples, cudaStream_t st)
     if (nsamples > 0) k_labels<<<nsamples, LBL_TARGETS, 0, st>>>(a);
 }
 
-// Per-batch error budget.  With the normalised prediction e (log10 of the
-// interaction's error over |q_C|_2 / d), the interaction's absolute error is
-// about 10^e |q_C|_2 / d.  Errors of a batch's interactions add at its
-// targets roughly like independent terms, so the batch's budget is shared
-// equally: each of its N cluster entries may contribute
-//   c tol Phi_u / sqrt(N),
-// Phi_u^2 = sum over its cluster entries of (|q_C|_2 / d)^2 + sum over its
-// near-field leaves L of 3 |q_L|_2^2 / max(d_L, r_L)^2
-// -- an estimate of the mean square potential at the batch's targets from
-// charges of either sign (3 / R^2 is the mean of 1 / r^2 over a ball of
-// radius R).  One warp per batch writes log10 of that share.
-__global__ void k_unit_budget(FeatureArgs a, const int64_t *__restrict__ d_off, const int *__restrict__ d_idx,
-                              double c_tol, float *__restrict__ log_share)
-{
-    const int u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (u >= a.units) return;
-    const int tn = a.unit_node[u];
-    const double tx = a.t_ctr[3 * tn], ty = a.t_ctr[3 * tn + 1], tz = a.t_ctr[3 * tn + 2];
-    double phi2 = 0.0;
-    for (int64_t e = a.off[u] + lane; e < a.off[u + 1]; e += 32) {
-        const int s = a.idx[e];
-        const double dx = tx - a.s_ctr[3 * s], dy = ty - a.s_ctr[3 * s + 1], dz = tz - a.s_ctr[3 * s + 2];
-        const double q2 = a.s_mom[2 * s + 1];
-        phi2 += q2 * q2 / (dx * dx + dy * dy + dz * dz);
-    }
-    for (int64_t e = d_off[u] + lane; e < d_off[u + 1]; e += 32) {
-        const int s = d_idx[e];
-        const double dx = tx - a.s_ctr[3 * s], dy = ty - a.s_ctr[3 * s + 1], dz = tz - a.s_ctr[3 * s + 2];
-        const double q2 = a.s_mom[2 * s + 1], r = a.s_rad[s];
-        const double d2 = fmax(dx * dx + dy * dy + dz * dz, r * r);
-        if (d2 > 0.0) phi2 += 3.0 * q2 * q2 / d2;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) phi2 += __shfl_xor_sync(0xffffffffu, phi2, o);
-    if (lane == 0) {
-        const double n = (double)max((int64_t)1, a.off[u + 1] - a.off[u]);
-        const double share = c_tol * sqrt(phi2 / n);
-        log_share[u] = share > 0.0 ? (float)log10(share) : -1.0e30f;
-    }
-}
-
-// choice per interaction under its batch's share: lowest degree d with
-// e_d + log10(|q_C|_2 / d) <= log10(share); direct evaluation as in k_select.
-__global__ void k_select_budget(FeatureArgs a, int64_t n, const float *__restrict__ pred,
-                                const float *__restrict__ feat, const float *__restrict__ log_share,
-                                unsigned char *__restrict__ choice)
-{
-    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    int lo = 0, hi = a.units;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (a.off[mid] <= e) lo = mid; else hi = mid;
-    }
-    const int tn = a.unit_node[lo], s = a.idx[e];
-    const double dx = a.t_ctr[3 * tn] - a.s_ctr[3 * s], dy = a.t_ctr[3 * tn + 1] - a.s_ctr[3 * s + 1],
-                 dz = a.t_ctr[3 * tn + 2] - a.s_ctr[3 * s + 2];
-    const double scale = a.s_mom[2 * s + 1] / sqrt(dx * dx + dy * dy + dz * dz);
-    const float budget = scale > 0.0 ? log_share[lo] - (float)log10(scale) : 1.0e30f;
-    unsigned char c = MLP_PP;
-    for (int d = MLP_DMIN; d <= MLP_DMAX; d++) {
-        if (pred[e * MLP_OUT + (d - MLP_DMIN)] <= budget) { c = (unsigned char)d; break; }
-    }
-    const float ns = exp10f(feat[e * MLP_IN + 0]);
-    if (c != MLP_PP) {
-        const float P = (float)((c + 1) * (c + 1) * (c + 1));
-        if (P >= ns) c = MLP_PP;
-    }
-    choice[e] = c;
-}
-
-void launch_select_budget(const FeatureArgs &a, const int64_t *d_off, const int *d_idx, double c_tol, int64_t n,
-                          const float *pred, const float *feat, float *log_share, unsigned char *choice,
-                          cudaStream_t st)
-{
-    if (n <= 0 || a.units <= 0) return;
-    k_unit_budget<<<(a.units + 7) / 8, 256, 0, st>>>(a, d_off, d_idx, c_tol, log_share);
-    k_select_budget<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, n, pred, feat, log_share, choice);
-}
-
 void launch_select(int64_t n, const float *pred, const float *feat, float log_budget, unsigned char *choice,
                    cudaStream_t st)
 {

@@ -62,13 +62,5 @@ void launch_features_pairs(const FeatureArgs &a, int n, const int *tnodes, const
 void launch_labels(const LabelArgs &a, int nsamples, cudaStream_t st);
 void launch_select(int64_t n, const float *pred, const float *feat, float log_budget, unsigned char *choice,
                    cudaStream_t st);
-// Selection under a per-batch error budget: every cluster entry of batch u
-// may contribute c_tol * Phi_u / sqrt(N_u) (absolute), Phi_u the batch's
-// potential scale estimated from the node charge moments of its cluster and
-// near-field entries (d_off / d_idx: its near-field leaves).  log_share:
-// `units` floats of scratch.
-void launch_select_budget(const FeatureArgs &a, const int64_t *d_off, const int *d_idx, double c_tol, int64_t n,
-                          const float *pred, const float *feat, float *log_share, unsigned char *choice,
-                          cudaStream_t st);
 
 }  // namespace bt

@@ -73,15 +73,33 @@ __device__ __forceinline__ uint32_t kmajor_off(int rows, int row, int k)
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// 1/d in FP32: the MUFU approximation refined by one Newton-Raphson step
+// r <- r (2 - d r), which leaves about one ulp of error
+__device__ __forceinline__ float rcp_nr(float d)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+    return r * fmaf(-d, r, 2.0f);
+}
+
 constexpr uint32_t TF32_MASK = 0xFFFFE000u;     // sign, exponent and the 10 stored mantissa bits of a TF32
 
-// p = hi + lo with hi = p truncated to TF32 and lo the exact FP32 rest, also
-// truncated to TF32: both are valid TF32 bit patterns, and hi + lo carries p
-// to about 2^-21 relative (the 3xTF32 products hi*hi + hi*lo + lo*hi)
+// x rounded to the nearest TF32 (ties away from zero): adding half a TF32
+// ulp to the magnitude bits and clearing the 13 low bits carries into the
+// exponent where the mantissa overflows, as rounding should (finite x well
+// below FLT_MAX, as here)
+__device__ __forceinline__ uint32_t tf32_round(float x)
+{
+    return (__float_as_uint(x) + 0x1000u) & TF32_MASK;
+}
+
+// p = hi + lo with hi = p rounded to TF32 and lo the rest (exact in FP32),
+// also rounded: hi + lo carries p to about 2^-22 relative, without bias (the
+// 3xTF32 products hi*hi + hi*lo + lo*hi)
 __device__ __forceinline__ void split_tf32(float p, uint32_t &hi, uint32_t &lo)
 {
-    hi = __float_as_uint(p) & TF32_MASK;
-    lo = __float_as_uint(p - __uint_as_float(hi)) & TF32_MASK;
+    hi = tf32_round(p);
+    lo = tf32_round(p - __uint_as_float(hi));
 }
 
 // Shared-memory matrix descriptor: no swizzle, K-major; LBO = distance of the
@@ -198,14 +216,26 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
     // Bases of one chunk: warp a < 3 evaluates axis a for the chunk's 32
     // particles (lane = particle), barycentric form in FP32 with the
     // exact-node rule on the FP32 relative coordinate; the x bases carry the
-    // charge.  Particles past the leaf's end get zero bases.
-    auto bases = [&](int c) {
+    // charge.  Particles past the leaf's end get zero bases.  The coordinate
+    // (and charge) of a lane's particle are loaded one chunk ahead, so the
+    // global-memory latency overlaps the previous chunk's work.
+    const double *src = warp == 0 ? sx : warp == 1 ? sy : sz;
+    const double ctr = warp == 0 ? cx : warp == 1 ? cy : cz;
+    auto fetch = [&](int c, double &v, double &qv) {
+        const int i = c * TC_KC + lane;
+        v = 0.0;
+        qv = 0.0;
+        if (warp < 3 && c < nch && i < m) {
+            v = src[b0 + i];
+            if (warp == 0) qv = sq[b0 + i];
+        }
+    };
+    auto bases = [&](int c, double v, double qv) {
         if (warp >= 3) return;
         const int i = c * TC_KC + lane;
         float L[NP1];
         if (i < m) {
-            const double *src = warp == 0 ? sx : warp == 1 ? sy : sz;
-            const float xr = (float)(src[b0 + i] - (warp == 0 ? cx : warp == 1 ? cy : cz));
+            const float xr = (float)(v - ctr);
             const float *nd = nodes + warp * NP1;
             float sum = 0.0f;
             int ex = -1;
@@ -214,16 +244,15 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
                 const float d = xr - nd[k];
                 if (fabsf(d) < FLT_MIN) ex = k;
                 const float w = ((k & 1) ? -1.0f : 1.0f) * ((k == 0 || k == n) ? 0.5f : 1.0f);
-                L[k] = w * __frcp_rn(d);
+                L[k] = w * rcp_nr(d);
                 sum += L[k];
             }
-            float scale = __frcp_rn(sum);
-            if (warp == 0) scale *= (float)sq[b0 + i];
+            const float qf = warp == 0 ? (float)qv : 1.0f;
             if (ex >= 0) {
-                const float qv = warp == 0 ? (float)sq[b0 + i] : 1.0f;
 #pragma unroll
-                for (int k = 0; k < NP1; k++) L[k] = k == ex ? qv : 0.0f;
+                for (int k = 0; k < NP1; k++) L[k] = k == ex ? qf : 0.0f;
             } else {
+                const float scale = rcp_nr(sum) * qf;
 #pragma unroll
                 for (int k = 0; k < NP1; k++) L[k] *= scale;
             }
@@ -239,7 +268,10 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
     // products into columns 16-31, from zero (short FP32 sums on the tensor
     // core), folded into FP64 registers once its MMAs have completed.  The
     // next chunk's bases are evaluated while the tensor core works.
-    if (ok) bases(0);
+    double pv, pq;                 // the next chunk's coordinate and charge (prefetched)
+    fetch(0, pv, pq);
+    if (ok) bases(0, pv, pq);
+    fetch(1, pv, pq);
     __syncthreads();
     for (int c = 0; c < nch && ok; c++) {
         // A rows (k2, k3): Ly[k2] * Lz[k3] for the chunk's particles
@@ -291,7 +323,10 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
             mma_commit(bar_a);
         }
         // the next chunk's bases (the operands of this chunk are formed)
-        if (c + 1 < nch) bases(c + 1);
+        if (c + 1 < nch) {
+            bases(c + 1, pv, pq);
+            fetch(c + 2, pv, pq);
+        }
         // this chunk's accumulators, once its MMAs have completed
         const bool done = bar_wait(bar_a, (uint32_t)(c & 1));
         if (done) {
@@ -401,14 +436,14 @@ __device__ __forceinline__ void basis_f32(float xr, const float *nd, float *L)
         const float d = xr - nd[k];
         if (fabsf(d) < FLT_MIN) ex = k;
         const float w = ((k & 1) ? -1.0f : 1.0f) * ((k == 0 || k == n) ? 0.5f : 1.0f);
-        L[k] = w * __frcp_rn(d);
+        L[k] = w * rcp_nr(d);
         sum += L[k];
     }
     if (ex >= 0) {
 #pragma unroll
         for (int k = 0; k < NP1; k++) L[k] = k == ex ? 1.0f : 0.0f;
     } else {
-        const float inv = __frcp_rn(sum);
+        const float inv = rcp_nr(sum);
 #pragma unroll
         for (int k = 0; k < NP1; k++) L[k] *= inv;
     }

@@ -99,14 +99,18 @@ typedef struct bt_options {
                              BT_DISPATCH_QUEUE (persistent blocks taking cost-sorted
                              work items from a device counter) or BT_DISPATCH_GRID
                              (one block per work item); results are identical     */
-    int upward;           /* mixed Lagrange upward pass: BT_UPWARD_AUTO (default: leaf
-                             P2M on the tensor cores in 3xTF32 where (n+1)^2 <= 128)
-                             or BT_UPWARD_FP64 (FP64 SIMT, as the FP64 path)         */
+    int upward;           /* mixed Lagrange leaf contractions: BT_UPWARD_AUTO (default:
+                             leaf P2M, and the leaf L2P of grid outputs, on the
+                             tensor cores in 3xTF32 where (n+1)^2 <= 128) or
+                             BT_UPWARD_FP64 (FP64 SIMT, as the FP64 path)            */
     /* Target sharding: with shard_count > 1 the call evaluates shard_index's
      * share of the target leaves (contiguous in tree order, equal estimated
      * cost) and leaves the other potentials 0; the sum of the outputs of all
-     * shards is the unsharded result with BT_SYMMETRY_OFF, bit for bit
-     * (shards do not pair leaves across shards).  Trees, lists and proxies
+     * shards is the unsharded result, bit for bit without the symmetric
+     * pass.  With it, a pair of near-field leaves belongs to the shard that
+     * owns its lower leaf, which also adds the partner's side into targets
+     * another shard owns; the sum then agrees with the unsharded result to
+     * FP64 rounding (the slice sums are grouped by shard).  Trees, lists and proxies
      * are built in full by every shard; with target grids (cluster-particle,
      * cluster-cluster) a shard evaluates the grids of its leaves and their
      * ancestors only, so the grids of shared ancestors are evaluated by
@@ -115,7 +119,7 @@ typedef struct bt_options {
     int shard_count;
     int symmetry;         /* mixed path, targets = sources (all of a batch's systems),
                              Coulomb, Yukawa or regularized Coulomb, leaves of at most 2048
-                             particles, not sharded: BT_SYMMETRY_AUTO (default)
+                             particles: BT_SYMMETRY_AUTO (default)
                              evaluates each pair of near-field leaves that list each
                              other (and can hold no close pair) once for both sides;
                              BT_SYMMETRY_OFF evaluates every direction separately.

@@ -5,7 +5,10 @@ and proxies, evaluates a contiguous run of target leaves of about equal cost
 leaves the other potentials 0, so one all-reduce (sum) over the shards gives
 the result.  Here the shards run one after another on one GPU: their sum
 must equal the unsharded potentials bit for bit, every target must come from
-exactly one shard, and the shards' costs must be balanced."""
+exactly one shard, and the shards' costs must be balanced.  With the
+symmetric near-field pass (targets = sources) a leaf pair's partner side can
+land on targets another shard owns; those sums agree with the unsharded
+result to FP64 rounding."""
 import numpy as np
 import pytest
 
@@ -42,18 +45,30 @@ def test_sharded_learned_degrees_and_sessions():
     x, y, z, q = _clustered(300000, 32)
     kw = dict(theta=0.7, degree=10, max_source_leaf=2000, max_target_leaf=2000, size_check=1.0,
               precision=B.PRECISION_MIXED, degree_policy=B.DEGREE_LEARNED, tolerance=1e-6)
-    # sharded calls evaluate every near-field direction themselves (no leaf
-    # pairs across shards): their sum is the unsharded call without the
-    # symmetric pass, bit for bit
-    full = B.treecode(x, y, z, x, y, z, q, symmetry=B.SYMMETRY_OFF, **kw)
-    parts = [B.treecode(x, y, z, x, y, z, q, shard=(k, 2), **kw) for k in range(2)]
-    assert np.array_equal(parts[0] + parts[1], full)
+    # without the symmetric pass every shard evaluates its own targets only:
+    # the sum is the unsharded result bit for bit
+    off = dict(kw, symmetry=B.SYMMETRY_OFF)
+    full_off = B.treecode(x, y, z, x, y, z, q, **off)
+    parts = [B.treecode(x, y, z, x, y, z, q, shard=(k, 2), **off) for k in range(2)]
+    assert np.array_equal(parts[0] + parts[1], full_off)
+    # with it, a leaf pair belongs to the shard owning its head leaf, which
+    # adds the partner's side into targets the other shard owns: the pair
+    # values are the unsharded ones, and the sum differs from the unsharded
+    # result only by the grouping of the FP64 sums of a leaf's slices
+    full = B.treecode(x, y, z, x, y, z, q, **kw)
+    parts, reps = zip(*[B.treecode(x, y, z, x, y, z, q, shard=(k, 2), return_report=True, **kw) for k in range(2)])
+    _, rfull = B.treecode(x, y, z, x, y, z, q, return_report=True, **kw)
+    assert rfull["sym_ptwise"] > 0 and all(r["sym_ptwise"] > 0 for r in reps)
+    assert reps[0]["sym_ptwise"] + reps[1]["sym_ptwise"] == rfull["sym_ptwise"]
+    total = parts[0] + parts[1]
+    assert np.max(np.abs(total - full)) <= 1e-13 * np.max(np.abs(full))
+    assert np.linalg.norm(total - full_off) <= 5e-7 * np.linalg.norm(full_off)
     sparts = []
     for k in range(2):
         s = B.Session([(x, y, z, x, y, z, q)], shard=(k, 2), **kw)
         sparts.append(s.evaluate(q)[0])
         s.close()
-    assert np.array_equal(sparts[0] + sparts[1], full)
+    assert np.array_equal(sparts[0], parts[0]) and np.array_equal(sparts[1], parts[1])
 
 
 def test_one_shard_is_the_unsharded_call():
