@@ -46,7 +46,17 @@ namespace bt {
 namespace {
 
 constexpr int SY_THREADS = 128;
-constexpr int SY_TPT = 4;                      // targets of A per thread: two packed pairs
+// targets of A per thread (packed in pairs) and the resident blocks per SM
+// the register budget is sized for; build-time choices.  Measured on the 16M
+// clustered step: 4 and 6 (856 ms) against 6 and 4 (872 ms), 8 and 4
+// (886 ms), 8 and 3 (894 ms)
+#ifndef BT_SYM_TPT
+#define BT_SYM_TPT 4
+#endif
+#ifndef BT_SYM_MIN_BLOCKS
+#define BT_SYM_MIN_BLOCKS 6
+#endif
+constexpr int SY_TPT = BT_SYM_TPT;
 constexpr int SY_NP = SY_TPT / 2;
 constexpr int SY_CHUNK = SY_TPT * SY_THREADS;  // targets of A per pass
 constexpr int SY_TILE = 512;                   // sources of B per shared-memory tile
@@ -133,7 +143,7 @@ __device__ int near_box(int *out, int n, int base, const double *__restrict__ x,
 }
 
 template <int KT, bool CLAMP>
-__global__ void __launch_bounds__(SY_THREADS, 6) k_pp_sym(SymArgs a)
+__global__ void __launch_bounds__(SY_THREADS, BT_SYM_MIN_BLOCKS) k_pp_sym(SymArgs a)
 {
     __shared__ __align__(16) f2_t tile[SY_TILE][4];     // {x, x}, {y, y}, {z, z}, {q, q}
     __shared__ float red[SY_WARPS][SY_TILE];
