@@ -9,11 +9,20 @@ chosen configuration.
   e2e    -- targets/s through the C ABI with pinned host buffers, host->device
             copies of the inputs and the device->host read of the potentials
             inside the timed region
-  roofline -- the dominant kernel (particle-output evaluation, PC + PP):
-            algorithmic FLOPs / its CUDA-event time against the SIMT FMA peak
-            measured on this GPU by the library's probes
-  cpu_baseline -- the reference BaryTree (built from its own sources) on a
-            bounded sample of the workload on the host cores
+  roofline -- the dominant kernels (particle-output evaluation, PC + PP, and
+            the symmetric near-field pairs): evaluations per second against
+            the MUFU rsqrt rate measured on this GPU by the library's probe
+            (mixed Lagrange), or FLOP/s against the measured FMA peak; DRAM
+            traffic from the committed ncu summary of the same workload
+  fp64_plain, baselines -- the plain FP64 treecode at the configuration's
+            degree (the north_star denominator), and for the learned
+            selection the lowest fixed degree meeting the tolerance (mixed and
+            FP64) and the reference's beta knob, with the speed-up's factors
+  cpu_baseline -- the reference BaryTree (built from its own sources) on the
+            host cores: the full system for configurations 1, 3 and 5 (its
+            setup timed, its evaluation sampled by target batch and
+            extrapolated by the interaction count), smaller independent
+            systems for 2 and 4
 
 Multi-GPU (--gpus N under torchrun): every rank evaluates its own independent
 system of the configuration (weak scaling, no data-path collective); the
@@ -306,10 +315,10 @@ def cpu_baseline(cfg, config_id, cores):
 
 # committed ncu summaries that carry a DRAM traffic figure for a configuration,
 # and what that figure is
-PROFILE_FOR_CONFIG = {5: ("eval_targets_mixed_blobs2M.md",
-                          "estimate: ncu captures of the three evaluation kernels on the 2M reduction of this "
-                          "configuration (815.5 MB), scaled x8 by the particle count to N = 16M; not a capture "
-                          "of the 16M launch")}
+PROFILE_FOR_CONFIG = {5: ("eval_traffic_blobs16M.md",
+                          "ncu capture (one pass per kernel) of the 16M evaluation's four kernels "
+                          "(k_eval_targets_mixed_rb, k_pp_sym x2, k_sym_gather), second evaluation of the process: "
+                          "dram__bytes_read.sum + dram__bytes_write.sum summed")}
 
 
 def traffic_from_profiles(config_id, n_override=None):
