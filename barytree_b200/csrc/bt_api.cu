@@ -828,7 +828,15 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
             }
         }
     } else if (need_src_clusters && ns > 0) {
-        if (herm) {
+        static_assert(sizeof(bt::HermChunkTc) == sizeof(bt::HermChunk), "the two chunk types share one array");
+        if (herm && v.tc_up && bt::p2m_hermite_tc_supported(n)) {
+            // mixed Hermite: the 8 moments per chunk on the tensor cores, then
+            // the same reduction of the nodes with several chunks
+            bt::launch_p2m_hermite_tc(n, v.n_hchunks, reinterpret_cast<const bt::HermChunkTc *>(v.d_hchunks), d_sgrid,
+                                      d_slen, d_ww, d_sx, d_sy, d_sz, d_sq, d_Q, v.d_hpartial, v.d_err, st);
+            bt::launch_hermite_reduce(n, v.n_hred, v.d_hred, v.d_hpartial, d_Q, st);
+            launches += v.n_hred > 0 ? 2 : 1;
+        } else if (herm) {
             bt::launch_p2m_hermite(n, v.n_hchunks, v.d_hchunks, v.n_hred, v.d_hred, d_sgrid, d_slen, d_ww, d_sx, d_sy,
                                    d_sz, d_sq, d_Q, v.d_hpartial, st);
             launches += v.n_hred > 0 ? 2 : 1;
@@ -1604,7 +1612,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.queue = shape.queue;
         v.tpt = shape.tpt;
         v.tile = shape.tile;
-        v.tc_up = shape.tc_up && mixed && !herm;
+        v.tc_up = shape.tc_up && mixed;
         v.sharded = shape.nshards > 1;
         v.sym_npairs = (int)sym_pairs.size();
         v.sym_far_pairs = (int)sym_far_pairs;

@@ -516,6 +516,11 @@ void launch_p2m_hermite(int n, int nchunks, const HermChunk *chunks, int nred, c
     default:
         k_p2m_hermite_chunks<<<nchunks, HP2M_THREADS, 0, st>>>(n, chunks, grid, box_len, ww, sx, sy, sz, sq, Q, partial);
     }
+    launch_hermite_reduce(n, nred, red, partial, Q, st);
+}
+
+void launch_hermite_reduce(int n, int nred, const int3 *red, const double *partial, double *Q, cudaStream_t st)
+{
     if (nred > 0) {
         const int width = 8 * (n + 1) * (n + 1) * (n + 1);
         dim3 g((width + 255) / 256, nred);

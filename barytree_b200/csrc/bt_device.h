@@ -51,6 +51,8 @@ int hermite_chunks(int nnodes, const int *ibeg, const int *numpar, std::vector<H
 void launch_p2m_hermite(int n, int nchunks, const HermChunk *chunks, int nred, const int3 *red, const double *grid,
                         const double *box_len, const double *ww, const double *sx, const double *sy, const double *sz,
                         const double *sq, double *Q, double *partial, cudaStream_t st);
+// Q of every node with several chunks: the sum of its partial moments in chunk order.
+void launch_hermite_reduce(int n, int nred, const int3 *red, const double *partial, double *Q, cudaStream_t st);
 void launch_m2m(int n, int nparents, const int *parents, const int *nchild, const int *child, const double *grid,
                 double *Q, cudaStream_t st);
 void launch_l2l(int n, int nparents, const int *parents, const int *nchild, const int *child, const double *grid,

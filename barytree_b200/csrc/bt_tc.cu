@@ -387,6 +387,258 @@ void p2m_tc_t(int nleaves, const int *leaves, const int *ibeg, const int *numpar
 }
 
 // ---------------------------------------------------------------------------
+// Hermite P2M on the tensor cores (pc_comp_ms_modifiedF_hermite,
+// src/clusters/clusters.c:1224-1514): the 8 moments of a node,
+//   Q_m[k1, k2, k3] = sum_i q_i X_i[k1] Y_i[k2] Z_i[k3],
+// each of X, Y, Z the value basis A or the derivative basis B of its axis
+// (m = AAA, BAA, ABA, AAB, BBA, ABB, BAB, BBB in x, y, z), are one GEMM:
+// rows (yz pair, k2, k3) of Y*Z for the four pairs AA, BA, AB, BB
+// (4 (n+1)^2 <= 256 rows: two M = 128 tiles), columns (x basis, k1) of
+// q X for A and B (2 (n+1) <= 16), the particles as K.  Same chunking as
+// the FP64 kernels (HermChunk: a node's particles in chunks of up to 2048,
+// partial moments summed by k_hermite_reduce) and the same pipeline as
+// k_p2m_tc: FP32 bases at FP32 relative coordinates, 3xTF32 products in
+// TMEM, folded into FP64 every 32 particles.  Degrees with n + 1 <= 8.
+// ---------------------------------------------------------------------------
+
+constexpr int HT_MAXNP1 = 8;
+constexpr uint32_t HT_A_TILE = TC_M * TC_KC * 4;                  // 16 KB per 128-row tile
+constexpr uint32_t HT_OFF_A = 0;                                  // [tile 0 hi, tile 1 hi, tile 0 lo, tile 1 lo]
+constexpr uint32_t HT_OFF_B = HT_OFF_A + 4 * HT_A_TILE;           // [hi, lo]
+constexpr uint32_t HT_OFF_L = HT_OFF_B + 2 * B_BYTES;             // float [axis][A/B][k][LSTR]
+constexpr uint32_t HT_OFF_NODES = HT_OFF_L + 3 * 2 * HT_MAXNP1 * LSTR * 4;   // float [3][8] nodes, [3][8] w_x
+constexpr uint32_t HT_OFF_BAR = (HT_OFF_NODES + 2 * 3 * HT_MAXNP1 * 4 + 15) / 16 * 16;
+constexpr uint32_t HT_OFF_MISC = HT_OFF_BAR + 16;
+constexpr uint32_t HT_SMEM = HT_OFF_MISC + 16;
+constexpr uint32_t HT_TMEM_COLS = 64;                             // per tile: hi*hi 16 columns, cross products 16
+
+template <int NP1>
+__global__ void __launch_bounds__(TC_THREADS)
+k_p2m_hermite_tc(const HermChunkTc *__restrict__ chunks, const double *__restrict__ grid,
+                 const double *__restrict__ box_len, const double *__restrict__ ww, const double *__restrict__ sx,
+                 const double *__restrict__ sy, const double *__restrict__ sz, const double *__restrict__ sq,
+                 double *__restrict__ Q, double *__restrict__ partial, int *err)
+{
+    constexpr int n = NP1 - 1, COLS = NP1 * NP1, P = COLS * NP1, ROWS = 4 * COLS, NT = (ROWS + TC_M - 1) / TC_M;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    float *Lb = reinterpret_cast<float *>(sm + HT_OFF_L);
+    float *nodes = reinterpret_cast<float *>(sm + HT_OFF_NODES);    // [3][8]
+    float *wx = nodes + 3 * HT_MAXNP1;                               // [3][8]: -4 w_k / len
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + HT_OFF_BAR);
+    uint32_t *misc = reinterpret_cast<uint32_t *>(sm + HT_OFF_MISC);
+    unsigned char *Bh = sm + HT_OFF_B, *Bl = Bh + B_BYTES;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const HermChunkTc ch = chunks[blockIdx.x];
+    const int node = ch.node;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(misc)),
+                     "r"(HT_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const double *g = grid + (size_t)node * 3 * NP1;
+    const double cx = 0.5 * (g[0] + g[n]), cy = 0.5 * (g[NP1] + g[NP1 + n]), cz = 0.5 * (g[2 * NP1] + g[2 * NP1 + n]);
+    if (t < 3 * NP1) {
+        const int ax = t / NP1, k = t % NP1;
+        nodes[ax * HT_MAXNP1 + k] = (float)(g[t] - (ax == 0 ? cx : ax == 1 ? cy : cz));
+        wx[ax * HT_MAXNP1 + k] = (float)(-4.0 * ww[k] / box_len[node * 3 + ax]);
+    }
+    for (uint32_t o = t * 16; o < HT_OFF_L; o += TC_THREADS * 16) *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = misc[0];
+    const int b0 = ch.begin, m = ch.count;
+    const int nch = (m + TC_KC - 1) / TC_KC;
+    double acc[NT][2 * NP1];
+#pragma unroll
+    for (int a = 0; a < NT; a++)
+#pragma unroll
+        for (int c = 0; c < 2 * NP1; c++) acc[a][c] = 0.0;
+    const uint32_t bar_a = smem_addr(bar);
+    bool ok = true;
+
+    const double *src = warp == 0 ? sx : warp == 1 ? sy : sz;
+    const double ctr = warp == 0 ? cx : warp == 1 ? cy : cz;
+    auto fetch = [&](int c, double &v, double &qv) {
+        const int i = c * TC_KC + lane;
+        v = 0.0;
+        qv = 0.0;
+        if (warp < 3 && c < nch && i < m) {
+            v = src[b0 + i];
+            if (warp == 0) qv = sq[b0 + i];
+        }
+    };
+    // value (A) and derivative (B) bases of one axis per warp, as
+    // hermite_basis (clusters.c:1289-1344) in FP32: A_k = dj/d^2 + wx_k/d,
+    // B_k = dj/d, both over sum_j A_j; exact node: A = indicator, B = 0.  The
+    // x bases carry the charge.
+    auto bases = [&](int c, double v, double qv) {
+        if (warp >= 3) return;
+        const int i = c * TC_KC + lane;
+        float A[NP1], Bv[NP1];
+        if (i < m) {
+            const float xr = (float)(v - ctr);
+            const float *nd = nodes + warp * HT_MAXNP1, *w = wx + warp * HT_MAXNP1;
+            float sum = 0.0f;
+            int ex = -1;
+#pragma unroll
+            for (int k = 0; k < NP1; k++) {
+                const float d = xr - nd[k];
+                if (fabsf(d) < FLT_MIN) ex = k;
+                const float r = rcp_nr(d), dj = (k == 0 || k == n) ? 0.25f : 1.0f;
+                Bv[k] = dj * r;
+                A[k] = r * fmaf(dj, r, w[k]);
+                sum += A[k];
+            }
+            const float qf = warp == 0 ? (float)qv : 1.0f;
+            if (ex >= 0) {
+#pragma unroll
+                for (int k = 0; k < NP1; k++) { A[k] = k == ex ? qf : 0.0f; Bv[k] = 0.0f; }
+            } else {
+                const float scale = rcp_nr(sum) * qf;
+#pragma unroll
+                for (int k = 0; k < NP1; k++) { A[k] *= scale; Bv[k] *= scale; }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < NP1; k++) A[k] = Bv[k] = 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < NP1; k++) {
+            Lb[((warp * 2 + 0) * HT_MAXNP1 + k) * LSTR + lane] = A[k];
+            Lb[((warp * 2 + 1) * HT_MAXNP1 + k) * LSTR + lane] = Bv[k];
+        }
+    };
+
+    double pv, pq;
+    fetch(0, pv, pq);
+    bases(0, pv, pq);
+    fetch(1, pv, pq);
+    __syncthreads();
+    for (int c = 0; c < nch && ok; c++) {
+        // A rows r = (pair s, k2, k3): Y_s[k2] Z_s[k3] for the chunk's particles
+#pragma unroll
+        for (int tile = 0; tile < NT; tile++) {
+            const int r = t + TC_M * tile;
+            if (r < ROWS) {
+                const int sp = r / COLS, col = r % COLS, k2 = col % NP1, k3 = col / NP1;
+                const float *ly = Lb + ((1 * 2 + (sp & 1)) * HT_MAXNP1 + k2) * LSTR;
+                const float *lz = Lb + ((2 * 2 + (sp >> 1)) * HT_MAXNP1 + k3) * LSTR;
+                unsigned char *Ah = sm + HT_OFF_A + tile * HT_A_TILE, *Al = Ah + 2 * HT_A_TILE;
+#pragma unroll
+                for (int k4 = 0; k4 < TC_KC; k4 += 4) {
+                    const float4 a = *reinterpret_cast<const float4 *>(ly + k4);
+                    const float4 b = *reinterpret_cast<const float4 *>(lz + k4);
+                    uint4 h, l;
+                    split_tf32(a.x * b.x, h.x, l.x);
+                    split_tf32(a.y * b.y, h.y, l.y);
+                    split_tf32(a.z * b.z, h.z, l.z);
+                    split_tf32(a.w * b.w, h.w, l.w);
+                    const uint32_t o = kmajor_off(TC_M, t, k4);
+                    *reinterpret_cast<uint4 *>(Ah + o) = h;
+                    *reinterpret_cast<uint4 *>(Al + o) = l;
+                }
+            }
+        }
+        {
+            // B rows (x basis X, k1): q X[k1]; thread t covers row t / 8, particles 4 (t % 8) .. +3
+            const int row = t >> 3, k4 = (t & 7) * 4;
+            if (row < 2 * NP1) {
+                const int X = row / NP1, k1 = row % NP1;
+                const float4 a = *reinterpret_cast<const float4 *>(Lb + ((0 * 2 + X) * HT_MAXNP1 + k1) * LSTR + k4);
+                uint4 h, l;
+                split_tf32(a.x, h.x, l.x);
+                split_tf32(a.y, h.y, l.y);
+                split_tf32(a.z, h.z, l.z);
+                split_tf32(a.w, h.w, l.w);
+                const uint32_t o = kmajor_off(TC_N, row, k4);
+                *reinterpret_cast<uint4 *>(Bh + o) = h;
+                *reinterpret_cast<uint4 *>(Bl + o) = l;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t bh = smem_addr(Bh), bl = smem_addr(Bl);
+#pragma unroll
+            for (int tile = 0; tile < NT; tile++) {
+                const uint32_t ah = smem_addr(sm + HT_OFF_A + tile * HT_A_TILE), al = ah + 2 * HT_A_TILE;
+                const uint32_t d = tmem + 32 * tile;
+#pragma unroll
+                for (int s = 0; s < TC_KSTEPS; s++) {
+                    const uint32_t oa = s * TC_M * 32, ob = s * TC_N * 32;
+                    mma_tf32(d, smem_desc(ah + oa), smem_desc(bh + ob), s > 0 ? 1u : 0u);
+                    mma_tf32(d + 16, smem_desc(ah + oa), smem_desc(bl + ob), s > 0 ? 1u : 0u);
+                    mma_tf32(d + 16, smem_desc(al + oa), smem_desc(bh + ob), 1u);
+                }
+            }
+            mma_commit(bar_a);
+        }
+        if (c + 1 < nch) {
+            bases(c + 1, pv, pq);
+            fetch(c + 2, pv, pq);
+        }
+        const bool done = bar_wait(bar_a, (uint32_t)(c & 1));
+        if (done) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int tile = 0; tile < NT; tile++) {
+                uint32_t r[32];
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + 32 * tile;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                      "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                      "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int k = 0; k < 2 * NP1; k++)
+                    acc[tile][k] += (double)__uint_as_float(r[k]) + (double)__uint_as_float(r[16 + k]);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        ok = !__syncthreads_or(done ? 0 : 1);
+        if (!ok && t == 0) bar_wait(bar_a, (uint32_t)(c & 1));
+    }
+    if (ok) {
+        // moment of (yz pair s, x basis X): AA -> AAA, BAA; BA -> ABA, BBA;
+        // AB -> AAB, BAB; BB -> ABB, BBB
+        constexpr int MOM[4][2] = {{0, 1}, {2, 4}, {3, 6}, {5, 7}};
+        double *dst = ch.slot < 0 ? Q + (size_t)node * 8 * P : partial + (size_t)ch.slot * 8 * P;
+#pragma unroll
+        for (int tile = 0; tile < NT; tile++) {
+            const int r = t + TC_M * tile;
+            if (r < ROWS) {
+                const int sp = r / COLS, col = r % COLS;
+#pragma unroll
+                for (int k = 0; k < 2 * NP1; k++)
+                    dst[(size_t)MOM[sp][k / NP1] * P + (k % NP1) + NP1 * col] = acc[tile][k];
+            }
+        }
+    } else if (t == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(HT_TMEM_COLS));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // L2P on the tensor cores (cp_comp_pot, src/interaction_compute/
 // interaction_compute_downpass.c:326-497): the potential of target i from its
 // leaf's grid values Phi[k1, k2, k3] is
@@ -623,6 +875,25 @@ void launch_l2p_tc(int n, int nitems, const int2 *items, const int *leaf_node, c
 #define BT_L2(N) case N: l2p_tc_t<N>(nitems, items, leaf_node, t_ibeg, t_numpar, t_grid, Phi, tx, ty, tz, pot, err, st); return;
         BT_L2(2) BT_L2(3) BT_L2(4) BT_L2(5) BT_L2(6) BT_L2(7) BT_L2(8) BT_L2(9) BT_L2(10) BT_L2(11)
 #undef BT_L2
+    }
+}
+
+bool p2m_hermite_tc_supported(int n) { return n >= 1 && n + 1 <= HT_MAXNP1; }
+
+void launch_p2m_hermite_tc(int n, int nchunks, const HermChunkTc *chunks, const double *grid, const double *box_len,
+                           const double *ww, const double *sx, const double *sy, const double *sz, const double *sq,
+                           double *Q, double *partial, int *err, cudaStream_t st)
+{
+    if (nchunks <= 0) return;
+    switch (n + 1) {
+#define BT_HT(N)                                                                                                       \
+    case N:                                                                                                            \
+        cudaFuncSetAttribute(k_p2m_hermite_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HT_SMEM);         \
+        k_p2m_hermite_tc<N><<<nchunks, TC_THREADS, HT_SMEM, st>>>(chunks, grid, box_len, ww, sx, sy, sz, sq, Q, partial, \
+                                                                  err);                                               \
+        return;
+        BT_HT(2) BT_HT(3) BT_HT(4) BT_HT(5) BT_HT(6) BT_HT(7) BT_HT(8)
+#undef BT_HT
     }
 }
 

@@ -5,6 +5,12 @@
 
 namespace bt {
 
+// A chunk of a node's particles for the Hermite P2M (the same as HermChunk of
+// bt_device.h): slot < 0 writes the node's moments, else partial slot `slot`.
+struct HermChunkTc {
+    int node, begin, count, slot;
+};
+
 // Leaf P2M (Lagrange) on the tensor cores in 3xTF32 with FP32 accumulation,
 // for degrees with (n+1)^2 <= 128.  Same output layout as launch_p2m
 // (Q[node * P + k1 + (n+1) (k2 + (n+1) k3)], FP64).  *err is set to 1 if a
@@ -21,5 +27,13 @@ void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const
 void launch_l2p_tc(int n, int nitems, const int2 *items, const int *leaf_node, const int *t_ibeg,
                    const int *t_numpar, const double *t_grid, const double *Phi, const double *tx, const double *ty,
                    const double *tz, double *pot, int *err, cudaStream_t st);
+
+// Hermite P2M on the tensor cores for degrees with n + 1 <= 8: the 8
+// moments of every chunk's node (or its partial slot), as launch_p2m_hermite
+// writes them before its reduction; *err as for launch_p2m_tc.
+bool p2m_hermite_tc_supported(int n);
+void launch_p2m_hermite_tc(int n, int nchunks, const HermChunkTc *chunks, const double *grid, const double *box_len,
+                           const double *ww, const double *sx, const double *sy, const double *sz, const double *sq,
+                           double *Q, double *partial, int *err, cudaStream_t st);
 
 }  // namespace bt

@@ -90,3 +90,28 @@ def test_expired_tensor_core_wait_is_reported_and_the_context_survives(monkeypat
     assert e.value.code == B.BT_ERR_TIMEOUT and "tensor-core wait expired" in B.last_error()
     monkeypatch.delenv("BARYTREE_B200_TEST_EXPIRE_TC_WAIT")
     assert np.array_equal(B.treecode(tx, ty, tz, sx, sy, sz, sq, **kw), good)
+
+
+@pytest.mark.parametrize("degree,leaf,clustered", [(6, 1000, True), (4, 300, False), (7, 2500, True), (2, 200, False)])
+def test_tensor_core_hermite_p2m_against_fp64(degree, leaf, clustered):
+    """Hermite particle-cluster in mixed precision: the 8 moments per node on
+    the tensor cores (degrees with n + 1 <= 8; leaves above 2048 particles
+    exercise the chunked nodes and their reduction) against the FP64 Hermite
+    P2M (BT_UPWARD_FP64), and both against the direct sum."""
+    rng = np.random.default_rng(40 + degree)
+    n = 120000
+    if clustered:
+        x, y, z = (np.clip(rng.normal(0, 0.25, n), -1, 1) for _ in range(3))
+    else:
+        x, y, z = (rng.uniform(-1, 1, n) for _ in range(3))
+    q = rng.choice([-1.0, 1.0], n)
+    kw = dict(approximation=B.Approximation.HERMITE, theta=0.7, degree=degree, max_source_leaf=leaf,
+              max_target_leaf=leaf, size_check=4.0, precision=B.PRECISION_MIXED)
+    tc, rep = B.treecode(x, y, z, x, y, z, q, return_report=True, **kw)
+    f64 = B.treecode(x, y, z, x, y, z, q, upward=B.UPWARD_FP64, **kw)
+    assert rep["pc_ptwise"] > 0
+    assert not np.array_equal(tc, f64)
+    assert _rel(tc, f64) < 5e-7
+    idx = np.arange(0, n, 60)
+    exact = B.direct(x[idx], y[idx], z[idx], x, y, z, q)
+    assert _rel(tc[idx], exact) <= 1.05 * _rel(f64[idx], exact) + 3e-7
