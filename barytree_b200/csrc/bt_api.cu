@@ -651,6 +651,7 @@ struct DevPlan {
     bool mixed = false, herm = false, need_src_clusters = false, need_tgt_grids = false;
     bool queue = false;     // mixed kernels on a device work queue
     int tpt = 2, tile = 1024;   // tile shape of the mixed particle-output kernel
+    int fp64_tb = 1;            // targets per thread of the FP64 particle-output kernel
     bool tc_up = false;         // leaf P2M on the tensor cores (bt_tc.cu)
     bool sharded = false;       // this call evaluates a share of the target leaves (others get 0)
     // symmetric near-field pairs (bt_sym.cu)
@@ -988,7 +989,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
         a.t_ibeg = d_tibeg; a.t_numpar = d_tnum; a.a_off = d_aoff; a.a_idx = d_aidx; a.d_off = d_doff; a.d_idx = d_didx;
         a.s_ibeg = d_sibeg; a.s_numpar = d_snum; a.s_grid = d_sgrid; a.Q = d_Q;
         a.sx = d_sx; a.sy = d_sy; a.sz = d_sz; a.sq = d_sq; a.tx = d_tx; a.ty = d_ty; a.tz = d_tz;
-        a.kp = v.kp; a.kp2 = v.kp2; a.pot = d_pot;
+        a.kp = v.kp; a.kp2 = v.kp2; a.pot = d_pot; a.tb = v.fp64_tb;
         bt::launch_eval_targets(v.kernel, herm, a, st);
         launches++;
     }
@@ -1105,7 +1106,11 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
 #pragma omp parallel for schedule(static)
         for (int64_t k = 0; k < n_approx; k++) {
             const int sl = slot[pl.a_deg[k]];
-            if (sl >= 0) __atomic_store_n(&need[(size_t)pl.t_approx.idx[k] * X + sl], (unsigned char)1, __ATOMIC_RELAXED);
+            if (sl < 0) continue;
+            // most entries find their node marked already: read first, so
+            // the threads do not keep pulling the same cache lines for writes
+            unsigned char *f = &need[(size_t)pl.t_approx.idx[k] * X + sl];
+            if (!__atomic_load_n(f, __ATOMIC_RELAXED)) __atomic_store_n(f, (unsigned char)1, __ATOMIC_RELAXED);
         }
         for (int v = 0; v < S.n; v++)
             for (int c = 0; c < S.nchild[v]; c++) {
@@ -1200,9 +1205,12 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
                     for (int v = T.leaves[u]; v >= 0 && !tnode_need[v]; v = T.parent[v]) tnode_need[v] = 1;
         }
     }
+    // FP64 particle-output kernel: two targets per thread where the items fill the GPU
+    const int fp64_tb = (!mixed && !ssm) ? bt::fp64_targets_per_thread(T.nleaves, leaf_count.data()) : 1;
     std::vector<int2> ev_items =
         make_items(T.nleaves, leaf_count.data(),
-                   mixed ? bt::mixed_targets_chunk() : ssm ? bt::ss_chunk() : bt::fp64_targets_chunk(), leaf_cost);
+                   mixed ? bt::mixed_targets_chunk() : ssm ? bt::ss_chunk() : bt::fp64_targets_chunk(fp64_tb),
+                   leaf_cost);
     std::vector<int2> grid_items, l2p_items;
     if (need_tgt_grids) {
         std::vector<int> pcount(T.n, P);
@@ -1614,6 +1622,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.tile = shape.tile;
         v.tc_up = shape.tc_up && mixed;
         v.sharded = shape.nshards > 1;
+        v.fp64_tb = fp64_tb;
         v.sym_npairs = (int)sym_pairs.size();
         v.sym_far_pairs = (int)sym_far_pairs;
         v.d_sbox = d_sbox;

@@ -530,17 +530,17 @@ void launch_hermite_reduce(int n, int nred, const int3 *red, const double *parti
 
 // ---------------------------------------------------------------------------
 // Particle-output evaluation: PC (clusters) + PP (particles) per target leaf.
-// One CTA per work item (target leaf, chunk of EV_TB * EV_THREADS targets),
-// EV_TB targets per thread (ti and ti + EV_THREADS, ...) so that every grid
-// point or source read from shared memory serves EV_TB evaluations; FP64
-// accumulation in registers in each target's own order (the same order as
-// one target per thread); exactly one writer per target.
+// One CTA per work item (target leaf, chunk of TB * EV_THREADS targets), TB
+// targets per thread (ti and ti + EV_THREADS, ...) so that every grid point
+// or source read from shared memory serves TB evaluations; FP64 accumulation
+// in registers in each target's own order (the same order for any TB);
+// exactly one writer per target.  TB = 2 where the work items fill the GPU
+// several times over, else 1 (fp64_targets_per_thread).
 // ---------------------------------------------------------------------------
 constexpr int EV_THREADS = 128;
-constexpr int EV_TB = 2;
 constexpr int PP_TILE = 512;
 
-template <int KT, bool HERM>
+template <int KT, bool HERM, int EV_TB>
 __global__ void __launch_bounds__(EV_THREADS)
 k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ leaf_node,
                const int *__restrict__ t_ibeg, const int *__restrict__ t_numpar,
@@ -646,7 +646,17 @@ k_eval_targets(int n, const int2 *__restrict__ items, const int *__restrict__ le
         if (active[b]) pot[t[b]] = acc[b];
 }
 
-int fp64_targets_chunk() { return EV_TB * EV_THREADS; }
+int fp64_targets_chunk(int tb) { return tb * EV_THREADS; }
+
+int fp64_targets_per_thread(int nunits, const int *count)
+{
+    // work items of two targets per thread; under about four waves of
+    // resident blocks (16 blocks of 128 threads on each of ~148 SMs) one
+    // target per thread keeps twice as many blocks in flight
+    long long items = 0;
+    for (int u = 0; u < nunits; u++) items += (count[u] + 2 * EV_THREADS - 1) / (2 * EV_THREADS);
+    return items >= 4LL * 16 * 148 ? 2 : 1;
+}
 
 // ---------------------------------------------------------------------------
 // Grid-output evaluation: M2L (source clusters, CC) + CP (source particles)
@@ -1011,7 +1021,7 @@ static void eval_targets_t(const EvalTargetsArgs &a, cudaStream_t st)
     size_t far = sizeof(double) * (size_t)(3 * np1 + (HERM ? 8 * P : P));
     size_t near = sizeof(double4) * PP_TILE;
     size_t sm = far > near ? far : near;
-    auto fn = k_eval_targets<KT, HERM>;
+    auto fn = a.tb == 2 ? k_eval_targets<KT, HERM, 2> : k_eval_targets<KT, HERM, 1>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     fn<<<a.nitems, EV_THREADS, sm, st>>>(a.n, a.items, a.leaf_node, a.t_ibeg, a.t_numpar, a.a_off, a.a_idx,
                                          a.d_off, a.d_idx, a.s_ibeg, a.s_numpar, a.s_grid, a.Q, a.sx, a.sy,

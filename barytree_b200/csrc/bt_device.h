@@ -21,6 +21,7 @@ struct EvalTargetsArgs {
     const double *tx, *ty, *tz;
     double kp, kp2;                             // kernel_params[0], [1]
     double *pot;
+    int tb = 1;                                 // targets per thread (1 or 2): items of tb * 128 targets
 };
 
 struct EvalGridsArgs {
@@ -58,7 +59,10 @@ void launch_m2m(int n, int nparents, const int *parents, const int *nchild, cons
 void launch_l2l(int n, int nparents, const int *parents, const int *nchild, const int *child, const double *grid,
                 double *Phi, cudaStream_t st);
 void launch_eval_targets(int kernel, bool hermite, const EvalTargetsArgs &a, cudaStream_t st);
-int fp64_targets_chunk();                    // targets per work item of launch_eval_targets
+// Targets per work item of launch_eval_targets with tb targets per thread, and
+// the tb to use for target leaves with count[u] targets.
+int fp64_targets_chunk(int tb);
+int fp64_targets_per_thread(int nunits, const int *count);
 void launch_eval_grids(int kernel, bool hermite, const EvalGridsArgs &a, cudaStream_t st);
 void launch_l2p(int n, bool hermite, int nitems, const int2 *items, const int *leaf_node, const int *parent,
                 const int *t_ibeg, const int *t_numpar, const double *t_grid, const double *box_len,
