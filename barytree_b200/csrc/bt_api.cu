@@ -652,6 +652,8 @@ struct DevPlan {
     bool queue = false;     // mixed kernels on a device work queue
     int tpt = 2, tile = 1024;   // tile shape of the mixed particle-output kernel
     int fp64_tb = 1;            // targets per thread of the FP64 particle-output kernel
+    bool base_full = true;      // proxies at the base degree for every node (else only the selected
+                                // degrees' marked subtrees, the base degree among them)
     bool tc_up = false;         // leaf P2M on the tensor cores (bt_tc.cu)
     bool sharded = false;       // this call evaluates a share of the target leaves (others get 0)
     // symmetric near-field pairs (bt_sym.cu)
@@ -829,39 +831,43 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
             }
         }
     } else if (need_src_clusters && ns > 0) {
-        static_assert(sizeof(bt::HermChunkTc) == sizeof(bt::HermChunk), "the two chunk types share one array");
-        if (herm && v.tc_up && bt::p2m_hermite_tc_supported(n)) {
-            // mixed Hermite: the 8 moments per chunk on the tensor cores, then
-            // the same reduction of the nodes with several chunks
-            bt::launch_p2m_hermite_tc(n, v.n_hchunks, reinterpret_cast<const bt::HermChunkTc *>(v.d_hchunks), d_sgrid,
-                                      d_slen, d_ww, d_sx, d_sy, d_sz, d_sq, d_Q, v.d_hpartial, v.d_err, st);
-            bt::launch_hermite_reduce(n, v.n_hred, v.d_hred, v.d_hpartial, d_Q, st);
-            launches += v.n_hred > 0 ? 2 : 1;
-        } else if (herm) {
-            bt::launch_p2m_hermite(n, v.n_hchunks, v.d_hchunks, v.n_hred, v.d_hred, d_sgrid, d_slen, d_ww, d_sx, d_sy,
-                                   d_sz, d_sq, d_Q, v.d_hpartial, st);
-            launches += v.n_hred > 0 ? 2 : 1;
-        } else if (v.tc_up && bt::p2m_tc_supported(n)) {
-            bt::launch_p2m_tc(n, v.S_nleaves, d_sleaves, d_sibeg, d_snum, d_sgrid, d_sx, d_sy, d_sz, d_sq, d_Q, v.d_err,
-                              st);
-            launches++;
-        } else {
-            bt::launch_p2m(n, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
-                           d_sz, d_sq, d_Q, st);
-            launches++;
-        }
-        if (!herm) {
-            for (int l = v.S_max_depth - 1; l >= 0; l--) {
-                int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
-                if (cnt > 0) {
-                    bt::launch_m2m(n, cnt, d_slvl + v.S_lvl_off[l], d_snch, d_sch, d_sgrid, d_Q, st);
-                    launches++;
+        // the base degree at every node, unless a learned selection lists it
+        // among its degrees (computed below under the nodes that use it)
+        if (v.base_full) {
+            static_assert(sizeof(bt::HermChunkTc) == sizeof(bt::HermChunk), "the two chunk types share one array");
+            if (herm && v.tc_up && bt::p2m_hermite_tc_supported(n)) {
+                // mixed Hermite: the 8 moments per chunk on the tensor cores, then
+                // the same reduction of the nodes with several chunks
+                bt::launch_p2m_hermite_tc(n, v.n_hchunks, reinterpret_cast<const bt::HermChunkTc *>(v.d_hchunks), d_sgrid,
+                                          d_slen, d_ww, d_sx, d_sy, d_sz, d_sq, d_Q, v.d_hpartial, v.d_err, st);
+                bt::launch_hermite_reduce(n, v.n_hred, v.d_hred, v.d_hpartial, d_Q, st);
+                launches += v.n_hred > 0 ? 2 : 1;
+            } else if (herm) {
+                bt::launch_p2m_hermite(n, v.n_hchunks, v.d_hchunks, v.n_hred, v.d_hred, d_sgrid, d_slen, d_ww, d_sx, d_sy,
+                                       d_sz, d_sq, d_Q, v.d_hpartial, st);
+                launches += v.n_hred > 0 ? 2 : 1;
+            } else if (v.tc_up && bt::p2m_tc_supported(n)) {
+                bt::launch_p2m_tc(n, v.S_nleaves, d_sleaves, d_sibeg, d_snum, d_sgrid, d_sx, d_sy, d_sz, d_sq, d_Q, v.d_err,
+                                  st);
+                launches++;
+            } else {
+                bt::launch_p2m(n, false, v.S_nleaves, d_sleaves, v.S_n, d_sibeg, d_snum, d_sgrid, d_slen, d_ww, d_sx, d_sy,
+                               d_sz, d_sq, d_Q, st);
+                launches++;
+            }
+            if (!herm) {
+                for (int l = v.S_max_depth - 1; l >= 0; l--) {
+                    int cnt = v.S_lvl_off[l + 1] - v.S_lvl_off[l];
+                    if (cnt > 0) {
+                        bt::launch_m2m(n, cnt, d_slvl + v.S_lvl_off[l], d_snch, d_sch, d_sgrid, d_Q, st);
+                        launches++;
+                    }
                 }
             }
-        }
-        if (mixed) {
-            bt::launch_to_f32((size_t)v.S_n * P * (herm ? 8 : 1), d_Q, d_Q32, st);
-            launches++;
+            if (mixed) {
+                bt::launch_to_f32((size_t)v.S_n * P * (herm ? 8 : 1), d_Q, d_Q32, st);
+                launches++;
+            }
         }
         // proxy charges at the other degrees chosen per interaction
         for (size_t i = 0; i < xdeg.size(); i++) {
@@ -1085,8 +1091,10 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
 #pragma omp critical
             for (int d = 0; d <= BT_MAX_DEGREE; d++) used[d] = used[d] || u[d];
         }
+        // the base degree is one of them: a selection uses it only where it
+        // chose it, so its proxies too are computed only under those nodes
         for (int d = 1; d <= BT_MAX_DEGREE; d++)
-            if (used[d] && d != n) xdeg.push_back(d);
+            if (used[d]) xdeg.push_back(d);
         xgrid.resize(xdeg.size());
         hvec<double> tmp;
         for (size_t i = 0; i < xdeg.size(); i++) fill_grids(S, xdeg[i], xgrid[i], tmp);
@@ -1623,6 +1631,7 @@ int run_plan(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double *out, bool out_on
         v.tc_up = shape.tc_up && mixed;
         v.sharded = shape.nshards > 1;
         v.fp64_tb = fp64_tb;
+        v.base_full = pl.a_deg == nullptr;
         v.sym_npairs = (int)sym_pairs.size();
         v.sym_far_pairs = (int)sym_far_pairs;
         v.d_sbox = d_sbox;
