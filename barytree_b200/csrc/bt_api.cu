@@ -1761,7 +1761,19 @@ done:
 // ---------------------------------------------------------------------------
 std::vector<float> g_selector;      // installed MLP weights (bt_selector_set), process-wide
 std::mutex g_selector_mu;
-constexpr double SELECT_MARGIN_DECADES = 0.5;   // predicted error must sit this far below the budget
+// The selection's error share: every interaction (target, cluster entry) of
+// a system may contribute SELECT_SHARE * tol * sqrt(sum_t phi_t^2 / sum_t N_t)
+// in absolute terms, phi_t^2 estimated per target leaf at one sampled
+// target, N_t its cluster entries (bt::launch_select_share), so that the
+// system's relative L2 error stays below the tolerance; calibrated across
+// eight workloads.  BARYTREE_B200_SELECT_SHARE overrides it (calibration).
+constexpr double SELECT_SHARE = 0.35;
+
+double select_share()
+{
+    const char *e = getenv("BARYTREE_B200_SELECT_SHARE");
+    return e ? atof(e) : SELECT_SHARE;
+}
 
 void node_geometry(const bt_tree &t, std::vector<double> &ctr, std::vector<double> &rad)
 {
@@ -1774,8 +1786,8 @@ void node_geometry(const bt_tree &t, std::vector<double> &ctr, std::vector<doubl
 }
 
 // Predict the error of every particle-cluster entry at every degree, choose
-// the lowest degree under the budget (or direct evaluation), and rewrite the
-// plan's target-leaf lists accordingly.
+// the lowest degree under the system's error share (or direct evaluation),
+// and rewrite the plan's target-leaf lists accordingly.
 int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const DevParts *dp = nullptr)
 {
     std::vector<float> w;
@@ -1813,6 +1825,25 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
         L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size());
         L.add(&d_pred, (size_t)ne * bt::MLP_OUT); L.add(&d_choice, ne);
+        // the error share: near-field lists, the target leaves' first
+        // particles, per-unit sums, one share per system; the particles in
+        // tree order (on the device already after a GPU tree build)
+        const double share_c = select_share();
+        const int64_t nd = pl.t_direct.off[pl.t_direct.rows];
+        const int nsys = T.nroots;
+        int64_t *d_doff;
+        int *d_didx, *d_tibeg, *d_sysoff;
+        double *d_usum;
+        float *d_share;
+        L.add(&d_doff, pl.t_direct.rows + 1); L.add(&d_didx, nd > 0 ? nd : 1); L.add(&d_tibeg, T.n);
+        L.add(&d_usum, 2 * (size_t)pl.t_approx.rows); L.add(&d_share, nsys); L.add(&d_sysoff, nsys + 1);
+        const double *px = dp ? dp->sx : nullptr, *py = dp ? dp->sy : nullptr, *pz = dp ? dp->sz : nullptr;
+        const double *ptx = dp ? dp->tx : nullptr, *pty = dp ? dp->ty : nullptr, *ptz = dp ? dp->tz : nullptr;
+        double *hx = nullptr, *hy = nullptr, *hz = nullptr, *htx = nullptr, *hty = nullptr, *htz = nullptr;
+        if (!dp) {
+            L.add(&hx, pl.src.n); L.add(&hy, pl.src.n); L.add(&hz, pl.src.n);
+            L.add(&htx, pl.tgt.n); L.add(&hty, pl.tgt.n); L.add(&htz, pl.tgt.n);
+        }
         if (!arena.reserve(L.total())) {
             set_err(arena.fixed ? "degree selection needs more scratch than the static array holds"
                                 : "device allocation failed");
@@ -1840,8 +1871,22 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             launches++;
             bt::mlp_infer(d_w, ne, d_feat, d_pred, st);
             launches++;
-            bt::launch_select(ne, d_pred, d_feat, (float)(log10(tol) - SELECT_MARGIN_DECADES), d_choice, st);
-            launches++;
+            CK(cudaMemcpyAsync(d_doff, pl.t_direct.off, sizeof(int64_t) * (pl.t_direct.rows + 1),
+                               cudaMemcpyHostToDevice, st));
+            if (nd > 0) CK(cudaMemcpyAsync(d_didx, pl.t_direct.idx, sizeof(int) * nd, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_tibeg, T.ibeg, sizeof(int) * T.n, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_sysoff, T.leaf_off, sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice, st));
+            if (!dp) {
+                const double *src[6] = {pl.src.x, pl.src.y, pl.src.z, pl.tgt.x, pl.tgt.y, pl.tgt.z};
+                double *dst[6] = {hx, hy, hz, htx, hty, htz};
+                for (int k = 0; k < 6; k++)
+                    CK(cudaMemcpyAsync(dst[k], src[k], sizeof(double) * (k < 3 ? pl.src.n : pl.tgt.n),
+                                       cudaMemcpyHostToDevice, st));
+                px = hx; py = hy; pz = hz; ptx = htx; pty = hty; ptz = htz;
+            }
+            bt::launch_select_share(fa, nsys, d_sysoff, d_tibeg, d_doff, d_didx, d_sibeg, px, py, pz, d_sq, ptx, pty,
+                                    ptz, share_c * tol, ne, d_pred, d_feat, d_usum, d_share, d_choice, st);
+            launches += 3;
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(choice.data(), d_choice, ne, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));

@@ -324,25 +324,6 @@ __global__ void k_gather_rows(int B, int width, const int *__restrict__ rows, co
     dst[idx] = src[(size_t)rows[b] * width + k];
 }
 
-// choice per interaction from predicted log10 errors: lowest degree under the
-// budget; direct evaluation (255) when no degree qualifies or when direct is
-// cheaper than the chosen degree.
-__global__ void k_select(int64_t n, const float *__restrict__ pred, const float *__restrict__ feat, float log_budget,
-                         unsigned char *__restrict__ choice)
-{
-    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    unsigned char c = MLP_PP;
-    for (int d = MLP_DMIN; d <= MLP_DMAX; d++) {
-        if (pred[e * MLP_OUT + (d - MLP_DMIN)] <= log_budget) { c = (unsigned char)d; break; }
-    }
-    float ns = exp10f(feat[e * MLP_IN + 0]);
-    if (c != MLP_PP) {
-        float P = (float)((c + 1) * (c + 1) * (c + 1));
-        if (P >= ns) c = MLP_PP;
-    }
-    choice[e] = c;
-}
 
 // ---------------------------------------------------------------------------
 // host-side drivers of the layer kernels
@@ -453,10 +434,149 @@ void launch_labels(const LabelArgs &a, int nsamples, cudaStream_t st)
     if (nsamples > 0) k_labels<<<nsamples, LBL_TARGETS, 0, st>>>(a);
 }
 
-void launch_select(int64_t n, const float *pred, const float *feat, float log_budget, unsigned char *choice,
-                   cudaStream_t st)
+// Degree selection under one absolute error share per system.  The network
+// predicts e_d, log10 of an interaction's error at degree d over its scale
+// |q_C|_2 / d.  Errors of different interactions add at a target roughly as
+// independent terms, so if every (target, cluster entry) pair of a system
+// contributes at most
+//   share = c tol sqrt(sum_t phi_t^2 / sum_t N_t)
+// (N_t the target's cluster entries, phi_t its potential), the system's
+// relative L2 error is about c tol.  phi_t^2 is estimated per target leaf
+// at two sampled targets: the near-field sum sum_j q_j^2 / r_j^2 over the
+// leaf's near-field leaves (r floored at each leaf's mean particle spacing)
+// plus, per cluster entry, (|q_C|_2 / d)^2 -- the mean square potential of
+// charges of either sign.  Each interaction then takes the lowest degree d with
+// e_d + log10(|q_C|_2 / d) <= log10(share), or direct evaluation when no
+// degree qualifies or direct is cheaper.
+__global__ void k_unit_phi2_sampled(FeatureArgs a, const int *__restrict__ t_ibeg, const int64_t *__restrict__ d_off,
+                                    const int *__restrict__ d_idx, const int *__restrict__ s_ibeg,
+                                    const double *__restrict__ sx, const double *__restrict__ sy,
+                                    const double *__restrict__ sz, const double *__restrict__ sq,
+                                    const double *__restrict__ tx, const double *__restrict__ ty,
+                                    const double *__restrict__ tz, double *__restrict__ unit_sums)
 {
-    if (n > 0) k_select<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, pred, feat, log_budget, choice);
+    constexpr int NS = 2;                  // sampled targets per leaf: a quarter and three quarters in
+    const int u = blockIdx.x;
+    const int tn = a.unit_node[u], nt = a.t_numpar[tn];
+    double px[NS], py[NS], pz[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+        const int t = t_ibeg[tn] + (int)(((2 * k + 1) * (int64_t)nt) / (2 * NS));
+        px[k] = tx[t]; py[k] = ty[t]; pz[k] = tz[t];
+    }
+    double phi2 = 0.0;
+    for (int64_t e = a.off[u] + threadIdx.x; e < a.off[u + 1]; e += blockDim.x) {
+        const int s = a.idx[e];
+        const double q2 = a.s_mom[2 * s + 1];
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            const double dx = px[k] - a.s_ctr[3 * s], dy = py[k] - a.s_ctr[3 * s + 1], dz = pz[k] - a.s_ctr[3 * s + 2];
+            phi2 += q2 * q2 / (dx * dx + dy * dy + dz * dz);
+        }
+    }
+    // near field: each particle's q^2 / r^2 with r no smaller than the leaf's
+    // mean particle spacing (radius / count^(1/3)), which keeps a chance
+    // close neighbour from dominating the estimate; FP32 (an estimate)
+    float near = 0.0f;
+    for (int64_t e = d_off[u]; e < d_off[u + 1]; e++) {
+        const int s = d_idx[e], b = s_ibeg[s], m = a.s_numpar[s];
+        const float h = (float)(a.s_rad[s] / cbrt((double)m));
+        const float h2 = fmaxf(h * h, FLT_MIN);
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            const float q = (float)sq[b + j];
+#pragma unroll
+            for (int k = 0; k < NS; k++) {
+                const float dx = (float)(px[k] - sx[b + j]), dy = (float)(py[k] - sy[b + j]),
+                            dz = (float)(pz[k] - sz[b + j]);
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                if (r2 > 0.0f) near += q * q / fmaxf(r2, h2);
+            }
+        }
+    }
+    phi2 += (double)near;
+    __shared__ double red[128];
+    red[threadIdx.x] = phi2;
+    __syncthreads();
+    for (int h = 64; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        unit_sums[2 * u] = nt * red[0] / NS;
+        unit_sums[2 * u + 1] = (double)nt * (double)(a.off[u + 1] - a.off[u]);
+    }
 }
+
+// One block per system: its share from the sums over its units (leaves
+// sys_off[k] .. sys_off[k+1]), added in a fixed order (deterministic).
+__global__ void k_system_share(const int *__restrict__ sys_off, const double *__restrict__ unit_sums, double c_tol,
+                               float *__restrict__ log_share)
+{
+    __shared__ double sp[256], sn[256];
+    const int k = blockIdx.x;
+    double p = 0.0, n = 0.0;
+    for (int u = sys_off[k] + threadIdx.x; u < sys_off[k + 1]; u += blockDim.x) {
+        p += unit_sums[2 * u];
+        n += unit_sums[2 * u + 1];
+    }
+    sp[threadIdx.x] = p;
+    sn[threadIdx.x] = n;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) { sp[threadIdx.x] += sp[threadIdx.x + s]; sn[threadIdx.x] += sn[threadIdx.x + s]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double share = sn[0] > 0.0 ? c_tol * sqrt(sp[0] / sn[0]) : 0.0;
+        log_share[k] = share > 0.0 ? (float)log10(share) : -1.0e30f;
+    }
+}
+
+__global__ void k_select_share(FeatureArgs a, int nsys, const int *__restrict__ sys_off, int64_t n,
+                               const float *__restrict__ pred, const float *__restrict__ feat,
+                               const float *__restrict__ log_share, unsigned char *__restrict__ choice)
+{
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    int lo = 0, hi = a.units;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (a.off[mid] <= e) lo = mid; else hi = mid;
+    }
+    int k0 = 0, k1 = nsys;                 // the unit's system
+    while (k1 - k0 > 1) {
+        const int mid = (k0 + k1) >> 1;
+        if (sys_off[mid] <= lo) k0 = mid; else k1 = mid;
+    }
+    const int tn = a.unit_node[lo], s = a.idx[e];
+    const double dx = a.t_ctr[3 * tn] - a.s_ctr[3 * s], dy = a.t_ctr[3 * tn + 1] - a.s_ctr[3 * s + 1],
+                 dz = a.t_ctr[3 * tn + 2] - a.s_ctr[3 * s + 2];
+    const double scale = a.s_mom[2 * s + 1] / sqrt(dx * dx + dy * dy + dz * dz);
+    const float budget = scale > 0.0 ? log_share[k0] - (float)log10(scale) : 1.0e30f;
+    unsigned char c = MLP_PP;
+    for (int d = MLP_DMIN; d <= MLP_DMAX; d++) {
+        if (pred[e * MLP_OUT + (d - MLP_DMIN)] <= budget) { c = (unsigned char)d; break; }
+    }
+    const float ns = exp10f(feat[e * MLP_IN + 0]);
+    if (c != MLP_PP) {
+        const float P = (float)((c + 1) * (c + 1) * (c + 1));
+        if (P >= ns) c = MLP_PP;
+    }
+    choice[e] = c;
+}
+
+void launch_select_share(const FeatureArgs &a, int nsys, const int *sys_off, const int *t_ibeg, const int64_t *d_off,
+                         const int *d_idx, const int *s_ibeg, const double *sx, const double *sy, const double *sz,
+                         const double *sq, const double *tx, const double *ty, const double *tz, double c_tol,
+                         int64_t n, const float *pred, const float *feat, double *unit_sums, float *log_share,
+                         unsigned char *choice, cudaStream_t st)
+{
+    if (n <= 0 || a.units <= 0 || nsys <= 0) return;
+    k_unit_phi2_sampled<<<a.units, 128, 0, st>>>(a, t_ibeg, d_off, d_idx, s_ibeg, sx, sy, sz, sq, tx, ty, tz,
+                                                  unit_sums);
+    k_system_share<<<nsys, 256, 0, st>>>(sys_off, unit_sums, c_tol, log_share);
+    k_select_share<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, nsys, sys_off, n, pred, feat, log_share, choice);
+}
+
 
 }  // namespace bt

@@ -60,7 +60,13 @@ void launch_features(const FeatureArgs &a, int64_t nentries, float *out, cudaStr
 void launch_features_pairs(const FeatureArgs &a, int n, const int *tnodes, const int *snodes, float *out,
                            cudaStream_t st);
 void launch_labels(const LabelArgs &a, int nsamples, cudaStream_t st);
-void launch_select(int64_t n, const float *pred, const float *feat, float log_budget, unsigned char *choice,
-                   cudaStream_t st);
+// Selection under one absolute error share per system (bt_learned.cu):
+// sys_off = nsys + 1 offsets of each system's units (target leaves);
+// unit_sums: 2 * units doubles, log_share: nsys floats of scratch.
+void launch_select_share(const FeatureArgs &a, int nsys, const int *sys_off, const int *t_ibeg, const int64_t *d_off,
+                         const int *d_idx, const int *s_ibeg, const double *sx, const double *sy, const double *sz,
+                         const double *sq, const double *tx, const double *ty, const double *tz, double c_tol,
+                         int64_t n, const float *pred, const float *feat, double *unit_sums, float *log_share,
+                         unsigned char *choice, cudaStream_t st);
 
 }  // namespace bt

@@ -73,3 +73,29 @@ def test_batch_rejects_bad_offsets():
     x = np.zeros(4)
     with pytest.raises(B.BaryTreeError):
         B.treecode_batch_ptr(2, np.array([0, 3, 2]), np.array([0, 2, 4]), *(x.ctypes.data,) * 8)
+
+
+def test_learned_batch_equals_separate_calls_and_host_tree():
+    """The learned selection's error share is computed per system, so a
+    batch of systems selects the same degrees as separate calls (bit for bit),
+    each system keeps its own accuracy, and the host-built trees give the
+    same selection as the GPU-built ones."""
+    from barytree_b200 import selector
+    selector.install_default()
+    systems = []
+    for k, n in enumerate((150_000, 60_000, 220_000)):
+        x, y, z, q = selector.blobs(n, 300 + k)
+        if k == 1:
+            q = q * 1e-3                         # a system with a much smaller potential scale
+        systems.append((x, y, z, x.copy(), y.copy(), z.copy(), q))
+    kw = dict(kernel=1, degree=10, theta=0.7, max_source_leaf=2000, max_target_leaf=2000,
+              precision=B.PRECISION_MIXED, degree_policy=B.DEGREE_LEARNED, tolerance=1e-6)
+    pots = B.treecode_batch(systems, **kw)
+    host = B.treecode_batch(systems, tree_build=B.TREE_HOST, **kw)
+    for s, p, h in zip(systems, pots, host):
+        ref = B.treecode(*s, **kw)
+        assert np.array_equal(p, ref)
+        assert np.array_equal(p, h)
+        idx = np.arange(0, len(s[0]), 37)
+        d = B.direct(s[0][idx], s[1][idx], s[2][idx], s[3], s[4], s[5], s[6])
+        assert np.linalg.norm(p[idx] - d) / np.linalg.norm(d) <= 1e-6
