@@ -1012,7 +1012,7 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
                 }
             }
         }
-        if (v.tc_up && !herm && !v.ss && bt::p2m_tc_supported(n))
+        if (v.tc_up && !herm && !v.ss && bt::l2p_tc_supported(n))
             // mixed Lagrange: the leaf interpolation as a GEMM on the tensor cores
             bt::launch_l2p_tc(n, v.n_l2p_items, d_l2pitems, d_tleaves, d_tibeg, d_tnum, d_tgrid, d_Phi, d_tx, d_ty,
                               d_tz, d_pot, v.d_err, st);

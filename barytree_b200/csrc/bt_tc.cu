@@ -46,8 +46,7 @@ constexpr int TC_M = 128;                  // MMA rows: (k2, k3) pairs, padded
 constexpr int TC_N = 16;                   // MMA columns: k1, padded
 constexpr int TC_KC = 32;                  // particles per chunk
 constexpr int TC_KSTEPS = TC_KC / 8;       // one tcgen05.mma (kind::tf32) covers K = 8
-constexpr int TC_MAXNP1 = 11;              // (n+1)^2 <= 128
-constexpr uint32_t TC_TMEM_COLS = 32;      // accumulators: hi*hi in columns 0-15, cross products in 16-31
+constexpr int TC_MAXNP1 = 16;              // (n+1)^2 <= 256: one or two 128-row tiles
 constexpr long long TC_WAIT_LIMIT = 1LL << 22;
 constexpr long long TC_TEST_WAIT_LIMIT = 1LL << 10;   // the failure-path test's wait
 
@@ -55,15 +54,24 @@ constexpr long long TC_TEST_WAIT_LIMIT = 1LL << 10;   // the failure-path test's
 // bases: float [axis][k][particle], rows padded to LSTR floats (16-byte rows
 // whose bank groups differ for consecutive k).
 constexpr int LSTR = 36;
-constexpr uint32_t A_BYTES = TC_M * TC_KC * 4;                  // 16 KB
+constexpr uint32_t A_BYTES = TC_M * TC_KC * 4;                  // 16 KB per 128-row tile
 constexpr uint32_t B_BYTES = TC_N * TC_KC * 4;                  // 2 KB
-constexpr uint32_t OFF_A = 0;                                   // [hi, lo]
-constexpr uint32_t OFF_B = OFF_A + 2 * A_BYTES;                 // [hi, lo]
-constexpr uint32_t OFF_L = OFF_B + 2 * B_BYTES;                 // float [3][TC_MAXNP1][LSTR]
-constexpr uint32_t OFF_NODES = OFF_L + 3 * TC_MAXNP1 * LSTR * 4;  // float [3][TC_MAXNP1], relative to the centre
-constexpr uint32_t OFF_BAR = (OFF_NODES + 3 * TC_MAXNP1 * 4 + 15) / 16 * 16;   // uint64
-constexpr uint32_t OFF_MISC = OFF_BAR + 16;                     // tmem address, status
-constexpr uint32_t TC_SMEM = OFF_MISC + 16;
+
+// Layout of k_p2m_tc<NP1>: NT = ceil((n+1)^2 / 128) row tiles of A (hi tiles,
+// then lo tiles), B [hi, lo], the bases float [3][NP1][LSTR], the grid
+// relative to its centre float [3][NP1], the mbarrier and the TMEM address.
+template <int NP1>
+struct P2mLayout {
+    static constexpr int NT = (NP1 * NP1 + TC_M - 1) / TC_M;
+    static constexpr uint32_t OFF_A = 0;
+    static constexpr uint32_t OFF_B = OFF_A + 2 * NT * A_BYTES;
+    static constexpr uint32_t OFF_L = OFF_B + 2 * B_BYTES;
+    static constexpr uint32_t OFF_NODES = OFF_L + 3 * NP1 * LSTR * 4;
+    static constexpr uint32_t OFF_BAR = (OFF_NODES + 3 * NP1 * 4 + 15) / 16 * 16;
+    static constexpr uint32_t OFF_MISC = OFF_BAR + 16;
+    static constexpr uint32_t SMEM = OFF_MISC + 16;
+    static constexpr uint32_t TMEM_COLS = NT == 1 ? 32 : 64;    // per tile: hi*hi 16 columns, cross products 16
+};
 
 // byte offset of element (row, k) of a K-major tile with `rows` rows
 __device__ __forceinline__ uint32_t kmajor_off(int rows, int row, int k)
@@ -161,19 +169,20 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
          const double *__restrict__ sz, const double *__restrict__ sq, double *__restrict__ Q, int *err,
          int expire_test)
 {
-    constexpr int n = NP1 - 1, ROWS = NP1 * NP1, P = ROWS * NP1;
+    using Ly = P2mLayout<NP1>;
+    constexpr int n = NP1 - 1, ROWS = NP1 * NP1, P = ROWS * NP1, NT = Ly::NT;
     extern __shared__ __align__(1024) unsigned char sm[];
-    float *Lb = reinterpret_cast<float *>(sm + OFF_L);          // [axis][k][particle], rows of LSTR
-    float *nodes = reinterpret_cast<float *>(sm + OFF_NODES);   // [axis][k], relative to the grid's centre
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
-    uint32_t *misc = reinterpret_cast<uint32_t *>(sm + OFF_MISC);  // [0] tmem address, [1] status
-    unsigned char *Ah = sm + OFF_A, *Al = Ah + A_BYTES, *Bh = sm + OFF_B, *Bl = Bh + B_BYTES;
+    float *Lb = reinterpret_cast<float *>(sm + Ly::OFF_L);      // [axis][k][particle], rows of LSTR
+    float *nodes = reinterpret_cast<float *>(sm + Ly::OFF_NODES);   // [axis][k], relative to the grid's centre
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Ly::OFF_BAR);
+    uint32_t *misc = reinterpret_cast<uint32_t *>(sm + Ly::OFF_MISC);  // [0] tmem address, [1] status
+    unsigned char *Bh = sm + Ly::OFF_B, *Bl = Bh + B_BYTES;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int node = leaves[blockIdx.x];
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(misc)),
-                     "r"(TC_TMEM_COLS));
+                     "r"(Ly::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (t == 0) {
@@ -190,7 +199,7 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
         nodes[t] = (float)(g[t] - (ax == 0 ? cx : ax == 1 ? cy : cz));
     }
     // operand tiles start zero: padding rows and columns are never written
-    for (uint32_t o = t * 16; o < OFF_L; o += TC_THREADS * 16) *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
+    for (uint32_t o = t * 16; o < Ly::OFF_L; o += TC_THREADS * 16) *reinterpret_cast<uint4 *>(sm + o) = make_uint4(0, 0, 0, 0);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -198,10 +207,11 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
 
     const int b0 = ibeg[node], m = numpar[node];
     const int nch = (m + TC_KC - 1) / TC_KC;
-    const int k2 = t % NP1, k3 = t / NP1;      // this thread's A row (valid for t < ROWS)
-    double acc[NP1];                           // this row of Q (TMEM lane t), FP64 across chunks
+    double acc[NT][NP1];                       // rows t + 128 tile of Q (TMEM lanes), FP64 across chunks
 #pragma unroll
-    for (int k = 0; k < NP1; k++) acc[k] = 0.0;
+    for (int a = 0; a < NT; a++)
+#pragma unroll
+        for (int k = 0; k < NP1; k++) acc[a][k] = 0.0;
     bool ok = true;
     const uint32_t bar_a = smem_addr(bar);
     if (expire_test) {
@@ -261,34 +271,41 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
             for (int k = 0; k < NP1; k++) L[k] = 0.0f;
         }
 #pragma unroll
-        for (int k = 0; k < NP1; k++) Lb[(warp * TC_MAXNP1 + k) * LSTR + lane] = L[k];
+        for (int k = 0; k < NP1; k++) Lb[(warp * NP1 + k) * LSTR + lane] = L[k];
     };
 
-    // chunk c: hi*hi into accumulator columns 0-15 and the two cross
-    // products into columns 16-31, from zero (short FP32 sums on the tensor
-    // core), folded into FP64 registers once its MMAs have completed.  The
-    // next chunk's bases are evaluated while the tensor core works.
+    // chunk c: per tile, hi*hi into accumulator columns 0-15 and the two
+    // cross products into columns 16-31 of the tile's 32, from zero (short
+    // FP32 sums on the tensor core), folded into FP64 registers once its
+    // MMAs have completed.  The next chunk's bases are evaluated while the
+    // tensor core works.
     double pv, pq;                 // the next chunk's coordinate and charge (prefetched)
     fetch(0, pv, pq);
     if (ok) bases(0, pv, pq);
     fetch(1, pv, pq);
     __syncthreads();
     for (int c = 0; c < nch && ok; c++) {
-        // A rows (k2, k3): Ly[k2] * Lz[k3] for the chunk's particles
-        if (t < ROWS) {
-            const float *ly = Lb + (1 * TC_MAXNP1 + k2) * LSTR, *lz = Lb + (2 * TC_MAXNP1 + k3) * LSTR;
+        // A rows r = (k2, k3): Ly[k2] * Lz[k3] for the chunk's particles
 #pragma unroll
-            for (int k4 = 0; k4 < TC_KC; k4 += 4) {
-                const float4 a = *reinterpret_cast<const float4 *>(ly + k4);
-                const float4 b = *reinterpret_cast<const float4 *>(lz + k4);
-                uint4 h, l;
-                split_tf32(a.x * b.x, h.x, l.x);
-                split_tf32(a.y * b.y, h.y, l.y);
-                split_tf32(a.z * b.z, h.z, l.z);
-                split_tf32(a.w * b.w, h.w, l.w);
-                const uint32_t o = kmajor_off(TC_M, t, k4);
-                *reinterpret_cast<uint4 *>(Ah + o) = h;
-                *reinterpret_cast<uint4 *>(Al + o) = l;
+        for (int tile = 0; tile < NT; tile++) {
+            const int r = t + TC_M * tile;
+            if (r < ROWS) {
+                const int k2 = r % NP1, k3 = r / NP1;
+                const float *ly = Lb + (1 * NP1 + k2) * LSTR, *lz = Lb + (2 * NP1 + k3) * LSTR;
+                unsigned char *Ah = sm + Ly::OFF_A + tile * A_BYTES, *Al = Ah + NT * A_BYTES;
+#pragma unroll
+                for (int k4 = 0; k4 < TC_KC; k4 += 4) {
+                    const float4 a = *reinterpret_cast<const float4 *>(ly + k4);
+                    const float4 b = *reinterpret_cast<const float4 *>(lz + k4);
+                    uint4 h, l;
+                    split_tf32(a.x * b.x, h.x, l.x);
+                    split_tf32(a.y * b.y, h.y, l.y);
+                    split_tf32(a.z * b.z, h.z, l.z);
+                    split_tf32(a.w * b.w, h.w, l.w);
+                    const uint32_t o = kmajor_off(TC_M, t, k4);
+                    *reinterpret_cast<uint4 *>(Ah + o) = h;
+                    *reinterpret_cast<uint4 *>(Al + o) = l;
+                }
             }
         }
         {
@@ -312,13 +329,18 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
         __syncthreads();
         if (t == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t ah = smem_addr(Ah), al = smem_addr(Al), bh = smem_addr(Bh), bl = smem_addr(Bl);
+            const uint32_t bh = smem_addr(Bh), bl = smem_addr(Bl);
 #pragma unroll
-            for (int s = 0; s < TC_KSTEPS; s++) {
-                const uint32_t oa = s * TC_M * 32, ob = s * TC_N * 32;
-                mma_tf32(tmem, smem_desc(ah + oa), smem_desc(bh + ob), s > 0 ? 1u : 0u);
-                mma_tf32(tmem + 16, smem_desc(ah + oa), smem_desc(bl + ob), s > 0 ? 1u : 0u);
-                mma_tf32(tmem + 16, smem_desc(al + oa), smem_desc(bh + ob), 1u);
+            for (int tile = 0; tile < NT; tile++) {
+                const uint32_t ah = smem_addr(sm + Ly::OFF_A + tile * A_BYTES), al = ah + NT * A_BYTES;
+                const uint32_t d = tmem + 32 * tile;
+#pragma unroll
+                for (int s = 0; s < TC_KSTEPS; s++) {
+                    const uint32_t oa = s * TC_M * 32, ob = s * TC_N * 32;
+                    mma_tf32(d, smem_desc(ah + oa), smem_desc(bh + ob), s > 0 ? 1u : 0u);
+                    mma_tf32(d + 16, smem_desc(ah + oa), smem_desc(bl + ob), s > 0 ? 1u : 0u);
+                    mma_tf32(d + 16, smem_desc(al + oa), smem_desc(bh + ob), 1u);
+                }
             }
             mma_commit(bar_a);
         }
@@ -331,22 +353,25 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
         const bool done = bar_wait(bar_a, (uint32_t)(c & 1));
         if (done) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint32_t r[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                "[%32];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int k = 0; k < NP1; k++)
-                acc[k] += (double)__uint_as_float(r[k]) + (double)__uint_as_float(r[16 + k]);
+            for (int tile = 0; tile < NT; tile++) {
+                uint32_t r[32];
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + 32 * tile;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                      "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                      "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int k = 0; k < NP1; k++)
+                    acc[tile][k] += (double)__uint_as_float(r[k]) + (double)__uint_as_float(r[16 + k]);
+            }
         }
         // orders the accumulator loads before the next MMAs and the new bases
         // before the next operands; a wait that expired anywhere ends the loop
@@ -358,9 +383,13 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
         }
     }
     if (ok) {
-        if (t < ROWS) {
 #pragma unroll
-            for (int k1 = 0; k1 < NP1; k1++) Q[(size_t)node * P + k1 + NP1 * t] = acc[k1];
+        for (int tile = 0; tile < NT; tile++) {
+            const int r = t + TC_M * tile;
+            if (r < ROWS) {
+#pragma unroll
+                for (int k1 = 0; k1 < NP1; k1++) Q[(size_t)node * P + k1 + NP1 * r] = acc[tile][k1];
+            }
         }
     } else if (t == 0) {
         atomicExch(err, 1);
@@ -369,7 +398,7 @@ k_p2m_tc(const int *__restrict__ leaves, const int *__restrict__ ibeg, const int
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Ly::TMEM_COLS));
     }
 }
 
@@ -381,8 +410,8 @@ void p2m_tc_t(int nleaves, const int *leaves, const int *ibeg, const int *numpar
     // BARYTREE_B200_TEST_EXPIRE_TC_WAIT=1 makes every block's first wait run
     // out (no MMA in flight), to test the timeout path end to end
     const int expire_now = getenv("BARYTREE_B200_TEST_EXPIRE_TC_WAIT") != nullptr;
-    cudaFuncSetAttribute(k_p2m_tc<NP1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
-    k_p2m_tc<NP1><<<nleaves, TC_THREADS, TC_SMEM, st>>>(leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err,
+    cudaFuncSetAttribute(k_p2m_tc<NP1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2mLayout<NP1>::SMEM);
+    k_p2m_tc<NP1><<<nleaves, TC_THREADS, P2mLayout<NP1>::SMEM, st>>>(leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err,
                                                           expire_now);
 }
 
@@ -652,13 +681,14 @@ k_p2m_hermite_tc(const HermChunkTc *__restrict__ chunks, const double *__restric
 // ---------------------------------------------------------------------------
 
 constexpr int L2_M = 128, L2_N = 128, L2_K = 16;
+constexpr int L2_MAXNP1 = 11;                           // (n+1)^2 <= 128 = N
 constexpr uint32_t L2_TMEM_COLS = 128;
 constexpr uint32_t L2_A_BYTES = L2_M * L2_K * 4;        // 8 KB
 constexpr uint32_t L2_B_BYTES = L2_N * L2_K * 4;        // 8 KB
 constexpr uint32_t L2_OFF_A = 0;                        // [hi, lo]
 constexpr uint32_t L2_OFF_B = L2_OFF_A + 2 * L2_A_BYTES;  // [hi, lo]
-constexpr uint32_t L2_OFF_NODES = L2_OFF_B + 2 * L2_B_BYTES;   // float [3][TC_MAXNP1]
-constexpr uint32_t L2_OFF_BAR = (L2_OFF_NODES + 3 * TC_MAXNP1 * 4 + 15) / 16 * 16;
+constexpr uint32_t L2_OFF_NODES = L2_OFF_B + 2 * L2_B_BYTES;   // float [3][L2_MAXNP1]
+constexpr uint32_t L2_OFF_BAR = (L2_OFF_NODES + 3 * L2_MAXNP1 * 4 + 15) / 16 * 16;
 constexpr uint32_t L2_OFF_MISC = L2_OFF_BAR + 16;
 constexpr uint32_t L2_SMEM = L2_OFF_MISC + 16;
 constexpr uint32_t L2_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(L2_N >> 3) << 17) |
@@ -854,6 +884,8 @@ void l2p_tc_t(int nitems, const int2 *items, const int *leaf_node, const int *t_
 
 bool p2m_tc_supported(int n) { return n >= 1 && n + 1 <= TC_MAXNP1; }
 
+bool l2p_tc_supported(int n) { return n >= 1 && n + 1 <= L2_MAXNP1; }
+
 void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const int *numpar, const double *grid,
                    const double *sx, const double *sy, const double *sz, const double *sq, double *Q, int *err,
                    cudaStream_t st)
@@ -861,7 +893,8 @@ void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const
     if (nleaves <= 0) return;
     switch (n + 1) {
 #define BT_TC(N) case N: p2m_tc_t<N>(nleaves, leaves, ibeg, numpar, grid, sx, sy, sz, sq, Q, err, st); return;
-        BT_TC(2) BT_TC(3) BT_TC(4) BT_TC(5) BT_TC(6) BT_TC(7) BT_TC(8) BT_TC(9) BT_TC(10) BT_TC(11)
+        BT_TC(2) BT_TC(3) BT_TC(4) BT_TC(5) BT_TC(6) BT_TC(7) BT_TC(8) BT_TC(9) BT_TC(10) BT_TC(11) BT_TC(12)
+        BT_TC(13) BT_TC(14) BT_TC(15) BT_TC(16)
 #undef BT_TC
     }
 }

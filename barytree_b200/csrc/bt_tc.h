@@ -12,7 +12,7 @@ struct HermChunkTc {
 };
 
 // Leaf P2M (Lagrange) on the tensor cores in 3xTF32 with FP32 accumulation,
-// for degrees with (n+1)^2 <= 128.  Same output layout as launch_p2m
+// for degrees with n + 1 <= 16 ((n+1)^2 rows in one or two 128-row tiles).  Same output layout as launch_p2m
 // (Q[node * P + k1 + (n+1) (k2 + (n+1) k3)], FP64).  *err is set to 1 if a
 // bounded wait for the tensor core expired (the leaf's Q is then not written).
 bool p2m_tc_supported(int n);
@@ -20,6 +20,7 @@ void launch_p2m_tc(int n, int nleaves, const int *leaves, const int *ibeg, const
                    const double *sx, const double *sy, const double *sz, const double *sq, double *Q, int *err,
                    cudaStream_t st);
 
+bool l2p_tc_supported(int n);     // n + 1 <= 11: the (n+1)^2 columns in one N = 128 MMA
 // L2P (Lagrange) at the target leaves on the tensor cores: each item (leaf,
 // chunk of 128 targets) adds its targets' interpolated grid values to pot
 // (3xTF32, FP32 accumulation); same items and layout as launch_l2p, degrees

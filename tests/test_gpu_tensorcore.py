@@ -3,12 +3,12 @@ Lagrange path, against the FP64 SIMT P2M (option BT_UPWARD_FP64) and the
 FP64 direct sum.
 
 The two upward passes must agree to within a few FP32 roundings at every
-degree the tensor-core kernel covers ((n+1)^2 <= 128): 5e-7 relative in the
-potentials, where the proxy charges carry about 1.4e-7 (3xTF32 products,
-short FP32 sums on the tensor core, FP64 across 32-particle chunks); the
-potentials must keep the mixed path's accuracy against the direct sum.  They must not be bit-identical there (proof that the
-tensor-core kernel ran); at degrees 11 and 12 the FP64 kernel serves both
-settings and the potentials are identical.  Every leaf exercises the
+degree (the tensor-core kernel covers n + 1 <= 16: (n+1)^2 rows in one or
+two 128-row tiles): 5e-7 relative in the potentials, where the proxy charges
+carry about 1.4e-7 (3xTF32 products, short FP32 sums on the tensor core,
+FP64 across 32-particle chunks); the potentials must keep the mixed path's
+accuracy against the direct sum.  They must not be bit-identical (proof that
+the tensor-core kernel ran).  Every leaf exercises the
 exact-node rule: its extreme particles sit on the end nodes of its grid.
 """
 import numpy as np
@@ -32,11 +32,8 @@ def test_tensor_core_p2m_against_fp64_p2m(degree):
     tc, rep = B.treecode(tx, ty, tz, sx, sy, sz, sq, return_report=True, **kw)
     f64 = B.treecode(tx, ty, tz, sx, sy, sz, sq, upward=B.UPWARD_FP64, **kw)
     assert rep["pc_ptwise"] > 0
-    if degree <= 10:
-        assert not np.array_equal(tc, f64)
-        assert _rel(tc, f64) < 5e-7
-    else:
-        assert np.array_equal(tc, f64)
+    assert not np.array_equal(tc, f64)
+    assert _rel(tc, f64) < 5e-7
     idx = np.arange(0, len(tx), 80)
     exact = B.direct(tx[idx], ty[idx], tz[idx], sx, sy, sz, sq)
     assert _rel(tc[idx], exact) <= 1.05 * _rel(f64[idx], exact) + 3e-7
