@@ -869,29 +869,49 @@ int issue_plan(const DevPlan &v, cudaStream_t st, cudaEvent_t *ev, double *scatt
                 launches++;
             }
         }
-        // proxy charges at the other degrees chosen per interaction
+        // proxy charges at the degrees chosen per interaction: independent
+        // chains (P2M, M2M level by level, FP32 copy), spread over the main
+        // stream and the two side streams so that one degree's small
+        // upper-level launches overlap another's
+        const bool xfork = xdeg.size() > 1 && fk && fk->side && fk->side2;
+        cudaStream_t xst[3] = {st, st, st};
+        if (xfork) {
+            CK(cudaEventRecord(fk->fork, st));
+            CK(cudaStreamWaitEvent(fk->side, fk->fork, 0));
+            CK(cudaStreamWaitEvent(fk->side2, fk->fork, 0));
+            xst[1] = fk->side;
+            xst[2] = fk->side2;
+        }
         for (size_t i = 0; i < xdeg.size(); i++) {
             const int d = xdeg[i];
             const int nl = v.xleaf_n[i];
+            cudaStream_t ds = xst[i % 3];
             if (nl > 0) {
                 if (v.tc_up && bt::p2m_tc_supported(d))
                     bt::launch_p2m_tc(d, nl, v.d_xleaves[i], d_sibeg, d_snum, d_xgrid[i], d_sx, d_sy, d_sz, d_sq,
-                                      d_xQ[i], v.d_err, st);
+                                      d_xQ[i], v.d_err, ds);
                 else
                     bt::launch_p2m(d, false, nl, v.d_xleaves[i], v.S_n, d_sibeg, d_snum, d_xgrid[i], d_slen, d_ww,
-                                   d_sx, d_sy, d_sz, d_sq, d_xQ[i], st);
+                                   d_sx, d_sy, d_sz, d_sq, d_xQ[i], ds);
                 launches++;
             }
             const std::vector<int> &lo = v.xlvl_off[i];
             for (int l = v.S_max_depth - 1; l >= 0; l--) {
                 int cnt = lo[l + 1] - lo[l];
                 if (cnt > 0) {
-                    bt::launch_m2m(d, cnt, v.d_xlvl[i] + lo[l], d_snch, d_sch, d_xgrid[i], d_xQ[i], st);
+                    bt::launch_m2m(d, cnt, v.d_xlvl[i] + lo[l], d_snch, d_sch, d_xgrid[i], d_xQ[i], ds);
                     launches++;
                 }
             }
-            bt::launch_to_f32((size_t)v.S_n * (d + 1) * (d + 1) * (d + 1), d_xQ[i], d_xQ32[i], st);
+            bt::launch_to_f32((size_t)v.S_n * (d + 1) * (d + 1) * (d + 1), d_xQ[i], d_xQ32[i], ds);
             launches++;
+        }
+        if (xfork) {
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(fk->join, fk->side));
+            CK(cudaEventRecord(fk->join2, fk->side2));
+            CK(cudaStreamWaitEvent(st, fk->join, 0));
+            CK(cudaStreamWaitEvent(st, fk->join2, 0));
         }
     }
     CK(cudaGetLastError());
