@@ -443,9 +443,10 @@ void launch_labels(const LabelArgs &a, int nsamples, cudaStream_t st)
 // (N_t the target's cluster entries, phi_t its potential), the system's
 // relative L2 error is about c tol.  phi_t^2 is estimated per target leaf
 // at two sampled targets: the near-field sum sum_j q_j^2 / r_j^2 over the
-// leaf's near-field leaves (r floored at each leaf's mean particle spacing)
-// plus, per cluster entry, (|q_C|_2 / d)^2 -- the mean square potential of
-// charges of either sign.  Each interaction then takes the lowest degree d with
+// leaf's near-field leaves within twice their radius (r floored at each
+// leaf's mean particle spacing), (|q_L|_2 / d)^2 for the other near-field
+// leaves and per cluster entry (|q_C|_2 / d)^2 -- the mean square potential
+// of charges of either sign.  Each interaction then takes the lowest degree d with
 // e_d + log10(|q_C|_2 / d) <= log10(share), or direct evaluation when no
 // degree qualifies or direct is cheaper.
 __global__ void k_unit_phi2_sampled(FeatureArgs a, const int *__restrict__ t_ibeg, const int64_t *__restrict__ d_off,
@@ -474,18 +475,32 @@ __global__ void k_unit_phi2_sampled(FeatureArgs a, const int *__restrict__ t_ibe
             phi2 += q2 * q2 / (dx * dx + dy * dy + dz * dz);
         }
     }
-    // near field: each particle's q^2 / r^2 with r no smaller than the leaf's
-    // mean particle spacing (radius / count^(1/3)), which keeps a chance
-    // close neighbour from dominating the estimate; FP32 (an estimate)
+    // near field: a leaf farther than twice its radius from a sampled
+    // target adds |q_L|_2^2 / d^2, as a cluster entry does; a closer one
+    // adds each particle's q^2 / r^2 with r no smaller than the leaf's mean
+    // particle spacing (radius / count^(1/3)), which keeps a chance close
+    // neighbour from dominating the estimate; FP32 (an estimate)
     float near = 0.0f;
     for (int64_t e = d_off[u]; e < d_off[u + 1]; e++) {
         const int s = d_idx[e], b = s_ibeg[s], m = a.s_numpar[s];
-        const float h = (float)(a.s_rad[s] / cbrt((double)m));
+        const double rs = a.s_rad[s], q2 = a.s_mom[2 * s + 1];
+        bool touch[NS], any = false;
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            const double dx = px[k] - a.s_ctr[3 * s], dy = py[k] - a.s_ctr[3 * s + 1], dz = pz[k] - a.s_ctr[3 * s + 2];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            touch[k] = d2 <= 4.0 * rs * rs;
+            any = any || touch[k];
+            if (!touch[k] && threadIdx.x == 0) phi2 += q2 * q2 / d2;
+        }
+        if (!any) continue;
+        const float h = (float)(rs / cbrt((double)m));
         const float h2 = fmaxf(h * h, FLT_MIN);
         for (int j = threadIdx.x; j < m; j += blockDim.x) {
             const float q = (float)sq[b + j];
 #pragma unroll
             for (int k = 0; k < NS; k++) {
+                if (!touch[k]) continue;
                 const float dx = (float)(px[k] - sx[b + j]), dy = (float)(py[k] - sy[b + j]),
                             dz = (float)(pz[k] - sz[b + j]);
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
