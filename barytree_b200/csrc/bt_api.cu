@@ -1845,6 +1845,8 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
         L.add(&d_tnum, T.n); L.add(&d_idx, ne); L.add(&d_unit, T.nleaves); L.add(&d_off, pl.t_approx.rows + 1);
         L.add(&d_feat, (size_t)ne * bt::MLP_IN); L.add(&d_w, w.size());
         L.add(&d_pred, (size_t)ne * bt::MLP_OUT); L.add(&d_choice, ne);
+        int *d_mlperr;          // set by the MLP kernel if a bounded wait expired
+        L.add(&d_mlperr, 1);
         // the error share: near-field lists, the target leaves' first
         // particles, per-unit sums, one share per system; the particles in
         // tree order (on the device already after a GPU tree build)
@@ -1889,7 +1891,8 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             fa.t_numpar = d_tnum; fa.s_numpar = d_snum;
             bt::launch_features(fa, ne, d_feat, st);
             launches++;
-            bt::mlp_infer(d_w, ne, d_feat, d_pred, st);
+            CK(cudaMemsetAsync(d_mlperr, 0, sizeof(int), st));
+            bt::mlp_infer_tc(d_w, ne, d_feat, d_pred, d_mlperr, st);
             launches++;
             CK(cudaMemcpyAsync(d_doff, pl.t_direct.off, sizeof(int64_t) * (pl.t_direct.rows + 1),
                                cudaMemcpyHostToDevice, st));
@@ -1909,8 +1912,14 @@ int select_degrees(DeviceCtx *ctx, Arena &arena, bt_plan &pl, double tol, const 
             launches += 3;
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(choice.data(), d_choice, ne, cudaMemcpyDeviceToHost, st));
+            int mlperr = 0;
+            CK(cudaMemcpyAsync(&mlperr, d_mlperr, sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             g_launches += launches;
+            if (mlperr) {
+                set_err("the degree selector's tensor-core kernel timed out waiting for its MMAs");
+                return BT_ERR_TIMEOUT;
+            }
         }
     }
     pt.mark("selection: features + MLP (GPU)");
@@ -2697,18 +2706,27 @@ int bt_mlp_predict(const float *weights, const float *features, long n, float *o
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t st = ctx->stream;
     float *d_w, *d_x, *d_yh;
+    int *d_mlperr;
     Layout L;
     L.add(&d_w, bt::MLP_NWEIGHTS); L.add(&d_x, (size_t)n * bt::MLP_IN); L.add(&d_yh, (size_t)n * bt::MLP_OUT);
+    L.add(&d_mlperr, 1);
     if (!ctx->arena.reserve(L.total())) { set_err("device allocation failed"); return BT_ERR_CUDA; }
     L.bind(ctx->arena);
     {
         CK(cudaMemcpyAsync(d_w, weights, sizeof(float) * bt::MLP_NWEIGHTS, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(d_x, features, sizeof(float) * (size_t)n * bt::MLP_IN, cudaMemcpyHostToDevice, st));
-        bt::mlp_infer(d_w, n, d_x, d_yh, st);
+        CK(cudaMemsetAsync(d_mlperr, 0, sizeof(int), st));
+        bt::mlp_infer_tc(d_w, n, d_x, d_yh, d_mlperr, st);
         g_launches += 1;
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out, d_yh, sizeof(float) * (size_t)n * bt::MLP_OUT, cudaMemcpyDeviceToHost, st));
+        int mlperr = 0;
+        CK(cudaMemcpyAsync(&mlperr, d_mlperr, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (mlperr) {
+            set_err("the MLP's tensor-core kernel timed out waiting for its MMAs");
+            rc = BT_ERR_TIMEOUT;
+        }
     }
 done:
     return rc;

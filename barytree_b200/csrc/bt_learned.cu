@@ -208,51 +208,6 @@ __global__ void k_linear_fwd(int B, int I, int O, const float *__restrict__ X, c
     Y[idx] = act ? tanhf(s) : s;
 }
 
-// Inference of the whole network in one kernel: weights in shared memory
-// (read as broadcasts, four per 16-byte load), one row per thread, the
-// activations in registers.  Each output accumulates its inputs in the same
-// order as k_linear_fwd (bias, then input 0, 1, ...), so the predictions are
-// the layer-by-layer ones bit for bit.
-constexpr int MI_THREADS = 128;
-
-template <int I, int O, bool ACT>
-__device__ __forceinline__ void dense(const float *__restrict__ W, const float *__restrict__ bias, const float *x,
-                                      float *y)
-{
-#pragma unroll
-    for (int o = 0; o < O; o++) y[o] = bias[o];
-#pragma unroll
-    for (int i = 0; i < I; i++) {
-#pragma unroll
-        for (int o = 0; o < O; o++) y[o] = fmaf(x[i], W[i * O + o], y[o]);
-    }
-    if (ACT) {
-#pragma unroll
-        for (int o = 0; o < O; o++) y[o] = tanhf(y[o]);
-    }
-}
-
-__global__ void __launch_bounds__(MI_THREADS) k_mlp_infer(const float *__restrict__ w, int64_t B,
-                                                          const float *__restrict__ X, float *__restrict__ Y)
-{
-    __shared__ __align__(16) float sw[(MLP_NWEIGHTS + 3) & ~3];
-    for (int i = threadIdx.x; i < MLP_NWEIGHTS; i += blockDim.x) sw[i] = w[i];
-    __syncthreads();
-    const float *norm = sw, *W0 = sw + 2 * MLP_IN, *b0 = W0 + MLP_IN * MLP_H, *W1 = b0 + MLP_H, *b1 = W1 + MLP_H * MLP_H,
-                *W2 = b1 + MLP_H, *b2 = W2 + MLP_H * MLP_H, *W3 = b2 + MLP_H, *b3 = W3 + MLP_H * MLP_OUT;
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < B; r += (int64_t)gridDim.x * blockDim.x) {
-        float x[MLP_IN], h[MLP_H], g[MLP_H], y[MLP_OUT];
-#pragma unroll
-        for (int i = 0; i < MLP_IN; i++) x[i] = norm_input(X[r * MLP_IN + i], norm[i], norm[MLP_IN + i]);
-        dense<MLP_IN, MLP_H, true>(W0, b0, x, h);
-        dense<MLP_H, MLP_H, true>(W1, b1, h, g);
-        dense<MLP_H, MLP_H, true>(W2, b2, g, h);
-        dense<MLP_H, MLP_OUT, false>(W3, b3, h, y);
-#pragma unroll
-        for (int o = 0; o < MLP_OUT; o++) Y[r * MLP_OUT + o] = y[o];
-    }
-}
-
 // dX[b][i] = (sum_o dY[b][o] W[i][o]) * (1 - A[b][i]^2)  (A = tanh output of the layer below)
 __global__ void k_linear_bwd_in(int B, int I, int O, const float *__restrict__ dY, const float *__restrict__ W,
                                 const float *__restrict__ A, float *__restrict__ dX)
@@ -353,17 +308,6 @@ void mlp_forward(const float *w, int B, const float *X, float *act, float *Yh, c
     k_linear_fwd<<<nb((long long)B * MLP_H, 256), 256, 0, st>>>(B, MLP_H, MLP_H, A1, v.W[1], v.b[1], nullptr, 1, A2);
     k_linear_fwd<<<nb((long long)B * MLP_H, 256), 256, 0, st>>>(B, MLP_H, MLP_H, A2, v.W[2], v.b[2], nullptr, 1, A3);
     k_linear_fwd<<<nb((long long)B * MLP_OUT, 256), 256, 0, st>>>(B, MLP_H, MLP_OUT, A3, v.W[3], v.b[3], nullptr, 0, Yh);
-}
-
-void mlp_infer(const float *w, int64_t B, const float *X, float *Yh, cudaStream_t st)
-{
-    if (B <= 0) return;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t need = (B + MI_THREADS - 1) / MI_THREADS;
-    const int grid = (int)std::min<int64_t>(need, (int64_t)sms * 8);
-    k_mlp_infer<<<grid, MI_THREADS, 0, st>>>(w, B, X, Yh);
 }
 
 // Forward + backward of the MSE loss on one batch; grad has the weight layout

@@ -41,8 +41,7 @@ struct LabelArgs {
 
 MlpView mlp_view(float *w);
 void mlp_forward(const float *w, int B, const float *X, float *act, float *Yh, cudaStream_t st);
-// Inference only, one fused kernel; bit-identical to mlp_forward's output.
-void mlp_infer(const float *w, int64_t B, const float *X, float *Yh, cudaStream_t st);
+// Inference: mlp_infer_tc (bt_tc.h), on the tensor cores.
 void mlp_forward_backward(const float *w, int B, const float *X, const float *Y, float *act, float *Yh, float *dbuf,
                           float *lossb, float *grad, cudaStream_t st);
 void mlp_adam(int n, float *w, const float *g, float *m, float *v, float lr, int step, cudaStream_t st);

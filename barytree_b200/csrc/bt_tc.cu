@@ -30,6 +30,7 @@
 // its tensor memory and returns without writing.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 #include <cstdlib>
@@ -880,6 +881,244 @@ void l2p_tc_t(int nitems, const int2 *items, const int *leaf_node, const int *t_
                                                          pot, err);
 }
 
+// ---------------------------------------------------------------------------
+// Inference of the degree selector's MLP (6 -> 64 -> 64 -> 64 -> 11, tanh)
+// on the tensor cores: every layer of a tile of 128 rows is one GEMM,
+// D[row, o] = sum_i A[row, i] W[i, o], with the rows as M = 128, the layer's
+// outputs as N (64, or 16 for the 11 outputs) and its inputs as K (8 for the
+// 6 features, else 64), 3xTF32 into TMEM.  Each thread (= TMEM lane = row)
+// reads its row, adds the bias, applies tanh and writes the next layer's A
+// operand.  The weights, split into TF32 pairs, sit in shared memory as the
+// B operands for the whole kernel; the two warpgroups of a CTA work on
+// different tiles (their own A buffers, mbarriers and TMEM columns), so one's
+// MMAs overlap the other's activations.  The network is the one the
+// training kernels of bt_learned.cu (k_linear_fwd) evaluate; the sums are
+// the tensor core's, so the predictions agree with theirs to FP32 rounding
+// (about 1e-6 relative), not bit for bit.
+// ---------------------------------------------------------------------------
+
+constexpr int MT_IN = 6, MT_H = 64, MT_OUT = 11, MT_NOUT = 16, MT_K1 = 8;
+constexpr uint32_t MT_W1 = 0;                                     // [hi, lo]: N = 64 x K = 8
+constexpr uint32_t MT_W1B = MT_H * MT_K1 * 4;                     // 2 KB
+constexpr uint32_t MT_W2 = MT_W1 + 2 * MT_W1B;                    // [hi, lo]: 64 x 64
+constexpr uint32_t MT_WHB = MT_H * MT_H * 4;                      // 16 KB
+constexpr uint32_t MT_W3 = MT_W2 + 2 * MT_WHB;
+constexpr uint32_t MT_W4 = MT_W3 + 2 * MT_WHB;                    // [hi, lo]: 16 x 64
+constexpr uint32_t MT_W4B = MT_NOUT * MT_H * 4;                   // 4 KB
+constexpr uint32_t MT_A = MT_W4 + 2 * MT_W4B;                     // per warpgroup [hi, lo]: 128 x 64
+constexpr uint32_t MT_AB = TC_M * MT_H * 4;                       // 32 KB
+constexpr uint32_t MT_PAR = MT_A + 2 * 2 * MT_AB;                 // floats: b1 b2 b3 [64], b4 [16], mean, std [6]
+constexpr uint32_t MT_NPAR = 3 * MT_H + MT_NOUT + 2 * MT_IN;
+constexpr uint32_t MT_BAR = (MT_PAR + MT_NPAR * 4 + 15) / 16 * 16;   // 2 mbarriers, then the TMEM address
+constexpr uint32_t MT_SMEM = MT_BAR + 32;
+constexpr uint32_t MT_TMEM_COLS = 128;                            // warpgroup w: columns 64 w .. 64 w + 63
+__host__ __device__ constexpr uint32_t mt_idesc(int n)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32_n(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// 1 if any of the 128 threads of named barrier `id` passes a nonzero flag
+__device__ __forceinline__ int wg_any(int flag, int id)
+{
+    int r;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t"
+        "}\n"
+        : "=r"(r)
+        : "r"(flag), "r"(id)
+        : "memory");
+    return r;
+}
+
+// the B operand of one layer: W[i][o] (I x O, row-major) as N = o rows, K = i
+// columns, K-major, zero past I and O, split into TF32 pairs
+__device__ void mt_weights(const float *W, int I, int O, int N, int K, unsigned char *hi, unsigned char *lo)
+{
+    for (int e = threadIdx.x; e < N * K; e += blockDim.x) {
+        const int o = e / K, i = e % K;
+        const float v = (o < O && i < I) ? W[i * O + o] : 0.0f;
+        uint32_t h, l;
+        split_tf32(v, h, l);
+        const uint32_t off = kmajor_off(N, o, i);
+        *reinterpret_cast<uint32_t *>(hi + off) = h;
+        *reinterpret_cast<uint32_t *>(lo + off) = l;
+    }
+}
+
+__global__ void __launch_bounds__(2 * TC_THREADS, 1)
+k_mlp_infer_tc(const float *__restrict__ w, int64_t B, const float *__restrict__ X, float *__restrict__ Y, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    float *par = reinterpret_cast<float *>(sm + MT_PAR);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + MT_BAR);
+    uint32_t *misc = reinterpret_cast<uint32_t *>(sm + MT_BAR + 16);
+    const int tid = threadIdx.x, wg = tid >> 7, t = tid & 127, warp = tid >> 5;
+    // weight layout of bt_learned.h: norm (mean[6], std[6]), W1[6][64], b1,
+    // W2[64][64], b2, W3[64][64], b3, W4[64][11], b4
+    const float *norm = w, *W1 = w + 2 * MT_IN, *b1 = W1 + MT_IN * MT_H, *W2 = b1 + MT_H, *b2 = W2 + MT_H * MT_H,
+                *W3 = b2 + MT_H, *b3 = W3 + MT_H * MT_H, *W4 = b3 + MT_H, *b4 = W4 + MT_H * MT_OUT;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(misc)),
+                     "r"(MT_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + 1)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    mt_weights(W1, MT_IN, MT_H, MT_H, MT_K1, sm + MT_W1, sm + MT_W1 + MT_W1B);
+    mt_weights(W2, MT_H, MT_H, MT_H, MT_H, sm + MT_W2, sm + MT_W2 + MT_WHB);
+    mt_weights(W3, MT_H, MT_H, MT_H, MT_H, sm + MT_W3, sm + MT_W3 + MT_WHB);
+    mt_weights(W4, MT_H, MT_OUT, MT_NOUT, MT_H, sm + MT_W4, sm + MT_W4 + MT_W4B);
+    for (int i = tid; i < (int)MT_NPAR; i += blockDim.x) {
+        float v;
+        if (i < 3 * MT_H) v = (i < MT_H ? b1 : i < 2 * MT_H ? b2 : b3)[i % MT_H];
+        else if (i < 3 * MT_H + MT_NOUT) v = i - 3 * MT_H < MT_OUT ? b4[i - 3 * MT_H] : 0.0f;
+        else v = norm[i - 3 * MT_H - MT_NOUT];
+        par[i] = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = misc[0] + 64 * wg;
+    const uint32_t tlane = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    unsigned char *Ah = sm + MT_A + wg * 2 * MT_AB, *Al = Ah + MT_AB;
+    const uint32_t bar = smem_addr(bars + wg);
+    const int bid = 1 + wg;                            // the warpgroup's named barrier
+    const float *bb1 = par, *bb2 = par + MT_H, *bb3 = par + 2 * MT_H, *bb4 = par + 3 * MT_H;
+    const float *mean = par + 3 * MT_H + MT_NOUT, *sdev = mean + MT_IN;
+    uint32_t phase = 0;
+    bool ok = true;
+
+    // one layer: thread 0 of the warpgroup issues the MMAs, all wait for them
+    auto layer = [&](uint32_t wofs, uint32_t wbytes, int n, int ksteps) -> bool {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        asm volatile("bar.sync %0, 128;" ::"r"(bid) : "memory");
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t ah = smem_addr(Ah), al = smem_addr(Al);
+            const uint32_t bh = smem_addr(sm + wofs), bl = bh + wbytes;
+            const uint32_t idesc = mt_idesc(n);
+            for (int s = 0; s < ksteps; s++) {
+                const uint32_t oa = s * TC_M * 32, ob = s * n * 32;
+                mma_tf32_n(tmem, smem_desc(ah + oa), smem_desc(bh + ob), idesc, s > 0 ? 1u : 0u);
+                mma_tf32_n(tmem, smem_desc(ah + oa), smem_desc(bl + ob), idesc, 1u);
+                mma_tf32_n(tmem, smem_desc(al + oa), smem_desc(bh + ob), idesc, 1u);
+            }
+            mma_commit(bar);
+        }
+        const bool done = bar_wait(bar, phase);
+        phase ^= 1u;
+        const bool fail = wg_any(done ? 0 : 1, bid) != 0;
+        if (!fail) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        return !fail;
+    };
+    // this thread's row of a 64-column layer output, bias and tanh, as the
+    // next layer's A operand
+    auto activate = [&](const float *bias) {
+#pragma unroll
+        for (int c0 = 0; c0 < MT_H; c0 += 32) {
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                "[%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(tlane + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int k4 = 0; k4 < 32; k4 += 4) {
+                uint4 h, l;
+                split_tf32(tanhf(__uint_as_float(r[k4]) + bias[c0 + k4]), h.x, l.x);
+                split_tf32(tanhf(__uint_as_float(r[k4 + 1]) + bias[c0 + k4 + 1]), h.y, l.y);
+                split_tf32(tanhf(__uint_as_float(r[k4 + 2]) + bias[c0 + k4 + 2]), h.z, l.z);
+                split_tf32(tanhf(__uint_as_float(r[k4 + 3]) + bias[c0 + k4 + 3]), h.w, l.w);
+                const uint32_t o = kmajor_off(TC_M, t, c0 + k4);
+                *reinterpret_cast<uint4 *>(Ah + o) = h;
+                *reinterpret_cast<uint4 *>(Al + o) = l;
+            }
+        }
+    };
+
+    const int64_t ntiles = (B + TC_M - 1) / TC_M;
+    for (int64_t tile = (int64_t)blockIdx.x * 2 + wg; tile < ntiles && ok; tile += (int64_t)gridDim.x * 2) {
+        const int64_t row = tile * TC_M + t;
+        // layer 1's A: the normalised features, K = 8
+        {
+            uint4 h = make_uint4(0, 0, 0, 0), l = make_uint4(0, 0, 0, 0), h2 = h, l2 = l;
+            uint32_t hv[MT_K1] = {}, lv[MT_K1] = {};
+            if (row < B) {
+#pragma unroll
+                for (int i = 0; i < MT_IN; i++)
+                    split_tf32(fminf(fmaxf((X[row * MT_IN + i] - mean[i]) / sdev[i], -4.f), 4.f), hv[i], lv[i]);
+            }
+            h = make_uint4(hv[0], hv[1], hv[2], hv[3]); h2 = make_uint4(hv[4], hv[5], hv[6], hv[7]);
+            l = make_uint4(lv[0], lv[1], lv[2], lv[3]); l2 = make_uint4(lv[4], lv[5], lv[6], lv[7]);
+            *reinterpret_cast<uint4 *>(Ah + kmajor_off(TC_M, t, 0)) = h;
+            *reinterpret_cast<uint4 *>(Ah + kmajor_off(TC_M, t, 4)) = h2;
+            *reinterpret_cast<uint4 *>(Al + kmajor_off(TC_M, t, 0)) = l;
+            *reinterpret_cast<uint4 *>(Al + kmajor_off(TC_M, t, 4)) = l2;
+        }
+        if (!(ok = layer(MT_W1, MT_W1B, MT_H, 1))) break;
+        activate(bb1);
+        if (!(ok = layer(MT_W2, MT_WHB, MT_H, MT_H / 8))) break;
+        activate(bb2);
+        if (!(ok = layer(MT_W3, MT_WHB, MT_H, MT_H / 8))) break;
+        activate(bb3);
+        if (!(ok = layer(MT_W4, MT_W4B, MT_NOUT, MT_H / 8))) break;
+        {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(tlane));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < B) {
+#pragma unroll
+                for (int o = 0; o < MT_OUT; o++) Y[row * MT_OUT + o] = __uint_as_float(r[o]) + bb4[o];
+            }
+        }
+        // the next tile's first MMAs overwrite these columns after the
+        // warpgroup's next barrier, which orders the loads above before them
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    }
+    if (!ok && t == 0) {
+        atomicExch(err, 1);
+        bar_wait(bar, phase ^ 1u);          // one more bounded wait for the MMAs in flight
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(misc[0]), "r"(MT_TMEM_COLS));
+    }
+}
+
 }  // namespace
 
 bool p2m_tc_supported(int n) { return n >= 1 && n + 1 <= TC_MAXNP1; }
@@ -928,6 +1167,18 @@ void launch_p2m_hermite_tc(int n, int nchunks, const HermChunkTc *chunks, const 
         BT_HT(2) BT_HT(3) BT_HT(4) BT_HT(5) BT_HT(6) BT_HT(7) BT_HT(8)
 #undef BT_HT
     }
+}
+
+void mlp_infer_tc(const float *w, int64_t B, const float *X, float *Y, int *err, cudaStream_t st)
+{
+    if (B <= 0) return;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t pairs = ((B + TC_M - 1) / TC_M + 1) / 2;
+    const int grid = (int)std::min<int64_t>(pairs, (int64_t)sms);
+    cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MT_SMEM);
+    k_mlp_infer_tc<<<grid, 2 * TC_THREADS, MT_SMEM, st>>>(w, B, X, Y, err);
 }
 
 }  // namespace bt

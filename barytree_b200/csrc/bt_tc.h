@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cstdint>
 
 namespace bt {
 
@@ -36,5 +37,10 @@ bool p2m_hermite_tc_supported(int n);
 void launch_p2m_hermite_tc(int n, int nchunks, const HermChunkTc *chunks, const double *grid, const double *box_len,
                            const double *ww, const double *sx, const double *sy, const double *sz, const double *sq,
                            double *Q, double *partial, int *err, cudaStream_t st);
+
+// Inference of the degree selector's MLP (weights as bt_learned.h lays them
+// out, B rows of 6 features -> 11 outputs) on the tensor cores, 3xTF32 with
+// FP32 accumulation; *err as for launch_p2m_tc.
+void mlp_infer_tc(const float *w, int64_t B, const float *X, float *Y, int *err, cudaStream_t st);
 
 }  // namespace bt

@@ -41,6 +41,23 @@ def test_mlp_gradient_matches_cpu_oracle():
     assert np.allclose(pred, M.forward(w, X)[-1], rtol=1e-4, atol=1e-4)
 
 
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 255, 257, 40_003])
+def test_tensor_core_inference_ragged_sizes(n):
+    """The tensor-core inference (two 128-row tiles per CTA, 3xTF32) with
+    the committed selector's weights, on row counts around the tile size,
+    against the oracle's FP64 forward pass; features drawn from the spread
+    the selector sees, some beyond the normalisation's clamp."""
+    rng = np.random.default_rng(n)
+    w = S.load()
+    mean, sd = w[:S.IN], w[S.IN:2 * S.IN]
+    X = (mean + sd * rng.normal(scale=1.6, size=(n, S.IN))).astype(np.float32)
+    pred = S.predict(w, X)
+    ref = M.forward(w, X)[-1]
+    assert pred.shape == (n, S.OUT)
+    # log10 errors of magnitude up to ~16: FP32 resolution of the sums
+    assert np.max(np.abs(pred - ref)) < 2e-4 * max(1.0, np.max(np.abs(ref)))
+
+
 @pytest.fixture(scope="module")
 def small_training_set():
     x, y, z, q = S.blobs(300_000, seed=5)
