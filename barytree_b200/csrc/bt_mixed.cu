@@ -89,6 +89,20 @@ __host__ __device__ constexpr int rb_blocks()
     return HERM ? BT_MX_MIN_BLOCKS_HERM : KT == 2 ? BT_MX_MIN_BLOCKS_YUK : BT_MX_MIN_BLOCKS_T2;
 }
 
+// Share of the Lagrange far field's grid points (Coulomb and regularised
+// Coulomb) whose 1/r comes from rsqrt_sw / f2_rsqrt_sw on the FP32 and
+// integer pipes instead of the MUFU: BT_FAR_SW of every 8 by k1 index (1:
+// k1 = 0, and 8 at degrees above 7).  A far-field value needs only two FP32
+// operations besides its 1/r, so the FP32 pipe has room that the MUFU
+// lacks, but less than that count suggests: on the 16M clustered system
+// the evaluation took 819.8 ms with none, 802.7 ms with 1 of 8, and 829,
+// 863 and 919 ms with 2, 3 and 4 of 8 (same rel-L2, 1.0e-7).  Both forms
+// round alike lane by lane, so every tile shape still gives the same bits.
+#ifndef BT_FAR_SW
+#define BT_FAR_SW 1
+#endif
+__host__ __device__ constexpr bool far_sw(int k1) { return (k1 * BT_FAR_SW) % 8 < BT_FAR_SW; }
+
 // Far field of one source cluster (degree NP1-1) for NT targets at (x,y,z),
 // relative to the target centre; g = grid coordinates relative to the same
 // centre, q = proxy charges (shared memory, FP32).
@@ -123,6 +137,7 @@ __device__ __forceinline__ void pc_cluster(const float *x, const float *y, const
                 for (int t = 0; t < NT; t++) {
                     const float r2 = fmaf(gx[t][k1], gx[t][k1], dyz[t]);
                     if (KT == 2) row[t] += kf_far<KT>(r2, qq, kc);
+                    else if (far_sw(k1)) row[t] = fmaf(qq, rsqrt_sw(KT == 3 ? r2 + kc : r2), row[t]);
                     else row[t] = fmaf(qq, rsqrt_apx(KT == 3 ? r2 + kc : r2), row[t]);
                 }
             }
@@ -258,9 +273,13 @@ __device__ __forceinline__ void pc_cluster_f2(const float *x, const float *y, co
                 for (int p = 0; p < NPR; p++) {
                     f2_t r2 = f2_fma(gx[p][k1], gx[p][k1], dyz[p]);
                     if (KT == 3) r2 = f2_fma(one, kc2, r2);
-                    float a, b;
-                    f2_split(r2, a, b);
-                    row[p] = f2_fma(qq, f2_make(rsqrt_apx(a), rsqrt_apx(b)), row[p]);
+                    if (far_sw(k1)) {             // resolved at compile time: k1 is unrolled
+                        row[p] = f2_fma(qq, f2_rsqrt_sw(r2), row[p]);
+                    } else {
+                        float a, b;
+                        f2_split(r2, a, b);
+                        row[p] = f2_fma(qq, f2_make(rsqrt_apx(a), rsqrt_apx(b)), row[p]);
+                    }
                 }
             }
             j += NP1;

@@ -411,7 +411,9 @@ def roofline(sfu, tflops, fma_peak, prec, rep, ev_ms, w, mufu_per_eval, rsqrt_ra
             phys = (evals - sym / 2) * mufu_per_eval / (ev_ms * 1e-3) / 1e9
             r.update(symmetric_evaluations=sym, mufu_physical=phys, frac_physical=phys / rsqrt_rate,
                      note="achieved counts evaluations as the reference does (each direction of a near-field "
-                          "pair); mufu_physical counts the 1/r the GPU computed (one per symmetric pair)")
+                          "pair); mufu_physical counts the 1/r the GPU computed (one per symmetric pair), as "
+                          "MUFU operations, although one grid point in eight (or fewer) of the Lagrange far "
+                          "field takes its 1/r on the FP32 pipe instead")
     else:
         r.update(bound="fp64-simt" if prec == 0 else "fp32-simt", achieved=tflops, peak=fma_peak, unit="TFLOP/s",
                  frac=tflops / fma_peak if tflops else None)
