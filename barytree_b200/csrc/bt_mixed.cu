@@ -89,19 +89,20 @@ __host__ __device__ constexpr int rb_blocks()
     return HERM ? BT_MX_MIN_BLOCKS_HERM : KT == 2 ? BT_MX_MIN_BLOCKS_YUK : BT_MX_MIN_BLOCKS_T2;
 }
 
-// Share of the Lagrange far field's grid points (Coulomb and regularised
-// Coulomb) whose 1/r comes from rsqrt_sw / f2_rsqrt_sw on the FP32 and
-// integer pipes instead of the MUFU: BT_FAR_SW of every 8 by k1 index (1:
-// k1 = 0, and 8 at degrees above 7).  A far-field value needs only two FP32
+// Grid points of each row of the Lagrange far field (Coulomb and
+// regularised Coulomb) whose 1/r comes from rsqrt_sw / f2_rsqrt_sw on the
+// FP32 and integer pipes instead of the MUFU: the first BT_FAR_SW of the
+// row's n+1 (k1 < BT_FAR_SW).  A far-field value needs only two FP32
 // operations besides its 1/r, so the FP32 pipe has room that the MUFU
 // lacks, but less than that count suggests: on the 16M clustered system
-// the evaluation took 819.8 ms with none, 802.7 ms with 1 of 8, and 829,
-// 863 and 919 ms with 2, 3 and 4 of 8 (same rel-L2, 1.0e-7).  Both forms
-// round alike lane by lane, so every tile shape still gives the same bits.
+// (degrees 4 to 11, mostly 5 to 7) the evaluation took 819.8 ms with none
+// on the FP32 pipe, 802.7 ms with one per row of up to 8, and 829, 863
+// and 919 ms with 2, 3 and 4 of 8 (same rel-L2, 1.0e-7).  Both forms round
+// alike lane by lane, so every tile shape still gives the same bits.
 #ifndef BT_FAR_SW
 #define BT_FAR_SW 1
 #endif
-__host__ __device__ constexpr bool far_sw(int k1) { return (k1 * BT_FAR_SW) % 8 < BT_FAR_SW; }
+__host__ __device__ constexpr bool far_sw(int k1) { return k1 < BT_FAR_SW; }
 
 // Far field of one source cluster (degree NP1-1) for NT targets at (x,y,z),
 // relative to the target centre; g = grid coordinates relative to the same
